@@ -1,0 +1,669 @@
+// C ABI (include/fpm.h) and the reconstruction loop.
+//
+// The loop is the reference's epoch x mini-batch schedule
+// (cuFPM_v3/cuFPM_pure_v3.cu:128-207): per batch, spectrum of the current
+// object -> per-LED forward model, loss gradient and back-propagation ->
+// gradient spectrum -> object gradient -> RMSprop on object and pupil; the
+// learning rate halves after epochs with index > lr_halve_after.  Unlike the
+// reference it never synchronises inside the loop: everything is queued on one
+// stream and the host waits once, at the end.
+#include "../../include/fpm.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "fft.h"
+
+using namespace fpm;
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    // grow-only: keeps an existing allocation that is large enough
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();  // clear the sticky-free allocation error
+            return e;
+        }
+        bytes = n;
+        return cudaSuccess;
+    }
+    template <class T>
+    T *as() const {
+        return static_cast<T *>(p);
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// per-stage device timing
+// ---------------------------------------------------------------------------
+namespace {
+
+enum Stage : int {
+    ST_FFT_LARGE_FWD, ST_CROP, ST_FFT_BATCH_INV, ST_FEATURE, ST_LOSS, ST_FFT_BATCH_FWD,
+    ST_STITCH, ST_PUPIL_GRAD, ST_FFT_LARGE_INV, ST_RMS_OBJECT, ST_RMS_PUPIL, ST_COUNT
+};
+const char *const kStageName[ST_COUNT] = {
+    "fft_large_forward", "crop_pupil", "fft_batch_inverse", "feature_grad", "loss_reduce",
+    "fft_batch_forward", "stitch_gather", "pupil_grad", "fft_large_inverse", "rmsprop_object",
+    "rmsprop_pupil"};
+const int kStageOwn[ST_COUNT] = {0, 1, 0, 1, 1, 0, 1, 1, 0, 1, 1};
+
+struct Profiler {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<int> rec_stage;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rec;
+    double ms[ST_COUNT] = {};
+    int n[ST_COUNT] = {};
+    cudaEvent_t open = nullptr;
+
+    ~Profiler() {
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+    void reset() {
+        used = 0;
+        rec.clear();
+        rec_stage.clear();
+        for (int i = 0; i < ST_COUNT; ++i) ms[i] = 0.0, n[i] = 0;
+    }
+    cudaEvent_t get() {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    void begin(cudaStream_t st) {
+        if (!on) return;
+        open = get();
+        if (open) cudaEventRecord(open, st);
+    }
+    void end(int stage, cudaStream_t st) {
+        if (!on || !open) return;
+        cudaEvent_t e = get();
+        if (!e) return;
+        cudaEventRecord(e, st);
+        rec.emplace_back(open, e);
+        rec_stage.push_back(stage);
+        open = nullptr;
+    }
+    // after the stream has been synchronised
+    void collect() {
+        if (!on) return;
+        for (size_t i = 0; i < rec.size(); ++i) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, rec[i].first, rec[i].second) == cudaSuccess) {
+                ms[rec_stage[i]] += t;
+                n[rec_stage[i]] += 1;
+            }
+        }
+        rec.clear();
+        rec_stage.clear();
+        used = 0;
+    }
+};
+
+}  // namespace
+
+struct fpm_context {
+    Profiler prof;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t mem_limit = 0;
+    std::string err;
+    FftEngine fft;
+    // work buffers, kept between calls
+    DevBuf O, m1, S, G, P, m2, P0, dP, T1, T2, Y, led, parts, loss, minmax, spec;
+};
+
+namespace {
+
+fpm_status fail(fpm_context *ctx, fpm_status s, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    return s;
+}
+
+fpm_status fail_cuda(fpm_context *ctx, cudaError_t e, const char *what, int line) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(ctx, FPM_ERR_OUT_OF_MEMORY, "%s: out of device memory (line %d)", what, line);
+    return fail(ctx, FPM_ERR_CUDA, "%s failed: %s (line %d)", what, cudaGetErrorString(e), line);
+}
+
+#define FPM_CK(call)                                                   \
+    do {                                                               \
+        cudaError_t e_ = (call);                                       \
+        if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call, __LINE__); \
+    } while (0)
+
+// Runs one stage launch, bracketed by profiling events when enabled.
+#define FPM_STAGE(id, call)                 \
+    do {                                    \
+        ctx->prof.begin(ctx->stream);       \
+        FPM_CK(call);                       \
+        ctx->prof.end((id), ctx->stream);   \
+    } while (0)
+
+bool is_device_ptr(const void *p, int device) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) &&
+           a.device == device;
+}
+
+bool is_host_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered || a.type == cudaMemoryTypeHost;
+}
+
+// crop box of one batch in centred coordinates, taken modulo H
+Box batch_box(const std::vector<int32_t> &led, int first, int nb, int h, int H) {
+    int rlo = 1 << 30, rhi = -(1 << 30), clo = 1 << 30, chi = -(1 << 30);
+    for (int i = first; i < first + nb; ++i) {
+        const int kl = led[2 * i], kt = led[2 * i + 1];
+        rlo = std::min(rlo, kt - 1);
+        rhi = std::max(rhi, kt - 1 + h);
+        clo = std::min(clo, kl - 1);
+        chi = std::max(chi, kl - 1 + h);
+    }
+    Box b;
+    b.r_lo = rlo;
+    b.r_span = rhi - rlo;
+    b.c_lo = clo;
+    b.c_span = chi - clo;
+    if (b.r_span >= H) b.r_lo = 0, b.r_span = H;
+    if (b.c_span >= H) b.c_lo = 0, b.c_span = H;
+    return b;
+}
+
+struct Shape {
+    int h, H, L, B, pratio;
+    size_t plane, big;
+};
+
+fpm_status validate(fpm_context *ctx, const fpm_problem *p, bool need_batch) {
+    if (!p) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "problem is NULL");
+    if (p->h < 2 || (p->h & 1))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "h = %d: must be even and >= 2", p->h);
+    if (p->pratio < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pratio = %d < 1", p->pratio);
+    const long long H = (long long)p->h * p->pratio;
+    if (H > 32768)
+        return fail(ctx, FPM_ERR_UNSUPPORTED, "H = h*pratio = %lld exceeds 32768", H);
+    if (p->n_leds < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "n_leds = %d < 1", p->n_leds);
+    if (need_batch) {
+        if (p->batch < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "batch = %d < 1", p->batch);
+        if (p->epochs < 0)
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "epochs = %d < 0", p->epochs);
+        if (!std::isfinite(p->lr) || !std::isfinite(p->beta) || !std::isfinite(p->eps) ||
+            !std::isfinite(p->pupil_margin) || !std::isfinite(p->lr_decay))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "non-finite optimiser parameter");
+        if (p->beta < 0.f || p->beta > 1.f)
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "beta = %g outside [0, 1]", p->beta);
+        if (p->eps < 0.f) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "eps = %g < 0", p->eps);
+    }
+    if (std::min(p->batch, p->n_leds) > 1024 && need_batch)
+        return fail(ctx, FPM_ERR_UNSUPPORTED, "batch of %d LEDs exceeds 1024",
+                    std::min(p->batch, p->n_leds));
+    if (p->loss_kind != FPM_LOSS_ANISOTROPIC)
+        return fail(ctx, FPM_ERR_UNSUPPORTED, "loss_kind %d not supported", p->loss_kind);
+    if (p->memory != FPM_MEM_HOST && p->memory != FPM_MEM_DEVICE)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", p->memory);
+    if (p->stack_type != FPM_STACK_F32_AMPLITUDE && p->stack_type != FPM_STACK_U16_COUNTS)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "stack_type = %d", p->stack_type);
+    if (!p->stack || !p->led_idx || !p->pupil_init || !p->pupil_amp)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT,
+                    "stack, led_idx, pupil_init and pupil_amp are required");
+    const void *ptrs[5] = {p->stack, p->led_idx, p->pupil_init, p->pupil_amp, p->object_init};
+    const char *names[5] = {"stack", "led_idx", "pupil_init", "pupil_amp", "object_init"};
+    for (int i = 0; i < 5; ++i) {
+        if (!ptrs[i]) continue;
+        if (p->memory == FPM_MEM_DEVICE && !is_device_ptr(ptrs[i], ctx->device))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT,
+                        "%s is not device memory of device %d", names[i], ctx->device);
+        if (p->memory == FPM_MEM_HOST && !is_host_ptr(ptrs[i]))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "%s is not host memory", names[i]);
+    }
+    return FPM_OK;
+}
+
+fpm_status check_leds(fpm_context *ctx, const std::vector<int32_t> &led, int L, int H) {
+    for (int i = 0; i < L; ++i) {
+        const int kl = led[2 * i], kt = led[2 * i + 1];
+        if (kl < 1 || kl > H || kt < 1 || kt > H)
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT,
+                        "led_idx[%d] = (%d, %d) outside [1, %d]", i, kl, kt, H);
+    }
+    return FPM_OK;
+}
+
+struct Inputs {
+    StackView Y;
+    const int2 *led = nullptr;
+    std::vector<int32_t> led_host;
+};
+
+// Brings every input to the device (or adopts device pointers) and fills `in`.
+fpm_status stage_inputs(fpm_context *ctx, const fpm_problem *p, const Shape &s, Inputs &in) {
+    cudaStream_t st = ctx->stream;
+    const size_t ybytes = s.plane * s.L * (p->stack_type == FPM_STACK_U16_COUNTS ? 2 : 4);
+    in.led_host.resize(2 * (size_t)s.L);
+    if (p->memory == FPM_MEM_HOST) {
+        std::memcpy(in.led_host.data(), p->led_idx, 2 * sizeof(int32_t) * s.L);
+    } else {
+        FPM_CK(cudaMemcpyAsync(in.led_host.data(), p->led_idx, 2 * sizeof(int32_t) * s.L,
+                               cudaMemcpyDeviceToHost, st));
+        FPM_CK(cudaStreamSynchronize(st));
+    }
+    fpm_status rc = check_leds(ctx, in.led_host, s.L, s.H);
+    if (rc != FPM_OK) return rc;
+    if (p->memory == FPM_MEM_HOST) {
+        FPM_CK(ctx->Y.ensure(ybytes));
+        FPM_CK(cudaMemcpyAsync(ctx->Y.p, p->stack, ybytes, cudaMemcpyHostToDevice, st));
+        FPM_CK(ctx->led.ensure(2 * sizeof(int32_t) * s.L));
+        FPM_CK(cudaMemcpyAsync(ctx->led.p, p->led_idx, 2 * sizeof(int32_t) * s.L,
+                               cudaMemcpyHostToDevice, st));
+        in.Y.ptr = ctx->Y.p;
+        in.led = ctx->led.as<int2>();
+    } else {
+        in.Y.ptr = p->stack;
+        in.led = reinterpret_cast<const int2 *>(p->led_idx);
+    }
+    in.Y.type = p->stack_type == FPM_STACK_U16_COUNTS ? kStackU16 : kStackF32;
+    if (in.Y.type == kStackU16) {
+        FPM_CK(ctx->minmax.ensure(2 * sizeof(unsigned)));
+        FPM_CK(launch_stack_minmax(static_cast<const uint16_t *>(in.Y.ptr), s.plane * s.L,
+                                   ctx->minmax.as<unsigned>(), st));
+        in.Y.minmax = ctx->minmax.as<unsigned>();
+    }
+    return FPM_OK;
+}
+
+size_t solve_bytes(const fpm_problem *p, const Shape &s, int nb_max, bool host) {
+    size_t b = 0;
+    b += s.big * 8 * 3;          // O, S, G
+    b += s.big * 4;              // m1
+    b += s.plane * (8 * 3 + 4 * 2);  // P, dP, spare, m2, P0
+    b += s.plane * 8 * 2 * nb_max;   // T1, T2
+    if (host) b += s.plane * s.L * (p->stack_type == FPM_STACK_U16_COUNTS ? 2 : 4);
+    return b;
+}
+
+// One mini-batch: gradients at the current (O, P) of LEDs [cur, cur+nb).
+// Leaves g = IFFT2(G) in ctx->G and dP in ctx->dP; adds the loss to *loss_slot.
+fpm_status run_batch(fpm_context *ctx, const Shape &s, const Inputs &in, float2 *O,
+                     const float2 *P, int cur, int nb, double *loss_slot) {
+    cudaStream_t st = ctx->stream;
+    float2 *S = ctx->S.as<float2>();
+    float2 *G = ctx->G.as<float2>();
+    float2 *T1 = ctx->T1.as<float2>();
+    float2 *T2 = ctx->T2.as<float2>();
+    FPM_STAGE(ST_FFT_LARGE_FWD, ctx->fft.run(O, S, s.H, 1, kForward, st));               // K1
+    FPM_STAGE(ST_CROP, launch_crop_pupil(S, P, in.led, cur, nb, s.h, s.H, T1, st));     // K2
+    FPM_STAGE(ST_FFT_BATCH_INV, ctx->fft.run(T1, T1, s.h, nb, kInverse, st));           // K3
+    FPM_STAGE(ST_FEATURE, launch_feature_grad(T1, in.Y, cur, nb, s.h, s.pratio, T2,      // K4
+                                              ctx->parts.as<double>(), st));
+    FPM_STAGE(ST_LOSS, launch_loss_accumulate(ctx->parts.as<double>(),
+                                              nb * feature_grad_blocks_per_image(s.h),
+                                              loss_slot, st));
+    FPM_STAGE(ST_FFT_BATCH_FWD, ctx->fft.run(T2, T1, s.h, nb, kForward, st));           // K5
+    const Box box = batch_box(in.led_host, cur, nb, s.h, s.H);
+    FPM_STAGE(ST_STITCH, launch_stitch_gather(T1, P, in.led, cur, nb, s.h, s.H, box, G, st));
+    FPM_STAGE(ST_PUPIL_GRAD,
+              launch_pupil_grad(S, T1, in.led, cur, nb, s.h, s.H, ctx->dP.as<float2>(), st));
+    FPM_STAGE(ST_FFT_LARGE_INV, ctx->fft.run(G, G, s.H, 1, kInverse, st));              // K8
+    return FPM_OK;
+}
+
+fpm_status shape_of(fpm_context *ctx, const fpm_problem *p, Shape &s, bool need_batch) {
+    fpm_status rc = validate(ctx, p, need_batch);
+    if (rc != FPM_OK) return rc;
+    s.h = p->h;
+    s.pratio = p->pratio;
+    s.H = p->h * p->pratio;
+    s.L = p->n_leds;
+    s.B = need_batch ? std::min(p->batch, p->n_leds) : p->n_leds;
+    s.plane = (size_t)s.h * s.h;
+    s.big = (size_t)s.H * s.H;
+    return FPM_OK;
+}
+
+fpm_status alloc_common(fpm_context *ctx, const fpm_problem *p, const Shape &s) {
+    const size_t need = solve_bytes(p, s, s.B, p->memory == FPM_MEM_HOST);
+    if (ctx->mem_limit && need > ctx->mem_limit)
+        return fail(ctx, FPM_ERR_OUT_OF_MEMORY,
+                    "solve needs %zu bytes of device memory, limit is %zu", need,
+                    ctx->mem_limit);
+    FPM_CK(ctx->S.ensure(s.big * 8));
+    FPM_CK(ctx->G.ensure(s.big * 8));
+    FPM_CK(ctx->T1.ensure(s.plane * 8 * s.B));
+    FPM_CK(ctx->T2.ensure(s.plane * 8 * s.B));
+    FPM_CK(ctx->dP.ensure(s.plane * 8));
+    FPM_CK(ctx->parts.ensure(sizeof(double) * (size_t)s.B * feature_grad_blocks_per_image(s.h)));
+    return FPM_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int32_t fpm_abi_version(void) { return FPM_ABI_VERSION; }
+
+const char *fpm_status_string(fpm_status s) {
+    switch (s) {
+        case FPM_OK: return "ok";
+        case FPM_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case FPM_ERR_UNSUPPORTED: return "unsupported";
+        case FPM_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case FPM_ERR_CUDA: return "CUDA error";
+        case FPM_ERR_NONFINITE: return "non-finite loss";
+        case FPM_ERR_NO_DEVICE: return "no CUDA device";
+        case FPM_ERR_INTERNAL: return "internal error";
+    }
+    return "unknown status";
+}
+
+const char *fpm_last_error(const fpm_context *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+fpm_status fpm_set_profiling(fpm_context *ctx, int32_t enable) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->prof.on = enable != 0;
+    ctx->prof.reset();
+    return FPM_OK;
+}
+
+int32_t fpm_stage_times(const fpm_context *ctx, fpm_stage_time *out, int32_t cap) {
+    if (!ctx) return 0;
+    int32_t k = 0;
+    for (int i = 0; i < ST_COUNT; ++i) {
+        if (ctx->prof.n[i] == 0) continue;
+        if (out && k < cap) {
+            out[k].name = kStageName[i];
+            out[k].launches = ctx->prof.n[i];
+            out[k].own_kernel = kStageOwn[i];
+            out[k].ms = ctx->prof.ms[i];
+        }
+        ++k;
+    }
+    return k;
+}
+
+fpm_status fpm_create(fpm_context **out, const fpm_device_opts *opts) {
+    if (!out) return FPM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return FPM_ERR_NO_DEVICE;
+    }
+    const int dev = opts ? opts->device : 0;
+    if (dev < 0 || dev >= ndev) return FPM_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        return FPM_ERR_NO_DEVICE;
+    }
+    fpm_context *ctx = new fpm_context();
+    ctx->device = dev;
+    ctx->mem_limit = opts ? opts->mem_limit_bytes : 0;
+    if (opts && opts->stream) {
+        ctx->stream = static_cast<cudaStream_t>(opts->stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            delete ctx;
+            return FPM_ERR_CUDA;
+        }
+        ctx->own_stream = true;
+    }
+    *out = ctx;
+    return FPM_OK;
+}
+
+void fpm_destroy(fpm_context *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->fft.release();
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    FPM_CK(cudaSetDevice(ctx->device));
+    Shape s;
+    fpm_status rc = shape_of(ctx, p, s, true);
+    if (rc != FPM_OK) return rc;
+    fpm_result none{};
+    if (!res) res = &none;
+    if (p->memory == FPM_MEM_DEVICE) {
+        void *outs[4] = {res->object, res->spectrum, res->pupil, res->loss};
+        for (int i = 0; i < 4; ++i)
+            if (outs[i] && !is_device_ptr(outs[i], ctx->device))
+                return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "result pointer %d is not device memory",
+                            i);
+    }
+    rc = alloc_common(ctx, p, s);
+    if (rc != FPM_OK) return rc;
+    cudaStream_t st = ctx->stream;
+    ctx->prof.reset();
+    Inputs in;
+    rc = stage_inputs(ctx, p, s, in);
+    if (rc != FPM_OK) return rc;
+
+    // object and pupil: work in the caller's device outputs when given, else internal
+    const bool dev = p->memory == FPM_MEM_DEVICE;
+    float2 *O, *P;
+    if (dev && res->object) {
+        O = reinterpret_cast<float2 *>(res->object);
+    } else {
+        FPM_CK(ctx->O.ensure(s.big * 8));
+        O = ctx->O.as<float2>();
+    }
+    if (dev && res->pupil) {
+        P = reinterpret_cast<float2 *>(res->pupil);
+    } else {
+        FPM_CK(ctx->P.ensure(s.plane * 8));
+        P = ctx->P.as<float2>();
+    }
+    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (p->object_init) {
+        if ((const void *)p->object_init != (const void *)O)
+            FPM_CK(cudaMemcpyAsync(O, p->object_init, s.big * 8, kin, st));
+    } else {
+        FPM_CK(launch_bicubic_init(in.Y, s.h, s.pratio, O, st));
+    }
+    if ((const void *)p->pupil_init != (const void *)P)
+        FPM_CK(cudaMemcpyAsync(P, p->pupil_init, s.plane * 8, kin, st));
+    const float *P0;
+    if (dev) {
+        P0 = p->pupil_amp;
+    } else {
+        FPM_CK(ctx->P0.ensure(s.plane * 4));
+        FPM_CK(cudaMemcpyAsync(ctx->P0.p, p->pupil_amp, s.plane * 4, kin, st));
+        P0 = ctx->P0.as<float>();
+    }
+    FPM_CK(ctx->m1.ensure(s.big * 4));
+    FPM_CK(ctx->m2.ensure(s.plane * 4));
+    FPM_CK(cudaMemsetAsync(ctx->m1.p, 0, s.big * 4, st));
+    FPM_CK(cudaMemsetAsync(ctx->m2.p, 0, s.plane * 4, st));
+    const int E = p->epochs;
+    FPM_CK(ctx->loss.ensure(sizeof(double) * std::max(E, 1)));
+    FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double) * std::max(E, 1), st));
+
+    float lr = p->lr;
+    for (int ep = 0; ep < E; ++ep) {
+        for (int cur = 0; cur < s.L; cur += p->batch) {
+            const int nb = std::min(p->batch, s.L - cur);
+            rc = run_batch(ctx, s, in, O, P, cur, nb, ctx->loss.as<double>() + ep);
+            if (rc != FPM_OK) return rc;
+            FPM_STAGE(ST_RMS_OBJECT, launch_rmsprop_object(ctx->G.as<float2>(), O,
+                                                           ctx->m1.as<float>(), s.big, lr,
+                                                           p->beta, p->eps, st));
+            FPM_STAGE(ST_RMS_PUPIL,
+                      launch_rmsprop_pupil(ctx->dP.as<float2>(), P, ctx->m2.as<float>(), P0,
+                                           (int)s.plane, lr, p->beta, p->eps, p->pupil_margin,
+                                           st));
+        }
+        if (ep > p->lr_halve_after) lr = (float)(lr * (double)p->lr_decay);
+    }
+
+    // outputs
+    if (res->spectrum) {
+        FPM_CK(ctx->fft.run(O, ctx->S.as<float2>(), s.H, 1, kForward, st));
+        if (dev) {
+            FPM_CK(launch_centre_spectrum(ctx->S.as<float2>(), s.H,
+                                          reinterpret_cast<float2 *>(res->spectrum), st));
+        } else {
+            FPM_CK(launch_centre_spectrum(ctx->S.as<float2>(), s.H, ctx->G.as<float2>(), st));
+            FPM_CK(cudaMemcpyAsync(res->spectrum, ctx->G.p, s.big * 8, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    if (!dev && res->object)
+        FPM_CK(cudaMemcpyAsync(res->object, O, s.big * 8, cudaMemcpyDeviceToHost, st));
+    if (!dev && res->pupil)
+        FPM_CK(cudaMemcpyAsync(res->pupil, P, s.plane * 8, cudaMemcpyDeviceToHost, st));
+    std::vector<double> loss_h(std::max(E, 1));
+    FPM_CK(cudaMemcpyAsync(loss_h.data(), ctx->loss.p, sizeof(double) * std::max(E, 1),
+                           cudaMemcpyDeviceToHost, st));
+    if (res->loss && dev && E > 0)
+        FPM_CK(cudaMemcpyAsync(res->loss, ctx->loss.p, sizeof(double) * E,
+                               cudaMemcpyDeviceToDevice, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    FPM_CK(cudaGetLastError());
+    ctx->prof.collect();
+    if (res->loss && !dev) std::memcpy(res->loss, loss_h.data(), sizeof(double) * E);
+    for (int ep = 0; ep < E; ++ep)
+        if (!std::isfinite(loss_h[ep]))
+            return fail(ctx, FPM_ERR_NONFINITE, "loss of epoch %d is not finite", ep);
+    return FPM_OK;
+}
+
+fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_object,
+                               float *d_pupil, double *loss) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    FPM_CK(cudaSetDevice(ctx->device));
+    Shape s;
+    fpm_status rc = shape_of(ctx, p, s, false);
+    if (rc != FPM_OK) return rc;
+    if (!p->object_init)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "object_init is required for gradients");
+    if (s.L > 1024) return fail(ctx, FPM_ERR_UNSUPPORTED, "batch of %d LEDs exceeds 1024", s.L);
+    const bool dev = p->memory == FPM_MEM_DEVICE;
+    void *outs[3] = {d_object, d_pupil, loss};
+    for (int i = 0; i < 3; ++i) {
+        if (!outs[i]) continue;
+        if (dev && !is_device_ptr(outs[i], ctx->device))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output %d is not device memory", i);
+        if (!dev && !is_host_ptr(outs[i]))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output %d is not host memory", i);
+    }
+    rc = alloc_common(ctx, p, s);
+    if (rc != FPM_OK) return rc;
+    cudaStream_t st = ctx->stream;
+    ctx->prof.reset();
+    Inputs in;
+    rc = stage_inputs(ctx, p, s, in);
+    if (rc != FPM_OK) return rc;
+    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    FPM_CK(ctx->O.ensure(s.big * 8));
+    FPM_CK(ctx->P.ensure(s.plane * 8));
+    FPM_CK(cudaMemcpyAsync(ctx->O.p, p->object_init, s.big * 8, kin, st));
+    FPM_CK(cudaMemcpyAsync(ctx->P.p, p->pupil_init, s.plane * 8, kin, st));
+    FPM_CK(ctx->loss.ensure(sizeof(double)));
+    FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double), st));
+    rc = run_batch(ctx, s, in, ctx->O.as<float2>(), ctx->P.as<float2>(), 0, s.L,
+                   ctx->loss.as<double>());
+    if (rc != FPM_OK) return rc;
+    const cudaMemcpyKind kout = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (d_object) FPM_CK(cudaMemcpyAsync(d_object, ctx->G.p, s.big * 8, kout, st));
+    if (d_pupil) FPM_CK(cudaMemcpyAsync(d_pupil, ctx->dP.p, s.plane * 8, kout, st));
+    if (loss) FPM_CK(cudaMemcpyAsync(loss, ctx->loss.p, sizeof(double), kout, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    ctx->prof.collect();
+    return FPM_OK;
+}
+
+fpm_status fpm_normalise_stack(fpm_context *ctx, const uint16_t *counts, size_t n,
+                               float *amplitude, int32_t memory) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (!counts || !amplitude || n == 0)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "counts/amplitude NULL or n == 0");
+    FPM_CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const bool dev = memory == FPM_MEM_DEVICE;
+    if (memory != FPM_MEM_DEVICE && memory != FPM_MEM_HOST)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", memory);
+    if (dev && (!is_device_ptr(counts, ctx->device) || !is_device_ptr(amplitude, ctx->device)))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not device memory");
+    if (!dev && (!is_host_ptr(counts) || !is_host_ptr(amplitude)))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not host memory");
+    const uint16_t *src = counts;
+    float *dst = amplitude;
+    if (!dev) {
+        FPM_CK(ctx->Y.ensure(n * 2));
+        FPM_CK(ctx->spec.ensure(n * 4));
+        FPM_CK(cudaMemcpyAsync(ctx->Y.p, counts, n * 2, cudaMemcpyHostToDevice, st));
+        src = ctx->Y.as<uint16_t>();
+        dst = ctx->spec.as<float>();
+    }
+    FPM_CK(ctx->minmax.ensure(2 * sizeof(unsigned)));
+    FPM_CK(launch_stack_minmax(src, n, ctx->minmax.as<unsigned>(), st));
+    FPM_CK(launch_normalise(src, n, ctx->minmax.as<unsigned>(), dst, st));
+    if (!dev) FPM_CK(cudaMemcpyAsync(amplitude, dst, n * 4, cudaMemcpyDeviceToHost, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    return FPM_OK;
+}
+
+}  // extern "C"

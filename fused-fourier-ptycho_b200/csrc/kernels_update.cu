@@ -1,0 +1,272 @@
+// Large-array stages (object update, spectrum output, initial object) and the
+// small reductions / ingest kernels.
+#include "common.cuh"
+#include "engine.h"
+
+namespace fpm {
+
+// ---------------------------------------------------------------------------
+// RMSprop on the object (constrained_RMSprop_both, first half,
+// cuFPM_v3/cuda/kernels.cuh:364-382):
+//   mu = beta*m + (1-beta)|g|²,  w -= g * lr/(sqrt(mu)+eps),  m = mu.
+// The reference also zeroes g; here the next stitch rewrites the whole
+// gradient spectrum, so that store is dropped.  Two complex pixels per thread
+// with 128-bit loads of g and O and a 64-bit load of m.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void rms_one(float gr, float gi, float &wr, float &wi, float &m,
+                                        float lr, float beta, float omb, float eps) {
+    float mu = gr * gr + gi * gi;
+    mu = beta * m + omb * mu;
+    const float sq = lr / (sqrtf(mu) + eps);
+    wr -= gr * sq;
+    wi -= gi * sq;
+    m = mu;
+}
+
+__global__ void __launch_bounds__(256) k_rmsprop_object(const float4 *__restrict__ g,
+                                                         float4 *__restrict__ O,
+                                                         float2 *__restrict__ m, size_t n2,
+                                                         float lr, float beta, float eps) {
+    const float omb = 1.0f - beta;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float4 gv = g[i];
+        float4 w = O[i];
+        float2 mv = m[i];
+        rms_one(gv.x, gv.y, w.x, w.y, mv.x, lr, beta, omb, eps);
+        rms_one(gv.z, gv.w, w.z, w.w, mv.y, lr, beta, omb, eps);
+        O[i] = w;
+        m[i] = mv;
+    }
+}
+
+cudaError_t launch_rmsprop_object(const float2 *g, float2 *O, float *m, size_t n, float lr,
+                                  float beta, float eps, cudaStream_t st) {
+    if (n % 2) return cudaErrorInvalidValue;
+    const size_t n2 = n / 2;
+    size_t gx = (n2 + 255) / 256;
+    const size_t cap = (size_t)kB200SMs * 8 * 8;
+    if (gx > cap) gx = cap;
+    k_rmsprop_object<<<(unsigned)gx, 256, 0, st>>>(reinterpret_cast<const float4 *>(g),
+                                                   reinterpret_cast<float4 *>(O),
+                                                   reinterpret_cast<float2 *>(m), n2, lr, beta,
+                                                   eps);
+    return cudaGetLastError();
+}
+
+// RMSprop on the pupil plus the amplitude box constraint
+// (kernels.cuh:384-410): |P| <- P0 * clamp(|P|, P0-am, P0+am), phase kept.
+__global__ void __launch_bounds__(256) k_rmsprop_pupil(const float2 *__restrict__ dP,
+                                                        float2 *__restrict__ P,
+                                                        float *__restrict__ m,
+                                                        const float *__restrict__ P0, int n,
+                                                        float lr, float beta, float eps,
+                                                        float am) {
+    const float omb = 1.0f - beta;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float2 gv = dP[i];
+        float2 w = P[i];
+        float mv = m[i];
+        rms_one(gv.x, gv.y, w.x, w.y, mv, lr, beta, omb, eps);
+        const float p0 = P0[i];
+        const float ang = atan2f(w.y, w.x);
+        float a = sqrtf(w.x * w.x + w.y * w.y);
+        a = p0 * fmaxf(fminf(a, p0 + am), p0 - am);
+        w.x = cosf(ang) * a;
+        w.y = sinf(ang) * a;
+        P[i] = w;
+        m[i] = mv;
+    }
+}
+
+cudaError_t launch_rmsprop_pupil(const float2 *dP, float2 *P, float *m, const float *P0, int n,
+                                 float lr, float beta, float eps, float am, cudaStream_t st) {
+    int gx = (n + 255) / 256;
+    if (gx > kB200SMs * 8) gx = kB200SMs * 8;
+    k_rmsprop_pupil<<<gx, 256, 0, st>>>(dP, P, m, P0, n, lr, beta, eps, am);
+    return cudaGetLastError();
+}
+
+// out = fftshift(S) (even H: swap halves on both axes).
+__global__ void __launch_bounds__(256) k_centre_spectrum(const float2 *__restrict__ S, int H,
+                                                          float2 *__restrict__ out) {
+    const size_t total = (size_t)H * H;
+    const int hh = H >> 1;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(q % H);
+        const int c = (int)(q / H);
+        const int rs = r + hh >= H ? r + hh - H : r + hh;
+        const int cs = c + hh >= H ? c + hh - H : c + hh;
+        out[q] = S[(size_t)cs * H + rs];
+    }
+}
+
+cudaError_t launch_centre_spectrum(const float2 *S, int H, float2 *out, cudaStream_t st) {
+    const size_t total = (size_t)H * H;
+    size_t gx = (total + 255) / 256;
+    const size_t cap = (size_t)kB200SMs * 8 * 8;
+    if (gx > cap) gx = cap;
+    k_centre_spectrum<<<(unsigned)gx, 256, 0, st>>>(S, H, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Initial object: MATLAB imresize(Y_1, pratio, 'bicubic') with zero phase
+// (codes_v2/main_run_FPM.m:47-48).  Output pixel u (1-based) samples input
+// x = u/p + (1 - 1/p)/2 with the a = -0.5 cubic on 4 taps, weights normalised
+// to sum 1, half-sample-symmetric edges; rows are resized first, in FP64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double cubic_w(double t) {
+    const double a = -0.5;
+    t = fabs(t);
+    if (t <= 1.0) return (a + 2.0) * t * t * t - (a + 3.0) * t * t + 1.0;
+    if (t < 2.0) return a * t * t * t - 5.0 * a * t * t + 8.0 * a * t - 4.0 * a;
+    return 0.0;
+}
+
+__device__ __forceinline__ void cubic_taps(int u0, int p, int n, int idx[4], double w[4]) {
+    const double x = (double)(u0 + 1) / p + 0.5 * (1.0 - 1.0 / p);
+    const double left = floor(x - 2.0);
+    double s = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        const double t = left + 1.0 + k;      // 1-based tap
+        w[k] = cubic_w(x - t);
+        s += w[k];
+        int j = (int)t - 1;                   // 0-based, mirror with the edge repeated
+        const int period = 2 * n;
+        j = ((j % period) + period) % period;
+        idx[k] = j < n ? j : period - 1 - j;
+    }
+    for (int k = 0; k < 4; ++k) w[k] /= s;
+}
+
+template <int TYPE>
+__global__ void __launch_bounds__(256) k_bicubic_init(StackView Y, int h, int p,
+                                                       float2 *__restrict__ O) {
+    const int H = h * p;
+    const size_t total = (size_t)H * H;
+    float mn = 0.f, range = 0.f;
+    if (TYPE == kStackU16) {
+        mn = (float)Y.minmax[0];
+        range = (float)(Y.minmax[1] - Y.minmax[0]);
+    }
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int R = (int)(q % H);
+        const int C = (int)(q / H);
+        int ir[4], ic[4];
+        double wr[4], wc[4];
+        cubic_taps(R, p, h, ir, wr);
+        cubic_taps(C, p, h, ic, wc);
+        double acc = 0.0;
+        for (int kc = 0; kc < 4; ++kc) {
+            double t = 0.0;
+            for (int kr = 0; kr < 4; ++kr) {
+                const size_t idx = (size_t)ic[kc] * h + ir[kr];
+                float a;
+                if (TYPE == kStackF32) {
+                    a = static_cast<const float *>(Y.ptr)[idx];
+                } else {
+                    const float x = (float)static_cast<const uint16_t *>(Y.ptr)[idx] - mn;
+                    a = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+                }
+                t += wr[kr] * (double)a;
+            }
+            acc += wc[kc] * t;
+        }
+        O[q] = make_float2((float)acc, 0.f);
+    }
+}
+
+cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, cudaStream_t st) {
+    const size_t total = (size_t)h * pratio * h * pratio;
+    size_t gx = (total + 255) / 256;
+    const size_t cap = (size_t)kB200SMs * 8 * 8;
+    if (gx > cap) gx = cap;
+    if (Y.type == kStackU16)
+        k_bicubic_init<kStackU16><<<(unsigned)gx, 256, 0, st>>>(Y, h, pratio, O);
+    else
+        k_bicubic_init<kStackF32><<<(unsigned)gx, 256, 0, st>>>(Y, h, pratio, O);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic FP64 loss reduction: one block sums the per-tile partials in a
+// fixed order (Kahan per thread, then a fixed tree) and adds them to *slot.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_loss_accumulate(const double *__restrict__ parts, int n,
+                                                           double *__restrict__ slot) {
+    __shared__ double s[1024];
+    KahanD acc;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc.add(parts[i]);
+    s[threadIdx.x] = acc.s;
+    __syncthreads();
+    for (int w = 512; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *slot += s[0];
+}
+
+cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cudaStream_t st) {
+    k_loss_accumulate<<<1, 1024, 0, st>>>(parts, n, slot);
+    return cudaGetLastError();
+}
+
+// Global min / max of a uint16 stack (integer atomics: order-independent).
+__global__ void __launch_bounds__(256) k_stack_minmax(const uint16_t *__restrict__ p, size_t n,
+                                                       unsigned *__restrict__ mm) {
+    unsigned lo = 0xffffu, hi = 0u;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const unsigned v = p[i];
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned a = __shfl_down_sync(0xffffffffu, lo, off);
+        const unsigned b = __shfl_down_sync(0xffffffffu, hi, off);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&mm[0], lo);
+        atomicMax(&mm[1], hi);
+    }
+}
+
+cudaError_t launch_stack_minmax(const uint16_t *p, size_t n, unsigned *mm, cudaStream_t st) {
+    const unsigned init[2] = {0xffffu, 0u};
+    cudaError_t e = cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    size_t gx = (n + 255) / 256;
+    if (gx > (size_t)kB200SMs * 16) gx = (size_t)kB200SMs * 16;
+    if (gx == 0) gx = 1;
+    k_stack_minmax<<<(unsigned)gx, 256, 0, st>>>(p, n, mm);
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) k_normalise(const uint16_t *__restrict__ p, size_t n,
+                                                    const unsigned *__restrict__ mm,
+                                                    float *__restrict__ out) {
+    const float mn = (float)mm[0];
+    const float range = (float)(mm[1] - mm[0]);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float x = (float)p[i] - mn;
+        out[i] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+    }
+}
+
+cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *mm, float *out,
+                             cudaStream_t st) {
+    size_t gx = (n + 255) / 256;
+    if (gx > (size_t)kB200SMs * 16) gx = (size_t)kB200SMs * 16;
+    if (gx == 0) gx = 1;
+    k_normalise<<<(unsigned)gx, 256, 0, st>>>(p, n, mm, out);
+    return cudaGetLastError();
+}
+
+}  // namespace fpm

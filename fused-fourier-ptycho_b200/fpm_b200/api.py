@@ -1,0 +1,302 @@
+"""ctypes binding of libfpm (include/fpm.h) and the Python mirror of the reference call.
+
+The mirror keeps the reference mex's argument list and MATLAB array shapes:
+
+    O, P = cuFPM_pure_v3(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, [lr, beta, eps])
+
+(``cuFPM_v3/cuFPM_pure_v3.cu:44-66``, call site ``codes_v2/main_run_FPM.m:98-106``)
+with ``O0`` complex H x H, ``P0c`` complex h x h, ``Y`` h x h x L (float32
+amplitude as the mex takes, or uint16 counts), ``ledIdx`` int32 2 x L
+(``[kl; kt]``), ``P0`` real h x h.  Arrays may be numpy arrays (host memory,
+copied by the engine) or torch CUDA tensors (device memory, used in place);
+their index order is MATLAB's, and they are handed to the C ABI in
+column-major memory order (numpy Fortran order; for torch, dimensions
+reversed and made contiguous, which is free for tensors already laid out so).
+
+There is no CPU path: without the built library or a CUDA device every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libfpm.so"
+
+FPM_OK = 0
+STATUS_NAMES = {0: "FPM_OK", 1: "FPM_ERR_INVALID_ARGUMENT", 2: "FPM_ERR_UNSUPPORTED",
+                3: "FPM_ERR_OUT_OF_MEMORY", 4: "FPM_ERR_CUDA", 5: "FPM_ERR_NONFINITE",
+                6: "FPM_ERR_NO_DEVICE", 7: "FPM_ERR_INTERNAL"}
+MEM_HOST, MEM_DEVICE = 0, 1
+STACK_F32, STACK_U16 = 0, 1
+LOSS_ANISOTROPIC = 0
+
+# Every symbol include/fpm.h declares.
+EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
+            "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
+            "fpm_last_error", "fpm_abi_version"]
+
+
+class FpmError(RuntimeError):
+    def __init__(self, status: int, detail: str):
+        self.status = status
+        self.detail = detail
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {detail}")
+
+
+class DeviceOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("reserved0", C.c_int32),
+                ("mem_limit_bytes", C.c_size_t), ("stream", C.c_void_p)]
+
+
+class Problem(C.Structure):
+    _fields_ = [("h", C.c_int32), ("n_leds", C.c_int32), ("pratio", C.c_int32),
+                ("batch", C.c_int32), ("epochs", C.c_int32),
+                ("lr", C.c_float), ("beta", C.c_float), ("eps", C.c_float),
+                ("pupil_margin", C.c_float), ("lr_halve_after", C.c_int32),
+                ("lr_decay", C.c_float), ("loss_kind", C.c_int32), ("memory", C.c_int32),
+                ("stack_type", C.c_int32),
+                ("stack", C.c_void_p), ("led_idx", C.c_void_p), ("pupil_init", C.c_void_p),
+                ("pupil_amp", C.c_void_p), ("object_init", C.c_void_p)]
+
+
+class StageTime(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("launches", C.c_int32), ("own_kernel", C.c_int32),
+                ("ms", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("object", C.c_void_p), ("spectrum", C.c_void_p), ("pupil", C.c_void_p),
+                ("loss", C.c_void_p)]
+
+
+_lib = None
+
+
+def load_library(path: str | Path | None = None):
+    """Load libfpm.so (built in-tree by ``fpm_b200._build.build``); raises if absent."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else _LIB_PATH
+    if not p.exists():
+        raise ImportError(f"libfpm.so not built at {p}; run __graft_entry__.build()")
+    lib = C.CDLL(str(p))
+    lib.fpm_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(DeviceOpts)]
+    lib.fpm_create.restype = C.c_int
+    lib.fpm_solve.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
+    lib.fpm_solve.restype = C.c_int
+    lib.fpm_batch_gradients.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_void_p, C.c_void_p,
+                                        C.c_void_p]
+    lib.fpm_batch_gradients.restype = C.c_int
+    lib.fpm_normalise_stack.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int32]
+    lib.fpm_normalise_stack.restype = C.c_int
+    lib.fpm_destroy.argtypes = [C.c_void_p]
+    lib.fpm_destroy.restype = None
+    lib.fpm_status_string.argtypes = [C.c_int]
+    lib.fpm_status_string.restype = C.c_char_p
+    lib.fpm_last_error.argtypes = [C.c_void_p]
+    lib.fpm_last_error.restype = C.c_char_p
+    lib.fpm_set_profiling.argtypes = [C.c_void_p, C.c_int32]
+    lib.fpm_set_profiling.restype = C.c_int
+    lib.fpm_stage_times.argtypes = [C.c_void_p, C.POINTER(StageTime), C.c_int32]
+    lib.fpm_stage_times.restype = C.c_int32
+    lib.fpm_abi_version.argtypes = []
+    lib.fpm_abi_version.restype = C.c_int32
+    if path is None:
+        _lib = lib
+    return lib
+
+
+# ---------------------------------------------------------------------------
+# array marshalling (MATLAB index order <-> column-major memory)
+# ---------------------------------------------------------------------------
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _colmajor(x, dtype):
+    """(pointer, keep-alive object, memory kind) of x in column-major memory."""
+    if _is_torch(x):
+        import torch
+        tdt = {np.complex64: torch.complex64, np.float32: torch.float32,
+               np.uint16: torch.uint16, np.int32: torch.int32}[dtype]
+        if x.dtype != tdt:
+            raise TypeError(f"expected {tdt}, got {x.dtype}")
+        y = x.permute(*reversed(range(x.dim()))).contiguous()
+        mem = MEM_DEVICE if y.is_cuda else MEM_HOST
+        return y.data_ptr(), y, mem
+    a = np.asfortranarray(np.asarray(x, dtype=dtype))
+    return a.ctypes.data, a, MEM_HOST
+
+
+def _empty_like_layout(shape, dtype, device_tensor_like):
+    """Output buffer whose MATLAB-order view is returned and whose memory is column-major."""
+    if device_tensor_like is not None:
+        import torch
+        tdt = {np.complex64: torch.complex64, np.float64: torch.float64}[dtype]
+        base = torch.empty(tuple(reversed(shape)), dtype=tdt, device=device_tensor_like.device)
+        return base.data_ptr(), base.permute(*reversed(range(len(shape))))
+    a = np.empty(shape, dtype=dtype, order="F")
+    return a.ctypes.data, a
+
+
+class Engine:
+    """One libfpm context (one CUDA device, one stream; not thread-safe)."""
+
+    def __init__(self, device: int = 0, mem_limit_bytes: int = 0, stream: int | None = None):
+        self.lib = load_library()
+        self._ctx = C.c_void_p()
+        opts = DeviceOpts(device, 0, mem_limit_bytes, stream or None)
+        st = self.lib.fpm_create(C.byref(self._ctx), C.byref(opts))
+        if st != FPM_OK:
+            raise FpmError(st, self.lib.fpm_status_string(st).decode())
+
+    def close(self):
+        if self._ctx:
+            self.lib.fpm_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int):
+        if st != FPM_OK:
+            detail = self.lib.fpm_last_error(self._ctx).decode()
+            raise FpmError(st, detail)
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.fpm_set_profiling(self._ctx, 1 if on else 0))
+
+    def stage_times(self):
+        """{stage: (launches, summed device ms, own kernel?)} of the last call."""
+        n = self.lib.fpm_stage_times(self._ctx, None, 0)
+        arr = (StageTime * max(n, 1))()
+        n = self.lib.fpm_stage_times(self._ctx, arr, n)
+        return {arr[i].name.decode(): (arr[i].launches, arr[i].ms, bool(arr[i].own_kernel))
+                for i in range(n)}
+
+    # -- raw entry points (pointers already laid out) --------------------------
+    def solve_raw(self, prob: Problem, res: Result) -> int:
+        return self.lib.fpm_solve(self._ctx, C.byref(prob), C.byref(res))
+
+    def gradients_raw(self, prob: Problem, d_obj, d_pup, loss) -> int:
+        return self.lib.fpm_batch_gradients(self._ctx, C.byref(prob), d_obj, d_pup, loss)
+
+    # -- MATLAB-shaped entry points --------------------------------------------
+    def _problem(self, O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr, beta, eps, am,
+                 lr_halve_after, lr_decay):
+        keep = []
+        y_is_u16 = (str(getattr(Y, "dtype", "")).endswith("uint16"))
+        ydt = np.uint16 if y_is_u16 else np.float32
+        ys, yk, ymem = _colmajor(Y, ydt)
+        keep.append(yk)
+        ls, lk, lmem = _colmajor(led_idx, np.int32)
+        keep.append(lk)
+        ps, pk, pmem = _colmajor(P0c, np.complex64)
+        keep.append(pk)
+        as_, ak, amem = _colmajor(P0, np.float32)
+        keep.append(ak)
+        os_ = None
+        omem = ymem
+        if O0 is not None:
+            os_, ok, omem = _colmajor(O0, np.complex64)
+            keep.append(ok)
+        if len({ymem, lmem, pmem, amem, omem}) != 1:
+            raise ValueError("all inputs must live in the same memory (host or one CUDA device)")
+        shp = tuple(Y.shape)
+        h = int(shp[0])
+        L = int(shp[2]) if len(shp) == 3 else 1
+        prob = Problem(h=h, n_leds=L, pratio=int(pratio), batch=int(batch), epochs=int(epochs),
+                       lr=lr, beta=beta, eps=eps, pupil_margin=am, lr_halve_after=lr_halve_after,
+                       lr_decay=lr_decay, loss_kind=LOSS_ANISOTROPIC, memory=ymem,
+                       stack_type=STACK_U16 if y_is_u16 else STACK_F32, stack=ys, led_idx=ls,
+                       pupil_init=ps, pupil_amp=as_, object_init=os_)
+        return prob, keep, ymem
+
+    def solve(self, O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr=5e-4, beta=0.999,
+              eps=1e-4, am=0.2, lr_halve_after=12, lr_decay=0.5, spectrum=True):
+        """Full reconstruction; returns dict(object, pupil, spectrum, loss) in MATLAB order."""
+        prob, keep, mem = self._problem(O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr,
+                                        beta, eps, am, lr_halve_after, lr_decay)
+        h = prob.h
+        H = h * prob.pratio
+        like = Y if mem == MEM_DEVICE else None
+        op, o = _empty_like_layout((H, H), np.complex64, like)
+        pp, p = _empty_like_layout((h, h), np.complex64, like)
+        sp, s = (None, None)
+        if spectrum:
+            sp, s = _empty_like_layout((H, H), np.complex64, like)
+        lp, loss = _empty_like_layout((max(int(epochs), 1),), np.float64, like)
+        res = Result(object=op, spectrum=sp, pupil=pp, loss=lp)
+        self._check(self.solve_raw(prob, res))
+        del keep
+        return {"object": o, "pupil": p, "spectrum": s, "loss": loss[: int(epochs)]}
+
+    def batch_gradients(self, O, P, Y, led_idx, P0, pratio):
+        """v3 gradients of one LED batch (the fullyfusedFPM contract): (dO, dP, loss)."""
+        prob, keep, mem = self._problem(O, P, Y, led_idx, P0, pratio, 0, 1, 0.0, 0.0, 0.0, 0.0,
+                                        12, 0.5)
+        h = prob.h
+        H = h * prob.pratio
+        like = Y if mem == MEM_DEVICE else None
+        op, o = _empty_like_layout((H, H), np.complex64, like)
+        pp, p = _empty_like_layout((h, h), np.complex64, like)
+        lp, loss = _empty_like_layout((1,), np.float64, like)
+        self._check(self.gradients_raw(prob, op, pp, lp))
+        del keep
+        return o, p, float(loss[0])
+
+    def normalise_stack(self, counts):
+        """Amplitude sqrt((I-min)/(max-min)) of a uint16 stack, same shape, float32."""
+        if _is_torch(counts):
+            import torch
+            x = counts.contiguous()
+            out = torch.empty(x.shape, dtype=torch.float32, device=x.device)
+            mem = MEM_DEVICE if x.is_cuda else MEM_HOST
+            self._check(self.lib.fpm_normalise_stack(self._ctx, x.data_ptr(), x.numel(),
+                                                     out.data_ptr(), mem))
+            return out
+        x = np.ascontiguousarray(counts, dtype=np.uint16)
+        out = np.empty(x.shape, np.float32)
+        self._check(self.lib.fpm_normalise_stack(self._ctx, x.ctypes.data, x.size,
+                                                 out.ctypes.data, MEM_HOST))
+        return out
+
+
+_default_engine = None
+
+
+def _engine() -> Engine:
+    global _default_engine
+    if _default_engine is None:
+        _default_engine = Engine()
+    return _default_engine
+
+
+def cuFPM_pure_v3(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, opt=(5e-4, 0.999, 1e-4)):
+    """Mirror of ``[O, P] = cuFPM_pure_v3(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, [lr beta eps])``."""
+    r = _engine().solve(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, lr=float(opt[0]),
+                        beta=float(opt[1]), eps=float(opt[2]), spectrum=False)
+    return r["object"], r["pupil"]
+
+
+def fullyfusedFPM(O, P, Y, ledIdx, pratio, P0=None):
+    """Mirror of ``[dldw1, dldw2] = fullyfusedFPM(O, P, Y, ledIdx, pratio)`` with the v3 loss."""
+    if P0 is None:
+        P0 = np.ones(np.asarray(P.shape), np.float32) if not _is_torch(P) else \
+            __import__("torch").ones(P.shape, dtype=__import__("torch").float32, device=P.device)
+    dO, dP, _ = _engine().batch_gradients(O, P, Y, ledIdx, P0, pratio)
+    return dO, dP

@@ -1,0 +1,178 @@
+/*
+ * fpm.h - C ABI of the B200 Fourier-ptychographic reconstruction engine.
+ *
+ * The engine is a drop-in for the reference's MATLAB mex call
+ *
+ *     [O, P] = cuFPM_pure_v3(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, [lr beta eps])
+ *
+ * (cuFPM_v3/cuFPM_pure_v3.cu:44-228; call site codes_v2/main_run_FPM.m:77-106)
+ * and for the gradient-only call of the first generation
+ *
+ *     [dldw1, dldw2] = fullyfusedFPM(O, P, Y, ledIdx, pratio)
+ *
+ * (codes/fusedfpm/fullyfusedFPM.cu:24-169), computed with the v3 loss.
+ *
+ * Conventions
+ *   - All images are square and column-major (MATLAB layout): element (row r,
+ *     col c) of an n x n image sits at index c*n + r.  Stacks are pages of
+ *     h*h elements, page l = LED l.
+ *   - Complex arrays are interleaved {float re, float im} (MATLAB creal32_T).
+ *   - led_idx holds 2*L int32: (kl, kt) per LED, the 1-based column and row of
+ *     the top-left corner of the LED's h x h crop in the centred H x H
+ *     spectrum (MATLAB int32([kl; kt]), codes_v2/main_run_FPM.m:53-55).  A
+ *     crop that runs past the spectrum edge wraps modulo H, as in v3
+ *     (cuFPM_v3/cuda/kernels.cuh:43-47).  1 <= kl, kt <= H is required.
+ *   - h must be even and H = h * pratio.  The caller owns every buffer.
+ *   - Every function returns an fpm_status; nothing throws across the ABI.
+ *   - A context is bound to one CUDA device and is not thread-safe: use one
+ *     context per host thread.
+ *   - There is no CPU fallback: without a usable CUDA device fpm_create fails
+ *     with FPM_ERR_NO_DEVICE.
+ */
+#ifndef FPM_H
+#define FPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FPM_ABI_VERSION 1
+
+typedef enum fpm_status {
+    FPM_OK = 0,
+    FPM_ERR_INVALID_ARGUMENT = 1, /* shapes, sizes, pointers or hyper-parameters rejected */
+    FPM_ERR_UNSUPPORTED = 2,      /* valid request this build does not implement */
+    FPM_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed or exceeded mem_limit_bytes */
+    FPM_ERR_CUDA = 4,             /* a CUDA runtime call or kernel launch failed */
+    FPM_ERR_NONFINITE = 5,        /* the loss became NaN/Inf; outputs hold the last state */
+    FPM_ERR_NO_DEVICE = 6,        /* no usable CUDA device */
+    FPM_ERR_INTERNAL = 7
+} fpm_status;
+
+/* Where the pointers of a problem / result live. */
+typedef enum fpm_memory {
+    FPM_MEM_HOST = 0,   /* ordinary or pinned host memory: copied in and out by the engine */
+    FPM_MEM_DEVICE = 1  /* device memory of the context's device: used in place (zero copy) */
+} fpm_memory;
+
+/* Element type of the measured stack. */
+typedef enum fpm_stack_type {
+    /* float amplitude, already normalised: the reference mex input Y (prhs[2]) */
+    FPM_STACK_F32_AMPLITUDE = 0,
+    /* raw uint16 counts; the engine applies Y = sqrt((I - min) / (max - min)) over
+       the whole stack on the device, bit-identical to codes_v2/main_run_FPM.m:43-45
+       in single precision, and keeps the stack resident as uint16 (2 B/px). */
+    FPM_STACK_U16_COUNTS = 1
+} fpm_stack_type;
+
+typedef enum fpm_loss_kind {
+    /* sum |d/dx (|x| - Y)| + |d/dy (|x| - Y)| with periodic forward differences,
+       sign(0) = +1 (cuFPM_v3/cuda/kernels.cuh:197-275, benchmark/func_ware/ret_loss.m) */
+    FPM_LOSS_ANISOTROPIC = 0
+} fpm_loss_kind;
+
+typedef struct fpm_device_opts {
+    int32_t device;          /* CUDA device ordinal */
+    int32_t reserved0;
+    size_t mem_limit_bytes;  /* 0 = no cap; otherwise solves needing more fail with
+                                FPM_ERR_OUT_OF_MEMORY before allocating anything */
+    void *stream;            /* cudaStream_t to run on, or NULL for a context-owned stream */
+} fpm_device_opts;
+
+/* Inputs of one reconstruction (the nine mex arguments, cuFPM_pure_v3.cu:51-65). */
+typedef struct fpm_problem {
+    int32_t h;               /* low-res side (rows == cols), even */
+    int32_t n_leds;          /* L: pages of the stack and entries of led_idx */
+    int32_t pratio;          /* up-sampling ratio; H = h * pratio (prhs[5]) */
+    int32_t batch;           /* LEDs per mini-batch B (prhs[7]); the last batch holds L mod B */
+    int32_t epochs;          /* prhs[6] */
+    float lr;                /* RMSprop learning rate (prhs[8][0]) */
+    float beta;              /* second-moment decay (prhs[8][1]) */
+    float eps;               /* added outside the square root (prhs[8][2]) */
+    float pupil_margin;      /* am: |P| clamped to P0 * [P0 - am, P0 + am]; reference 0.2 */
+    int32_t lr_halve_after;  /* lr *= lr_decay after each epoch whose 0-based index
+                                exceeds this; reference 12 (cuFPM_pure_v3.cu:204-206) */
+    float lr_decay;          /* reference 0.5 */
+    int32_t loss_kind;       /* fpm_loss_kind */
+    int32_t memory;          /* fpm_memory of every pointer below */
+    int32_t stack_type;      /* fpm_stack_type */
+    const void *stack;       /* h*h*L measured stack (prhs[2]) */
+    const int32_t *led_idx;  /* 2*L int32 (kl, kt) (prhs[3]) */
+    const float *pupil_init; /* complex h*h initial pupil P0c (prhs[1]) */
+    const float *pupil_amp;  /* real h*h pupil amplitude P0 (prhs[4]) */
+    const float *object_init;/* complex H*H initial object O0 (prhs[0]); NULL = bicubic
+                                up-sampling of stack page 0 with zero phase
+                                (codes_v2/main_run_FPM.m:48) */
+} fpm_problem;
+
+/* Outputs.  Any pointer may be NULL to skip that output.  Pointers follow the
+   problem's fpm_memory.  With FPM_MEM_DEVICE, object may alias object_init and
+   pupil may alias pupil_init (updated in place). */
+typedef struct fpm_result {
+    float *object;    /* complex H*H reconstructed object (plhs[0]) */
+    float *spectrum;  /* complex H*H centred spectrum fftshift(fft2(object)) */
+    float *pupil;     /* complex h*h reconstructed pupil (plhs[1]) */
+    double *loss;     /* epochs values: feature-domain loss summed over each epoch's
+                         batches, each batch evaluated before its update */
+} fpm_result;
+
+typedef struct fpm_context fpm_context;
+
+/* Replaces mxInitGPU + the per-call set-up of cuFPM_pure_v3.cu:49-126. */
+fpm_status fpm_create(fpm_context **ctx, const fpm_device_opts *opts);
+
+/* Replaces the body of mexFunction, cuFPM_pure_v3.cu:44-228. */
+fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *prob, fpm_result *res);
+
+/* Gradients of one LED batch at (object, pupil), v3 loss: replaces
+   fullyfusedFPM (codes/fusedfpm/fullyfusedFPM.cu:24-169).  prob->n_leds LEDs
+   form one batch (prob->batch, epochs and optimiser fields are ignored);
+   object_init / pupil_init give the current estimate (object_init must not be
+   NULL).  d_object receives IFFT2 of the stitched gradient spectrum
+   (complex H*H, the dldw1 the RMSprop of cuFPM_pure_v3.cu:189 consumes),
+   d_pupil the pupil gradient (complex h*h, dldw2), loss the batch loss.
+   Any output may be NULL. */
+fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *prob,
+                               float *d_object, float *d_pupil, double *loss);
+
+/* Ingest helper (codes_v2/main_run_FPM.m:43-45): amplitude = sqrt((I-min)/(max-min))
+   over a whole uint16 stack of n elements, computed on the device in single
+   precision.  Pointers follow `memory`. */
+fpm_status fpm_normalise_stack(fpm_context *ctx, const uint16_t *counts, size_t n,
+                               float *amplitude, int32_t memory);
+
+void fpm_destroy(fpm_context *ctx);
+
+/* Per-stage device timing (no counterpart in the reference, which only times
+   the whole mex call with tic/toc, benchmark/cuFPM_recon_2025_circular.m:152-169).
+   When enabled, every stage launch of the next fpm_solve / fpm_batch_gradients
+   is bracketed by CUDA events on the context's stream; fpm_stage_times then
+   reports, per stage, the launches and their summed device time. */
+typedef struct fpm_stage_time {
+    const char *name;   /* static string, e.g. "rmsprop_object" */
+    int32_t launches;   /* stage launches in the last call */
+    int32_t own_kernel; /* 1: a libfpm kernel, 0: a library call (FFT back end) */
+    double ms;          /* summed device time of those launches */
+} fpm_stage_time;
+
+fpm_status fpm_set_profiling(fpm_context *ctx, int32_t enable);
+
+/* Fills up to `cap` entries (stages with launches > 0) and returns how many
+   stages have data. */
+int32_t fpm_stage_times(const fpm_context *ctx, fpm_stage_time *out, int32_t cap);
+
+const char *fpm_status_string(fpm_status s);
+
+/* Human-readable detail of the last failure on this context ("" if none). */
+const char *fpm_last_error(const fpm_context *ctx);
+
+int32_t fpm_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FPM_H */

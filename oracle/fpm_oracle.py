@@ -1,0 +1,348 @@
+"""CPU oracle for the cuFPM_pure_v3 reconstruction loop.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference arm may
+import it.  The product (``libfpm.so``) never calls it and has no CPU path.
+
+It restates, in numpy, the algorithm of the reference solver
+``cuFPM_v3/cuFPM_pure_v3.cu:128-207`` and its kernels
+``cuFPM_v3/cuda/kernels.cuh``.  The readable MATLAB statement of the same math is
+``codes_v2/func_ware/fpm_forward_GPU.m:23-58`` with the loss of
+``benchmark/func_ware/ret_loss.m:1-22``; where MATLAB and the v3 CUDA disagree the
+v3 CUDA semantics are followed:
+
+* ``sign(0) = +1`` (``copysignf``), ``kernels.cuh:11-15``;
+* the phase factor is ``z/|z|`` and 0 where ``|z| = 0``, ``kernels.cuh:265-273``;
+* crop indices wrap modulo H, ``kernels.cuh:43-47``;
+* RMSprop keeps an exponential moving average and adds ``eps`` outside the
+  square root, ``kernels.cuh:368-371``;
+* the pupil amplitude clamp goes through atan2/cos/sin with ``am = 0.2``,
+  ``kernels.cuh:396-402``, ``cuFPM_pure_v3.cu:198``;
+* the learning rate halves after every epoch with index > 12,
+  ``cuFPM_pure_v3.cu:204-206``.
+
+Array convention: every image is a numpy array indexed ``A[row, col]`` exactly
+like the MATLAB arrays the reference receives (MATLAB dim 1 = rows).  The
+column-major memory the C ABI takes is ``np.asfortranarray(A)``.  ``led_idx`` is
+``(L, 2)`` int32 rows ``(kl, kt)``: the 1-based column and row of the top-left
+corner of LED ``l``'s crop in the *centred* H x H spectrum
+(``codes_v2/main_run_FPM.m:53-55``), i.e. MATLAB's ``int32([kl; kt])``.
+
+Two precisions are provided.  ``dtype=np.float64`` is the FP64 transcription
+that the relative errors are quoted against.  ``dtype=np.float32`` is an FP32
+twin that performs the elementwise arithmetic in single precision with the
+same operation order as the CUDA kernels (FFTs by pocketfft in single
+precision); it is what the CPU baseline times.
+
+Parity pins: the reference ships no tests, fixtures or golden vectors.  The
+oracle's stage functions are pinned by known-answer tests against direct
+transcriptions of the MATLAB statements (``ret_loss.m``, ``fft2_ware.m``,
+``ifft2_ware.m``, the stitch loop of ``fpm_forward_GPU.m:48-54``) in
+``tests/test_oracle.py``.
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+try:  # pocketfft with threads; numpy's own FFT is the fallback inside the oracle
+    import scipy.fft as _sfft
+
+    def _fft2(a, workers):
+        return _sfft.fft2(a, workers=workers)
+
+    def _ifft2(a, workers):
+        return _sfft.ifft2(a, workers=workers)
+except Exception:  # pragma: no cover
+    def _fft2(a, workers):
+        return np.fft.fft2(a)
+
+    def _ifft2(a, workers):
+        return np.fft.ifft2(a)
+
+
+def default_workers() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:  # pragma: no cover
+        return os.cpu_count() or 1
+
+
+def sign_copysign(x):
+    """``copysignf(1.0f, x)``: +1 for +0, -1 for -0 (``kernels.cuh:11-15``)."""
+    return np.copysign(np.ones_like(x), x)
+
+
+# ---------------------------------------------------------------------------
+# stage functions (one per reference kernel)
+# ---------------------------------------------------------------------------
+
+def crop_indices(kl: int, kt: int, h: int, H: int):
+    """Row / column indices into the *un-shifted* spectrum of LED ``(kl, kt)``.
+
+    ``fused_getSubpupil_shifted``, ``kernels.cuh:43-47``: the centred-spectrum
+    position ``kt-1+r`` (row) / ``kl-1+c`` (col) is mapped to the un-shifted FFT
+    by adding ``H/2`` modulo ``H``.
+    """
+    r = (kt - 1 + np.arange(h) + H // 2) % H
+    c = (kl - 1 + np.arange(h) + H // 2) % H
+    return r, c
+
+
+def shift_half(a):
+    """Swap halves along both axes (fftshift == ifftshift for even sizes).
+
+    ``kernels.cuh:62-63`` (store at ``(i + h/2) % h``) and ``:92-95`` (load at
+    the same index).
+    """
+    return np.roll(np.roll(a, a.shape[0] // 2, axis=0), a.shape[1] // 2, axis=1)
+
+
+def abs_c(z, dtype):
+    """``sqrtf(re*re + im*im)`` in the working precision (``kernels.cuh:5-9``)."""
+    re = z.real.astype(dtype, copy=False)
+    im = z.imag.astype(dtype, copy=False)
+    return np.sqrt(re * re + im * im)
+
+
+def residual(z, Y_l, h: int, pratio: int, dtype):
+    """``|z| / (h*h*pratio^2) - Y`` (``kernels.cuh:223,233``)."""
+    ratio = dtype(h * h * pratio * pratio)
+    return abs_c(z, dtype) / ratio - Y_l.astype(dtype, copy=False)
+
+
+def feature_grad(res, pratio: int, dtype):
+    """Anisotropic feature-domain gradient of ``Σ|∂c res| + |∂r res|``.
+
+    ``differenceKernel_acc``, ``kernels.cuh:234-263``; MATLAB statement in
+    ``benchmark/func_ware/ret_loss.m:3-4,11-12,18-19`` with periodic forward
+    differences along columns (``x``) and rows (``y``).
+    Returns ``(d, loss)`` with ``d = (ox(c-1)-ox(c) + oy(r-1)-oy(r))·pratio²``
+    and ``loss = Σ |Rx| + |Ry|`` (accumulated in float64).
+    """
+    rx = np.roll(res, -1, axis=1) - res          # res(:, c+1) - res(:, c)
+    ry = np.roll(res, -1, axis=0) - res          # res(r+1, :) - res(r, :)
+    ox = sign_copysign(rx)
+    oy = sign_copysign(ry)
+    d = ((np.roll(ox, 1, axis=1) - ox) + (np.roll(oy, 1, axis=0) - oy)) * dtype(pratio * pratio)
+    loss = float(np.abs(rx.astype(np.float64)).sum() + np.abs(ry.astype(np.float64)).sum())
+    return d.astype(dtype, copy=False), loss
+
+
+def phase_times(z, d, dtype):
+    """``d · z/|z|`` with 0 where ``|z| = 0`` (``kernels.cuh:265-273``)."""
+    ctype = np.complex64 if dtype == np.float32 else np.complex128
+    re = z.real.astype(dtype, copy=False)
+    im = z.imag.astype(dtype, copy=False)
+    mag = np.sqrt(re * re + im * im)
+    nz = mag > 0
+    inv = np.zeros_like(mag)
+    inv[nz] = dtype(1.0) / mag[nz]
+    out = np.empty(z.shape, ctype)
+    out.real = np.where(nz, re * inv * d, 0)
+    out.imag = np.where(nz, im * inv * d, 0)
+    return out
+
+
+def rmsprop_step(w, g, m, lr, beta, eps, dtype):
+    """RMSprop with EMA second moment (``kernels.cuh:365-377``).
+
+    ``mu = beta*m + (1-beta)|g|²``; ``w -= g * lr/(sqrt(mu)+eps)``.
+    Returns ``(w_new, mu)``.
+    """
+    gr = g.real.astype(dtype, copy=False)
+    gi = g.imag.astype(dtype, copy=False)
+    b = dtype(beta)
+    mu = gr * gr + gi * gi
+    mu = b * m + (dtype(1.0) - b) * mu
+    sq = dtype(lr) / (np.sqrt(mu) + dtype(eps))
+    out = np.empty_like(w)
+    out.real = w.real - gr * sq
+    out.imag = w.imag - gi * sq
+    return out, mu
+
+
+def pupil_clamp(w, P0, am, dtype):
+    """``|P| <- P0 · clamp(|P|, P0-am, P0+am)``, phase kept (``kernels.cuh:396-402``)."""
+    re = w.real.astype(dtype, copy=False)
+    im = w.imag.astype(dtype, copy=False)
+    ang = np.arctan2(im, re)
+    a = np.sqrt(re * re + im * im)
+    p0 = P0.astype(dtype, copy=False)
+    a = p0 * np.maximum(np.minimum(a, p0 + dtype(am)), p0 - dtype(am))
+    out = np.empty_like(w)
+    out.real = np.cos(ang) * a
+    out.imag = np.sin(ang) * a
+    return out
+
+
+# ---------------------------------------------------------------------------
+# one LED batch (cuFPM_pure_v3.cu:135-199)
+# ---------------------------------------------------------------------------
+
+def batch_gradients(S, P, Y_b, leds_b, pratio: int, dtype, workers: int = 1):
+    """Gradients of one LED batch at the current object spectrum ``S``.
+
+    ``S`` is the *un-shifted* FFT2 of the object (``cuFPM_pure_v3.cu:135-140``).
+    Returns ``(G, dP, loss)`` where ``G`` is the un-shifted gradient spectrum
+    already divided by ``H²`` (``kernels.cuh:114-116``), ``dP`` the pupil
+    gradient (``kernels.cuh:118-128``, no normalisation) and ``loss`` the
+    feature-domain loss of the batch.
+    """
+    ctype = np.complex64 if dtype == np.float32 else np.complex128
+    H = S.shape[0]
+    h = P.shape[0]
+    G = np.zeros((H, H), ctype)
+    dP = np.zeros((h, h), ctype)
+    loss = 0.0
+    inv_H2 = dtype(1.0) / dtype(H * H)
+    for l in range(len(leds_b)):
+        kl, kt = int(leds_b[l][0]), int(leds_b[l][1])
+        rr, cc = crop_indices(kl, kt, h, H)
+        sub = S[np.ix_(rr, cc)]
+        # K2: latentZ[ifftshift] = sub·P  (kernels.cuh:49-64)
+        lat = shift_half((sub * P).astype(ctype, copy=False))
+        # K3: unnormalised inverse FFT (cuFPM_pure_v3.cu:151-156)
+        z = (_ifft2(lat, workers) * ctype(h * h)).astype(ctype, copy=False)
+        # K4: feature-domain loss gradient (kernels.cuh:197-275)
+        res = residual(z, Y_b[l], h, pratio, dtype)
+        d, lval = feature_grad(res, pratio, dtype)
+        loss += lval
+        rec = phase_times(z, d, dtype)
+        # K5: unnormalised forward FFT (cuFPM_pure_v3.cu:164-169), read shifted
+        X = shift_half(_fft2(rec, workers).astype(ctype, copy=False))
+        # K7: G += conj(P)·X / H² at the crop; dP += conj(sub)·X (kernels.cuh:95-128)
+        G[np.ix_(rr, cc)] += (np.conj(P) * X) * inv_H2
+        dP += np.conj(sub) * X
+    return G, dP, loss
+
+
+# ---------------------------------------------------------------------------
+# full solver (cuFPM_pure_v3.cu:44-228)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class OracleResult:
+    object: np.ndarray
+    pupil: np.ndarray
+    spectrum: np.ndarray
+    loss: np.ndarray
+    m_object: np.ndarray = field(repr=False, default=None)
+    m_pupil: np.ndarray = field(repr=False, default=None)
+
+
+def cufpm_pure_v3(O0, P0c, Y, led_idx, P0, pratio: int, epochs: int, batch: int,
+                  opt=(5e-4, 0.999, 1e-4), am: float = 0.2, lr_halve_after: int = 12,
+                  dtype=np.float64, workers: int | None = None) -> OracleResult:
+    """Oracle of ``[O, P] = cuFPM_pure_v3(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, [lr beta eps])``.
+
+    ``Y`` is ``(L, h, h)`` amplitude (page ``l`` = LED ``l``, the reference's
+    ``h x h x L`` MATLAB array with the page axis moved first).  The
+    hyper-parameters are rounded to float32 first, as the mex does
+    (``cuFPM_pure_v3.cu:63-65``).  Returns the object, pupil, the centred
+    spectrum ``fftshift(fft2(O))`` and the per-epoch loss.
+    """
+    if workers is None:
+        workers = default_workers()
+    ctype = np.complex64 if dtype == np.float32 else np.complex128
+    lr = float(np.float32(opt[0]))
+    beta = float(np.float32(opt[1]))
+    eps = float(np.float32(opt[2]))
+    am = float(np.float32(am))
+    O = np.array(O0, dtype=ctype, copy=True)
+    P = np.array(P0c, dtype=ctype, copy=True)
+    P0 = np.asarray(P0, dtype=dtype)
+    Y = np.asarray(Y)
+    L = Y.shape[0]
+    H = O.shape[0]
+    h = P.shape[0]
+    m1 = np.zeros((H, H), dtype)
+    m2 = np.zeros((h, h), dtype)
+    losses = np.zeros(epochs, np.float64)
+    for ep in range(epochs):
+        cur = 0
+        while cur < L:                       # cuFPM_pure_v3.cu:131-141
+            nb = min(batch, L - cur)
+            S = _fft2(O, workers).astype(ctype, copy=False)
+            G, dP, lv = batch_gradients(S, P, Y[cur:cur + nb], led_idx[cur:cur + nb],
+                                        pratio, dtype, workers)
+            losses[ep] += lv
+            # K8: unnormalised inverse FFT of G (the 1/H² is already inside G)
+            g = (_ifft2(G, workers) * ctype(H * H)).astype(ctype, copy=False)
+            del G
+            # K9: RMSprop on O and P, then the pupil clamp (kernels.cuh:364-410)
+            O, m1 = rmsprop_step(O, g, m1, lr, beta, eps, dtype)
+            del g
+            Pn, m2 = rmsprop_step(P, dP, m2, lr, beta, eps, dtype)
+            P = pupil_clamp(Pn, P0, am, dtype)
+            cur += batch
+        if ep > lr_halve_after:              # cuFPM_pure_v3.cu:204-206
+            lr = float(np.float32(lr * 0.5))
+    spec = np.fft.fftshift(_fft2(O, workers)).astype(ctype, copy=False)
+    return OracleResult(O, P, spec, losses, m1, m2)
+
+
+def rel_err(a, b) -> float:
+    """``||a-b||₂ / ||b||₂`` on complex arrays, no phase alignment."""
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
+    nb = np.linalg.norm(b.ravel())
+    return float(np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0))
+
+
+# ---------------------------------------------------------------------------
+# set-up helpers that the reference runs in MATLAB (restated for checking)
+# ---------------------------------------------------------------------------
+
+def normalise_stack_u16(I_u16):
+    """``Y = sqrt((I - min) / max(I - min))`` over the whole stack, in single.
+
+    ``codes_v2/main_run_FPM.m:43-45`` (MATLAB ``single`` arithmetic; the
+    subtraction of integers below 2^24 is exact, then one correctly rounded
+    division and one correctly rounded square root).
+    """
+    x = np.asarray(I_u16).astype(np.float32)
+    x = x - x.min()
+    mx = x.max()
+    x = x / mx if mx > 0 else x
+    return np.sqrt(x).astype(np.float32)
+
+
+def _cubic(x, a=-0.5):
+    ax = np.abs(x)
+    ax2 = ax * ax
+    ax3 = ax2 * ax
+    return np.where(ax <= 1, (a + 2) * ax3 - (a + 3) * ax2 + 1,
+                    np.where(ax < 2, a * ax3 - 5 * a * ax2 + 8 * a * ax - 4 * a, 0.0))
+
+
+def imresize_bicubic_weights(n_in: int, scale: int):
+    """Tap indices and weights of MATLAB ``imresize(..., scale, 'bicubic')`` (up-scaling).
+
+    Output pixel ``u`` (1-based) samples input ``x = u/scale + 0.5(1-1/scale)``
+    with the a=-0.5 cubic, four taps, weights normalised to sum 1 and
+    half-sample-symmetric edge handling (``codes_v2/main_run_FPM.m:48``).
+    Returns 0-based ``(idx[n_out, 4], w[n_out, 4])``.
+    """
+    n_out = n_in * scale
+    u = np.arange(1, n_out + 1, dtype=np.float64)
+    x = u / scale + 0.5 * (1.0 - 1.0 / scale)
+    left = np.floor(x - 2.0)
+    idx = left[:, None] + np.arange(1, 5)[None, :]      # 1-based taps floor(x-2)+1 .. +4
+    w = _cubic(x[:, None] - idx)
+    w = w / w.sum(axis=1, keepdims=True)
+    aux = np.concatenate([np.arange(1, n_in + 1), np.arange(n_in, 0, -1)])
+    idx = aux[np.mod(idx.astype(np.int64) - 1, 2 * n_in)] - 1
+    return idx.astype(np.int64), w
+
+
+def imresize_bicubic(img, scale: int):
+    """Separable bicubic up-scaling in float64 (rows first, then columns)."""
+    img = np.asarray(img, np.float64)
+    ir, wr = imresize_bicubic_weights(img.shape[0], scale)
+    ic, wc = imresize_bicubic_weights(img.shape[1], scale)
+    t = (img[ir, :] * wr[:, :, None]).sum(axis=1)            # (n_out_r, n_c)
+    out = (t[:, ic] * wc[None, :, :]).sum(axis=2)            # (n_out_r, n_out_c)
+    return out

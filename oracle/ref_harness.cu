@@ -1,0 +1,207 @@
+// TEST INFRASTRUCTURE.  Drives the reference's own v3 kernels
+// (cuFPM_v3/cuda/kernels.cuh, compiled from the read-only reference tree by
+// oracle/build_ref.py into oracle/_ref/libcufpm_ref.so) with a replica of the
+// host loop of cuFPM_v3/cuFPM_pure_v3.cu:75-207, minus MATLAB.  Used only by
+// tests/ as a checker (it pins the numpy oracle against the reference itself)
+// and to time the reference's GPU build on the same device; never by the
+// product.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include "kernels.cuh"
+
+namespace {
+
+// cuFPM_pure_v3.cu:10-18: dims of an (rows, cols, pages) array -> {cols, rows, pages}
+dim3 dims_of(int rows, int cols, int pages) { return dim3((unsigned)cols, (unsigned)rows, (unsigned)pages); }
+
+struct Bufs {
+    creal32_t *O = nullptr, *P = nullptr, *latentZ = nullptr, *recordZ = nullptr,
+              *subwave = nullptr, *dldw1 = nullptr, *dldw2 = nullptr;
+    real32_T *mom1 = nullptr, *mom2 = nullptr, *Y = nullptr, *P0 = nullptr;
+    int2 *led = nullptr;
+    void free_all() {
+        void *ps[] = {O, P, latentZ, recordZ, subwave, dldw1, dldw2, mom1, mom2, Y, P0, led};
+        for (void *p : ps)
+            if (p) cudaFree(p);
+    }
+};
+
+#define RCK(x)                                   \
+    do {                                         \
+        if ((x) != 0) {                          \
+            b.free_all();                        \
+            return __LINE__;                     \
+        }                                        \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+// Full solve (cuFPM_pure_v3 semantics).  Host arrays in, host arrays out,
+// column-major.  ms[0] = epoch-loop time, ms[1] = allocation + plans + loop.
+int ref_solve(int h, int H, int L, int pratio, int epochs, int batch, float lr, float beta,
+              float eps, const float *O0, const float *P0c, const float *Y, const int *led,
+              const float *P0, float *O_out, float *P_out, float *ms) {
+    Bufs b;
+    const size_t plane = (size_t)h * h, big = (size_t)H * H;
+    RCK(cudaMalloc(&b.O, big * 8));
+    RCK(cudaMalloc(&b.P, plane * 8));
+    RCK(cudaMalloc(&b.Y, plane * L * 4));
+    RCK(cudaMalloc(&b.P0, plane * 4));
+    RCK(cudaMalloc(&b.led, (size_t)L * 8));
+    RCK(cudaMemcpy(b.O, O0, big * 8, cudaMemcpyHostToDevice));
+    RCK(cudaMemcpy(b.P, P0c, plane * 8, cudaMemcpyHostToDevice));
+    RCK(cudaMemcpy(b.Y, Y, plane * L * 4, cudaMemcpyHostToDevice));
+    RCK(cudaMemcpy(b.P0, P0, plane * 4, cudaMemcpyHostToDevice));
+    RCK(cudaMemcpy(b.led, led, (size_t)L * 8, cudaMemcpyHostToDevice));
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    RCK(cudaDeviceSynchronize());
+    cudaEventRecord(e0);
+
+    dim3 imLs_sz = dims_of(h, h, L);
+    dim3 imHs_sz = dims_of(H, H, 1);
+    const size_t arraysize = plane * batch;
+    RCK(cudaMalloc(&b.latentZ, arraysize * 8));
+    RCK(cudaMalloc(&b.subwave, arraysize * 8));
+    RCK(cudaMalloc(&b.recordZ, arraysize * 8));
+    RCK(cudaMalloc(&b.dldw1, big * 8));
+    RCK(cudaMalloc(&b.dldw2, plane * 8));
+    RCK(cudaMalloc(&b.mom1, big * 4));
+    RCK(cudaMalloc(&b.mom2, plane * 4));
+    cudaMemset(b.mom1, 0, big * 4);
+    cudaMemset(b.mom2, 0, plane * 4);
+    dim3 N_THREADS = {BLOCK_X, BLOCK_Y, 1};
+    dim3 N_BLOCKS_L = {(imHs_sz.x + BLOCK_X - 1) / BLOCK_X, (imHs_sz.y + BLOCK_Y - 1) / BLOCK_Y, 1};
+    dim3 N_BLOCKS = {(imLs_sz.x + BLOCK_X - 1) / BLOCK_X, (imLs_sz.y + BLOCK_Y - 1) / BLOCK_Y, 1};
+    const int led_total = (int)imLs_sz.z;
+    int inembed[2] = {(int)imLs_sz.x, (int)imLs_sz.y};
+    imLs_sz.z = batch;
+    cufftHandle planLarge, planBatch;
+    if (cufftPlan2d(&planLarge, imHs_sz.x, imHs_sz.y, CUFFT_C2C) != CUFFT_SUCCESS) {
+        b.free_all();
+        return -1;
+    }
+    if (cufftPlanMany(&planBatch, 2, inembed, inembed, 1, (int)plane, inembed, 1, (int)plane,
+                      CUFFT_C2C, batch) != CUFFT_SUCCESS) {
+        cufftDestroy(planLarge);
+        b.free_all();
+        return -2;
+    }
+    cudaEventRecord(e1);
+    for (int epoch = 0; epoch < epochs; ++epoch) {
+        int remain = led_total, curr = 0;
+        while (remain > 0) {
+            remain -= batch;
+            cufftExecC2C(planLarge, (cufftComplex *)b.O, (cufftComplex *)b.dldw1, CUFFT_FORWARD);
+            N_BLOCKS.z = (unsigned)(min(curr + batch - 1, led_total - 1) - curr + 1);
+            fused_getSubpupil_shifted<<<N_BLOCKS, N_THREADS>>>(curr, b.dldw1, b.P, b.led, imLs_sz,
+                                                              imHs_sz, b.subwave, b.latentZ);
+            cufftExecC2C(planBatch, (cufftComplex *)b.latentZ, (cufftComplex *)b.latentZ,
+                         CUFFT_INVERSE);
+            differenceKernel_acc<<<N_BLOCKS, N_THREADS>>>(curr, imLs_sz, pratio, b.Y, b.latentZ,
+                                                          b.recordZ);
+            cufftExecC2C(planBatch, (cufftComplex *)b.recordZ, (cufftComplex *)b.latentZ,
+                         CUFFT_FORWARD);
+            cudaMemset(b.dldw1, 0, big * 8);
+            cudaMemset(b.dldw2, 0, plane * 8);
+            fused_deconvPIE_shifted<<<N_BLOCKS, N_THREADS>>>(curr, b.latentZ, b.subwave, b.led,
+                                                             b.P, imLs_sz, imHs_sz, b.dldw1,
+                                                             b.dldw2);
+            cufftExecC2C(planLarge, (cufftComplex *)b.dldw1, (cufftComplex *)b.dldw1,
+                         CUFFT_INVERSE);
+            constrained_RMSprop_both<<<N_BLOCKS_L, N_THREADS>>>(b.dldw1, b.dldw2, beta, lr, eps,
+                                                                imHs_sz, imLs_sz, b.mom1, b.mom2,
+                                                                b.O, b.P, b.P0, 0.2f);
+            curr += batch;
+            cudaDeviceSynchronize();
+        }
+        if (epoch > 12) lr = lr * 0.5;
+    }
+    cudaEventRecord(e2);
+    cudaEventSynchronize(e2);
+    float t_loop = 0.f, t_all = 0.f;
+    cudaEventElapsedTime(&t_loop, e1, e2);
+    cudaEventElapsedTime(&t_all, e0, e2);
+    if (ms) {
+        ms[0] = t_loop;
+        ms[1] = t_all;
+    }
+    int rc = (int)cudaGetLastError();
+    if (rc == 0) {
+        cudaMemcpy(O_out, b.O, big * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(P_out, b.P, plane * 8, cudaMemcpyDeviceToHost);
+    }
+    cufftDestroy(planBatch);
+    cufftDestroy(planLarge);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    b.free_all();
+    return rc;
+}
+
+// Gradients of one batch of all L LEDs at (O, P): the K1..K8 part of one
+// iteration of the loop above.  dO = IFFT2(stitched gradient spectrum), dP
+// the pupil gradient.
+int ref_gradients(int h, int H, int L, int pratio, const float *O, const float *P, const float *Y,
+                  const int *led, float *dO_out, float *dP_out) {
+    Bufs b;
+    const size_t plane = (size_t)h * h, big = (size_t)H * H;
+    RCK(cudaMalloc(&b.O, big * 8));
+    RCK(cudaMalloc(&b.P, plane * 8));
+    RCK(cudaMalloc(&b.Y, plane * L * 4));
+    RCK(cudaMalloc(&b.led, (size_t)L * 8));
+    RCK(cudaMalloc(&b.latentZ, plane * L * 8));
+    RCK(cudaMalloc(&b.subwave, plane * L * 8));
+    RCK(cudaMalloc(&b.recordZ, plane * L * 8));
+    RCK(cudaMalloc(&b.dldw1, big * 8));
+    RCK(cudaMalloc(&b.dldw2, plane * 8));
+    RCK(cudaMemcpy(b.O, O, big * 8, cudaMemcpyHostToDevice));
+    RCK(cudaMemcpy(b.P, P, plane * 8, cudaMemcpyHostToDevice));
+    RCK(cudaMemcpy(b.Y, Y, plane * L * 4, cudaMemcpyHostToDevice));
+    RCK(cudaMemcpy(b.led, led, (size_t)L * 8, cudaMemcpyHostToDevice));
+    dim3 imLs_sz = dims_of(h, h, L);
+    dim3 imHs_sz = dims_of(H, H, 1);
+    dim3 N_THREADS = {BLOCK_X, BLOCK_Y, 1};
+    dim3 N_BLOCKS = {(imLs_sz.x + BLOCK_X - 1) / BLOCK_X, (imLs_sz.y + BLOCK_Y - 1) / BLOCK_Y,
+                     (unsigned)L};
+    int inembed[2] = {(int)imLs_sz.x, (int)imLs_sz.y};
+    cufftHandle planLarge, planBatch;
+    if (cufftPlan2d(&planLarge, imHs_sz.x, imHs_sz.y, CUFFT_C2C) != CUFFT_SUCCESS) {
+        b.free_all();
+        return -1;
+    }
+    if (cufftPlanMany(&planBatch, 2, inembed, inembed, 1, (int)plane, inembed, 1, (int)plane,
+                      CUFFT_C2C, L) != CUFFT_SUCCESS) {
+        cufftDestroy(planLarge);
+        b.free_all();
+        return -2;
+    }
+    cufftExecC2C(planLarge, (cufftComplex *)b.O, (cufftComplex *)b.dldw1, CUFFT_FORWARD);
+    fused_getSubpupil_shifted<<<N_BLOCKS, N_THREADS>>>(0, b.dldw1, b.P, b.led, imLs_sz, imHs_sz,
+                                                      b.subwave, b.latentZ);
+    cufftExecC2C(planBatch, (cufftComplex *)b.latentZ, (cufftComplex *)b.latentZ, CUFFT_INVERSE);
+    differenceKernel_acc<<<N_BLOCKS, N_THREADS>>>(0, imLs_sz, pratio, b.Y, b.latentZ, b.recordZ);
+    cufftExecC2C(planBatch, (cufftComplex *)b.recordZ, (cufftComplex *)b.latentZ, CUFFT_FORWARD);
+    cudaMemset(b.dldw1, 0, big * 8);
+    cudaMemset(b.dldw2, 0, plane * 8);
+    fused_deconvPIE_shifted<<<N_BLOCKS, N_THREADS>>>(0, b.latentZ, b.subwave, b.led, b.P, imLs_sz,
+                                                     imHs_sz, b.dldw1, b.dldw2);
+    cufftExecC2C(planLarge, (cufftComplex *)b.dldw1, (cufftComplex *)b.dldw1, CUFFT_INVERSE);
+    int rc = (int)cudaDeviceSynchronize();
+    if (rc == 0) {
+        cudaMemcpy(dO_out, b.dldw1, big * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(dP_out, b.dldw2, plane * 8, cudaMemcpyDeviceToHost);
+    }
+    cufftDestroy(planBatch);
+    cufftDestroy(planLarge);
+    b.free_all();
+    return rc;
+}
+
+}  // extern "C"
