@@ -63,6 +63,24 @@ class Cfg:
                 "l2": "no flush needed: object 2 GiB, stack 3 GB, both larger than L2"}
 
 
+def make_quick_workload_gpu(cfg: Cfg, dev):
+    """Random uint16 stack with the real optics: for profiler runs, whose per-kernel timing does
+    not depend on the pixel values and whose launch list must hold the engine's kernels only."""
+    import torch
+    from fpm_b200 import synth
+    g = torch.Generator(device=dev)
+    g.manual_seed(cfg.seed)
+    optics = synth.Optics(led_grid=cfg.grid)
+    circ = synth.pupil_circle(cfg.h, optics)
+    led = synth.led_indices(cfg.h, cfg.pratio, optics)
+    stack = torch.randint(0, 30000, (cfg.L, cfg.h, cfg.h), generator=g, device=dev,
+                          dtype=torch.int32).to(torch.uint16)
+    P0 = torch.from_numpy(np.ascontiguousarray(circ.T)).to(dev)
+    torch.cuda.synchronize(dev)
+    return {"stack": stack, "P0": P0, "P0c": P0.to(torch.complex64),
+            "led": torch.from_numpy(np.ascontiguousarray(led)).to(dev), "led_np": led, "circ": circ}
+
+
 def make_workload_gpu(cfg: Cfg, dev):
     """Seeded synthetic data set generated with torch on the GPU (same model as fpm_b200.synth)."""
     import torch
@@ -272,7 +290,7 @@ def run_ours(args, cfg: Cfg):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
     eng = fpm_b200.Engine(local, stream=stream.cuda_stream)
-    wl = make_workload_gpu(cfg, dev)
+    wl = make_quick_workload_gpu(cfg, dev) if args.quick_data else make_workload_gpu(cfg, dev)
     H, h = cfg.H, cfg.h
     O = torch.empty((H, H), dtype=torch.complex64, device=dev)
     P = torch.empty((h, h), dtype=torch.complex64, device=dev)
@@ -371,7 +389,8 @@ def _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e
             "metric": METRIC, "value": round(ms_step * JOB_EPOCHS / 1e3, 4), "unit": "s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms_step, 3), "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (complex64)", "data": "synthetic (seeded, generated on GPU)",
+            "vs_baseline": None, "dtype": "f32 (complex64)",
+            "data": "synthetic (seeded, generated on GPU)" if not args.quick_data else "random stack (profiling)",
             "config": dict(cfg.describe(), parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                            step="one epoch (361 LEDs, 14 mini-batches)"),
             "s_per_epoch": round(ms_step / 1e3, 5),
@@ -448,6 +467,8 @@ def main():
     ap.add_argument("--grid", type=int, default=19)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--quick-data", action="store_true",
+                    help="random stack instead of the simulated one (profiler runs only)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

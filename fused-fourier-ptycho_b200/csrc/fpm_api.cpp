@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -266,6 +267,9 @@ fpm_status validate(fpm_context *ctx, const fpm_problem *p, bool need_batch) {
         if (p->memory == FPM_MEM_DEVICE && !is_device_ptr(ptrs[i], ctx->device))
             return fail(ctx, FPM_ERR_INVALID_ARGUMENT,
                         "%s is not device memory of device %d", names[i], ctx->device);
+        // kernels use 64/128-bit accesses on device buffers
+        if (p->memory == FPM_MEM_DEVICE && (reinterpret_cast<uintptr_t>(ptrs[i]) & 15u))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "%s is not 16-byte aligned", names[i]);
         if (p->memory == FPM_MEM_HOST && !is_host_ptr(ptrs[i]))
             return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "%s is not host memory", names[i]);
     }
@@ -487,10 +491,14 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     if (!res) res = &none;
     if (p->memory == FPM_MEM_DEVICE) {
         void *outs[4] = {res->object, res->spectrum, res->pupil, res->loss};
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i) {
             if (outs[i] && !is_device_ptr(outs[i], ctx->device))
                 return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "result pointer %d is not device memory",
                             i);
+            if (outs[i] && (reinterpret_cast<uintptr_t>(outs[i]) & 15u))
+                return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "result pointer %d is not 16-byte aligned",
+                            i);
+        }
     }
     rc = alloc_common(ctx, p, s);
     if (rc != FPM_OK) return rc;
@@ -605,6 +613,8 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
         if (!outs[i]) continue;
         if (dev && !is_device_ptr(outs[i], ctx->device))
             return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output %d is not device memory", i);
+        if (dev && (reinterpret_cast<uintptr_t>(outs[i]) & 15u))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output %d is not 16-byte aligned", i);
         if (!dev && !is_host_ptr(outs[i]))
             return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output %d is not host memory", i);
     }

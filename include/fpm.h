@@ -55,7 +55,8 @@ typedef enum fpm_status {
 /* Where the pointers of a problem / result live. */
 typedef enum fpm_memory {
     FPM_MEM_HOST = 0,   /* ordinary or pinned host memory: copied in and out by the engine */
-    FPM_MEM_DEVICE = 1  /* device memory of the context's device: used in place (zero copy) */
+    FPM_MEM_DEVICE = 1  /* device memory of the context's device, 16-byte aligned: used in
+                           place (zero copy) */
 } fpm_memory;
 
 /* Element type of the measured stack. */
