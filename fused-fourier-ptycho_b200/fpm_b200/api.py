@@ -36,7 +36,7 @@ LOSS_ANISOTROPIC = 0
 # Every symbol include/fpm.h declares.
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
-            "fpm_last_error", "fpm_abi_version"]
+            "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc"]
 
 
 class FpmError(RuntimeError):

@@ -145,6 +145,29 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *prob,
 fpm_status fpm_normalise_stack(fpm_context *ctx, const uint16_t *counts, size_t n,
                                float *amplitude, int32_t memory);
 
+/* Loss-gradient stage that allocates nothing.  No counterpart in the reference.
+   For callers that cannot call cudaMalloc (a mex inside MATLAB's GPU memory
+   manager, a framework whose caching allocator owns the device, an acquisition
+   loop that must not stall on the device-wide synchronisation an allocation
+   implies).  For n_images fields z (complex h*h each, the unnormalised inverse
+   FFT of crop x pupil, as after cuFPM_pure_v3.cu:151) and their amplitudes
+   (float h*h each) it writes gradient = d * z/|z| (complex h*h each, the
+   loss-gradient stage of fpm_solve) and *loss = the feature-domain loss summed
+   over all images.  All pointers: device memory of the current device, on
+   `stream` (a cudaStream_t; NULL = legacy default stream).
+   Scratch: a fixed device array of FPM_NOALLOC_MAX_TILES FP64 tile partials
+   (512 KiB), held by every GPU that loads the library until exit.  The first
+   call on a device looks up its address (cudaGetSymbolAddress, with that device
+   current); make that first call before any stream capture.  Limit: n_images *
+   ceil(h/32)^2 <= FPM_NOALLOC_MAX_TILES (e.g. 16 images of 2048^2, 256 of 512^2)
+   and n_images <= 65535, else FPM_ERR_UNSUPPORTED before any device work.  Every
+   call shares the one array: calls whose work overlaps on the GPU (other
+   streams, other host threads) race and must be serialised by the caller. */
+#define FPM_NOALLOC_MAX_TILES 65536
+fpm_status fpm_feature_gradient_noalloc(const float *z, const float *amplitude, int32_t h,
+                                        int32_t n_images, int32_t pratio, float *gradient,
+                                        double *loss, void *stream);
+
 void fpm_destroy(fpm_context *ctx);
 
 /* Per-stage device timing (no counterpart in the reference, which only times
