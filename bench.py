@@ -139,25 +139,52 @@ def make_workload_gpu(cfg: Cfg, dev):
 # ---------------------------------------------------------------------------
 # algorithmic bytes per launch of each stage (documented in DESIGN.md)
 # ---------------------------------------------------------------------------
-def stage_bytes(cfg: Cfg):
-    H2 = cfg.H * cfg.H
-    h2 = cfg.h * cfg.h
-    b = cfg.batch
-    L = cfg.L
-    nb_avg = L / math.ceil(L / b)          # LEDs per launch averaged over an epoch
-    return {
-        "fft_large_forward": 16 * H2,      # one read + one write of H x H complex64
-        "fft_large_inverse": 16 * H2,
-        "rmsprop_object": 32 * H2,         # g r8, O r8 w8, m r4 w4
-        "stitch_gather": (8 * H2 + 8 * h2 * nb_avg),   # G w8 per px + X r8 per LED px
-        "crop_pupil": 16 * h2 * nb_avg,    # S crop r8 + T w8 (P from cache)
-        "fft_batch_inverse": 16 * h2 * nb_avg,
-        "fft_batch_forward": 16 * h2 * nb_avg,
-        "feature_grad": 18 * h2 * nb_avg,  # z r8 + Y r2 + out w8
-        "pupil_grad": 16 * h2 * nb_avg,    # S crop r8 + X r8 per LED px
-        "rmsprop_pupil": 36 * h2,
-        "loss_reduce": 8 * (h2 // 1024) * nb_avg,
-    }
+def batch_boxes(led, h, H, batch):
+    """Crop box (rspan, cspan) of every mini-batch, as the engine plans them."""
+    out = []
+    L = len(led)
+    for cur in range(0, L, batch):
+        sl = led[cur:cur + batch]
+        kt = sl[:, 1] - 1
+        kl = sl[:, 0] - 1
+        rspan = min(int((kt + h).max() - kt.min()), H)
+        cspan = min(int((kl + h).max() - kl.min()), H)
+        out.append((len(sl), rspan, cspan))
+    return out
+
+
+def stage_bytes(cfg: Cfg, led):
+    """Average algorithmic bytes per launch of each stage over one epoch."""
+    H, h = cfg.H, cfg.h
+    H2, h2 = H * H, h * h
+    boxes = batch_boxes(led, h, H, cfg.batch)
+    nbatch = len(boxes)
+    group = max(1, min(cfg.batch, (96 << 20) // (h2 * 12)))
+    lr_launches = sum(math.ceil(nb / group) for nb, _, _ in boxes)
+    tot = {k: 0.0 for k in ("lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
+                            "lr_cols_forward", "pupil_grad", "rows_inverse_stitch",
+                            "cols_update", "rows_forward", "rmsprop_pupil")}
+    for bi, (nb, rspan, cspan) in enumerate(boxes):
+        _, rn, cn = boxes[(bi + 1) % nbatch]
+        px = h2 * nb
+        tot["lr_cols_inverse"] += 16 * px      # crop of the spectrum box r8, field w8
+        tot["lr_rows_inverse"] += 22 * px      # field r8 w8, residual w4, stack r2
+        tot["lr_rows_forward"] += 20 * px      # residual r4, field r8 w8
+        tot["lr_cols_forward"] += 16 * px      # field r8, gradient spectrum w8
+        tot["pupil_grad"] += 16 * px + 8 * h2  # spectrum box r8 + gradient spectrum r8 per LED px
+        tot["rows_inverse_stitch"] += 8 * px + 8 * H * rspan
+        tot["cols_update"] += 8 * H * rspan + 24 * H2 + 8 * H * rn
+        tot["rows_forward"] += 8 * H * rn + 8 * rn * cn
+        tot["rmsprop_pupil"] += 36 * h2
+    per = {}
+    for k, v in tot.items():
+        n = lr_launches if k.startswith("lr_") else nbatch
+        per[k] = v / n
+    nb0, r0, c0 = boxes[0]
+    per["cols_forward"] = 8 * H2 + 8 * H * r0
+    per["spectrum_fft2"] = 32 * H2
+    per["loss_reduce"] = 8 * 1024
+    return per
 
 
 # ---------------------------------------------------------------------------
@@ -336,8 +363,8 @@ def run_ours(args, cfg: Cfg):
 
     # e2e: the full 10-epoch job through the C ABI with pinned host buffers
     if args.no_e2e:
-        return _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, None), \
-            wl, rank, world
+        return _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, None,
+                       wl["led_np"]), wl, rank, world
     pin = lambda x: x.cpu().pin_memory()
     hs, hl, hp, ha = pin(wl["stack"]), pin(wl["led"]), pin(wl["P0c"]), pin(wl["P0"])
     hO = torch.empty((H, H), dtype=torch.complex64).pin_memory()
@@ -364,16 +391,17 @@ def run_ours(args, cfg: Cfg):
            "d2h_bytes_per_step": d2h,
            "note": "one 10-epoch job per step through fpm_solve with pinned host buffers; "
                    "stack/LEDs/pupil in, object+spectrum+pupil+loss out"}
-    out = _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e)
+    out = _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e,
+                  wl["led_np"])
     eng.close()
     return out, wl, rank, world
 
 
-def _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e):
+def _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e, wl_led):
     out = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        sb = stage_bytes(cfg)
+        sb = stage_bytes(cfg, wl_led)
         st_rep = {}
         for name, (n, tms, own) in stages.items():
             avg = tms / n

@@ -41,6 +41,7 @@ cudaError_t launch_rmsprop_object(const float2 *g, float2 *O, float *m, size_t n
 cudaError_t launch_rmsprop_pupil(const float2 *dP, float2 *P, float *m, const float *P0, int n,
                                  float lr, float beta, float eps, float am, cudaStream_t st);
 cudaError_t launch_centre_spectrum(const float2 *S, int H, float2 *out, cudaStream_t st);
+cudaError_t launch_centre_in_place(float2 *S, int H, cudaStream_t st);
 cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, cudaStream_t st);
 
 // ---- reductions and ingest ------------------------------------------------

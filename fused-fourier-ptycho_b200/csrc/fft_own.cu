@@ -1,0 +1,177 @@
+// 2-D FFT passes built on the shared-memory line FFT of fft_core.cuh.
+#include <cmath>
+#include <vector>
+
+#include "fft.h"
+#include "fft_core.cuh"
+
+namespace fpm {
+
+namespace {
+
+template <int N>
+struct Geo : fft::Geo<N> {
+    static constexpr int SMEM = fft::Geo<N>::LINE_BYTES + fft::Geo<N>::TW_BYTES;
+};
+
+// Lines along the contiguous axis: line L (over all pages) = elements [L*N, (L+1)*N).
+template <int N, int DIR>
+__global__ void __launch_bounds__(Geo<N>::THREADS) k_fft_contig(const float2 *__restrict__ in,
+                                                                 float2 *__restrict__ out,
+                                                                 long long n_lines,
+                                                                 const float2 *__restrict__ g_hi,
+                                                                 const float2 *__restrict__ g_lo) {
+    using G = Geo<N>;
+    extern __shared__ float2 smem[];
+    float2 *s_hi = smem + G::LPC * N;
+    float2 *s_lo = s_hi + 128;
+    fft::load_twiddles(s_hi, s_lo, g_hi, g_lo, G::NHI, G::NLO);
+    const int line = threadIdx.x / G::T;
+    const int t = threadIdx.x % G::T;
+    const long long L = (long long)blockIdx.x * G::LPC + line;
+    float2 *s = smem + line * N;
+    const bool live = L < n_lines;
+    if (live) {
+        const float2 *src = in + L * N;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) s[fft::swz(t + j * G::T)] = src[t + j * G::T];
+    }
+    __syncthreads();
+    fft::line_fft<N, DIR>(s, s_hi, s_lo, t);
+    if (live) {
+        float2 *dst = out + L * N;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) dst[t + j * G::T] = s[fft::swz(t + j * G::T)];
+    }
+}
+
+// Lines along the strided axis: line (p, r) = elements p*N*N + c*N + r, c = 0..N-1.
+// Lines are numbered g = p*N + r; a CTA takes LPC consecutive g (consecutive r of
+// one page when LPC <= N, whole pages when LPC > N), so each c contributes LPC*8
+// contiguous bytes per page.
+template <int N, int DIR>
+__global__ void __launch_bounds__(Geo<N>::THREADS) k_fft_strided(const float2 *__restrict__ in,
+                                                                  float2 *__restrict__ out,
+                                                                  long long n_lines,
+                                                                  const float2 *__restrict__ g_hi,
+                                                                  const float2 *__restrict__ g_lo) {
+    using G = Geo<N>;
+    extern __shared__ float2 smem[];
+    float2 *s_hi = smem + G::LPC * N;
+    float2 *s_lo = s_hi + 128;
+    fft::load_twiddles(s_hi, s_lo, g_hi, g_lo, G::NHI, G::NLO);
+    const long long g0 = (long long)blockIdx.x * G::LPC;
+    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
+        const int line = q % G::LPC;
+        const int c = q / G::LPC;
+        const long long g = g0 + line;
+        if (g < n_lines) {
+            const size_t addr = (size_t)(g / N) * N * N + (size_t)c * N + (size_t)(g % N);
+            smem[line * N + fft::swz(c)] = in[addr];
+        }
+    }
+    __syncthreads();
+    const int line = threadIdx.x / G::T;
+    fft::line_fft<N, DIR>(smem + line * N, s_hi, s_lo, threadIdx.x % G::T);
+    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
+        const int l2 = q % G::LPC;
+        const int c = q / G::LPC;
+        const long long g = g0 + l2;
+        if (g < n_lines) {
+            const size_t addr = (size_t)(g / N) * N * N + (size_t)c * N + (size_t)(g % N);
+            out[addr] = smem[l2 * N + fft::swz(c)];
+        }
+    }
+}
+
+template <int N, int DIR>
+cudaError_t run_n(const float2 *in, float2 *out, int count, const float2 *hi, const float2 *lo,
+                  cudaStream_t st) {
+    using G = Geo<N>;
+    // per device and cheap: set on every call rather than cached
+    cudaError_t e = cudaFuncSetAttribute(k_fft_contig<N, DIR>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_fft_strided<N, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             G::SMEM);
+    if (e != cudaSuccess) return e;
+    const long long lines = (long long)count * N;
+    const long long blocks = (lines + G::LPC - 1) / G::LPC;
+    k_fft_contig<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(in, out, lines, hi, lo);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_fft_strided<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(out, out, lines, hi, lo);
+    return cudaGetLastError();
+}
+
+template <int DIR>
+cudaError_t dispatch(int n, const float2 *in, float2 *out, int count, const float2 *hi,
+                     const float2 *lo, cudaStream_t st) {
+    switch (n) {
+        case 16: return run_n<16, DIR>(in, out, count, hi, lo, st);
+        case 32: return run_n<32, DIR>(in, out, count, hi, lo, st);
+        case 64: return run_n<64, DIR>(in, out, count, hi, lo, st);
+        case 128: return run_n<128, DIR>(in, out, count, hi, lo, st);
+        case 256: return run_n<256, DIR>(in, out, count, hi, lo, st);
+        case 512: return run_n<512, DIR>(in, out, count, hi, lo, st);
+        case 1024: return run_n<1024, DIR>(in, out, count, hi, lo, st);
+        case 2048: return run_n<2048, DIR>(in, out, count, hi, lo, st);
+        case 4096: return run_n<4096, DIR>(in, out, count, hi, lo, st);
+        case 8192: return run_n<8192, DIR>(in, out, count, hi, lo, st);
+        case 16384: return run_n<16384, DIR>(in, out, count, hi, lo, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+bool fft_supported(int n) { return n >= 16 && n <= kMaxFftLen && (n & (n - 1)) == 0; }
+
+FftEngine::~FftEngine() { release(); }
+
+void FftEngine::release() {
+    for (auto &kv : tw_) cudaFree(kv.second);
+    tw_.clear();
+}
+
+cudaError_t FftEngine::tables(int n, const float2 **hi, const float2 **lo) {
+    auto it = tw_.find(n);
+    const int nhi = n >= 128 ? n / 128 : 1;
+    const int nlo = n >= 128 ? 128 : n;
+    if (it == tw_.end()) {
+        std::vector<float2> h(nhi + nlo);
+        const double two_pi = 6.283185307179586476925286766559;
+        for (int j = 0; j < nhi; ++j) {
+            const double a = -two_pi * (double)(j * 128) / n;
+            h[j] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        for (int j = 0; j < nlo; ++j) {
+            const double a = -two_pi * (double)j / n;
+            h[nhi + j] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        float2 *d = nullptr;
+        cudaError_t e = cudaMalloc(&d, h.size() * sizeof(float2));
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(d);
+            return e;
+        }
+        it = tw_.emplace(n, d).first;
+    }
+    *hi = it->second;
+    *lo = it->second + nhi;
+    return cudaSuccess;
+}
+
+cudaError_t FftEngine::run(const float2 *in, float2 *out, int n, int count, FftDir dir,
+                           cudaStream_t st) {
+    if (!fft_supported(n) || count < 1) return cudaErrorInvalidValue;
+    const float2 *hi, *lo;
+    cudaError_t e = tables(n, &hi, &lo);
+    if (e != cudaSuccess) return e;
+    return dir == kForward ? dispatch<-1>(n, in, out, count, hi, lo, st)
+                           : dispatch<+1>(n, in, out, count, hi, lo, st);
+}
+
+}  // namespace fpm

@@ -6,7 +6,9 @@
 // gradient spectrum -> object gradient -> RMSprop on object and pupil; the
 // learning rate halves after epochs with index > lr_halve_after.  Unlike the
 // reference it never synchronises inside the loop: everything is queued on one
-// stream and the host waits once, at the end.
+// stream and the host waits once, at the end.  Each batch runs the fused
+// pipeline of pipeline.cu (low-resolution passes, stitch + row inverse FFT,
+// column pass with the object RMSprop, row forward FFT of the next batch's box).
 #include "../../include/fpm.h"
 
 #include <cuda_runtime.h>
@@ -22,6 +24,7 @@
 
 #include "engine.h"
 #include "fft.h"
+#include "pipeline.h"
 
 using namespace fpm;
 
@@ -70,14 +73,15 @@ struct DevBuf {
 namespace {
 
 enum Stage : int {
-    ST_FFT_LARGE_FWD, ST_CROP, ST_FFT_BATCH_INV, ST_FEATURE, ST_LOSS, ST_FFT_BATCH_FWD,
-    ST_STITCH, ST_PUPIL_GRAD, ST_FFT_LARGE_INV, ST_RMS_OBJECT, ST_RMS_PUPIL, ST_COUNT
+    ST_COLS_FORWARD, ST_ROWS_FORWARD, ST_LR_COLS_INV, ST_LR_ROWS_INV, ST_LR_ROWS_FWD,
+    ST_LR_COLS_FWD, ST_LOSS, ST_PUPIL_GRAD, ST_ROWS_INV, ST_COLS_UPDATE, ST_RMS_PUPIL,
+    ST_SPECTRUM, ST_COUNT
 };
 const char *const kStageName[ST_COUNT] = {
-    "fft_large_forward", "crop_pupil", "fft_batch_inverse", "feature_grad", "loss_reduce",
-    "fft_batch_forward", "stitch_gather", "pupil_grad", "fft_large_inverse", "rmsprop_object",
-    "rmsprop_pupil"};
-const int kStageOwn[ST_COUNT] = {0, 1, 0, 1, 1, 0, 1, 1, 0, 1, 1};
+    "cols_forward", "rows_forward", "lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
+    "lr_cols_forward", "loss_reduce", "pupil_grad", "rows_inverse_stitch", "cols_update",
+    "rmsprop_pupil", "spectrum_fft2"};
+const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
 
 struct Profiler {
     bool on = false;
@@ -147,7 +151,7 @@ struct fpm_context {
     std::string err;
     FftEngine fft;
     // work buffers, kept between calls
-    DevBuf O, m1, S, G, P, m2, P0, dP, T1, T2, Y, led, parts, loss, minmax, spec;
+    DevBuf O, m1, S, P, m2, P0, dP, T1, Rs, Xs, Sbox, U, V, Y, led, parts, loss, minmax, spec;
 };
 
 namespace {
@@ -234,8 +238,10 @@ fpm_status validate(fpm_context *ctx, const fpm_problem *p, bool need_batch) {
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "h = %d: must be even and >= 2", p->h);
     if (p->pratio < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pratio = %d < 1", p->pratio);
     const long long H = (long long)p->h * p->pratio;
-    if (H > 32768)
-        return fail(ctx, FPM_ERR_UNSUPPORTED, "H = h*pratio = %lld exceeds 32768", H);
+    if (H > kMaxFftLen || !pipeline_supported(p->h, (int)H))
+        return fail(ctx, FPM_ERR_UNSUPPORTED,
+                    "h = %d, H = %lld: this build needs powers of two, 16 <= h <= 8192, H <= %d",
+                    p->h, H, kMaxFftLen);
     if (p->n_leds < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "n_leds = %d < 1", p->n_leds);
     if (need_batch) {
         if (p->batch < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "batch = %d < 1", p->batch);
@@ -328,39 +334,129 @@ fpm_status stage_inputs(fpm_context *ctx, const fpm_problem *p, const Shape &s, 
     return FPM_OK;
 }
 
-size_t solve_bytes(const fpm_problem *p, const Shape &s, int nb_max, bool host) {
+// Crop boxes of every mini-batch of an epoch (the same every epoch).
+struct Plan {
+    std::vector<BatchGeom> geoms;
+    int ldU = 0;        // max box rows
+    size_t sbox = 0;    // max box rows x cols
+    int group = 1;      // LEDs per low-resolution launch group
+    int parts = 0;      // loss partial slots of the largest batch
+};
+
+Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch) {
+    Plan pl;
+    for (int cur = 0; cur < s.L; cur += batch) {
+        const int nb = std::min(batch, s.L - cur);
+        const Box b = batch_box(led, cur, nb, s.h, s.H);
+        BatchGeom g;
+        g.H = s.H;
+        g.h = s.h;
+        g.pratio = s.pratio;
+        g.z_off = cur;
+        g.nb = nb;
+        g.rlo = b.r_lo;
+        g.rspan = b.r_span;
+        g.clo = b.c_lo;
+        g.cspan = b.c_span;
+        g.Ru0 = (g.rlo + s.H / 2) % s.H;
+        g.Cu0 = (g.clo + s.H / 2) % s.H;
+        pl.geoms.push_back(g);
+        pl.ldU = std::max(pl.ldU, g.rspan);
+        pl.sbox = std::max(pl.sbox, (size_t)g.rspan * g.cspan);
+    }
+    // keep a group's field + residual (12 B/px) within ~96 MiB so they stay in L2
+    const size_t per = s.plane * 12;
+    pl.group = (int)std::max<size_t>(1, std::min<size_t>(s.B, (96u << 20) / per));
+    int parts = 0;
+    for (int l0 = 0; l0 < s.B; l0 += pl.group) parts += lr_blocks(s.h, std::min(pl.group, s.B - l0));
+    pl.parts = parts;
+    return pl;
+}
+
+size_t solve_bytes(const fpm_problem *p, const Shape &s, const Plan &pl, bool host, bool spec) {
     size_t b = 0;
-    b += s.big * 8 * 3;          // O, S, G
-    b += s.big * 4;              // m1
-    b += s.plane * (8 * 3 + 4 * 2);  // P, dP, spare, m2, P0
-    b += s.plane * 8 * 2 * nb_max;   // T1, T2
+    b += s.big * 8 + s.big * 4;                       // O, m1
+    b += (size_t)s.H * pl.ldU * 8 * 2;                // U, V
+    b += pl.sbox * 8;                                 // Sbox
+    b += s.plane * 8 * s.B;                           // Xs
+    b += s.plane * 12 * pl.group;                     // T1, Rs
+    b += s.plane * (8 * 3 + 4 * 2);                   // P, dP, m2, P0
+    if (spec) b += s.big * 8;                         // spectrum / gradient staging
     if (host) b += s.plane * s.L * (p->stack_type == FPM_STACK_U16_COUNTS ? 2 : 4);
     return b;
 }
 
-// One mini-batch: gradients at the current (O, P) of LEDs [cur, cur+nb).
-// Leaves g = IFFT2(G) in ctx->G and dP in ctx->dP; adds the loss to *loss_slot.
-fpm_status run_batch(fpm_context *ctx, const Shape &s, const Inputs &in, float2 *O,
-                     const float2 *P, int cur, int nb, double *loss_slot) {
+fpm_status alloc_pipeline(fpm_context *ctx, const fpm_problem *p, const Shape &s, const Plan &pl,
+                          bool spec) {
+    const size_t need = solve_bytes(p, s, pl, p->memory == FPM_MEM_HOST, spec);
+    if (ctx->mem_limit && need > ctx->mem_limit)
+        return fail(ctx, FPM_ERR_OUT_OF_MEMORY,
+                    "solve needs %zu bytes of device memory, limit is %zu", need,
+                    ctx->mem_limit);
+    FPM_CK(ctx->U.ensure((size_t)s.H * pl.ldU * 8));
+    FPM_CK(ctx->V.ensure((size_t)s.H * pl.ldU * 8));
+    FPM_CK(ctx->Sbox.ensure(pl.sbox * 8));
+    FPM_CK(ctx->Xs.ensure(s.plane * 8 * s.B));
+    FPM_CK(ctx->T1.ensure(s.plane * 8 * pl.group));
+    FPM_CK(ctx->Rs.ensure(s.plane * 4 * pl.group));
+    FPM_CK(ctx->dP.ensure(s.plane * 8));
+    FPM_CK(ctx->parts.ensure(sizeof(double) * (size_t)std::max(pl.parts, 1)));
+    return FPM_OK;
+}
+
+fpm_status twiddles_of(fpm_context *ctx, const Shape &s, Twiddles &tw) {
+    FPM_CK(ctx->fft.tables(s.h, &tw.lo_hi, &tw.lo_lo));
+    FPM_CK(ctx->fft.tables(s.H, &tw.hi_hi, &tw.hi_lo));
+    return FPM_OK;
+}
+
+BatchBufs bufs_of(fpm_context *ctx) {
+    BatchBufs b;
+    b.Sbox = ctx->Sbox.as<float2>();
+    b.T1 = ctx->T1.as<float2>();
+    b.Rs = ctx->Rs.as<float>();
+    b.Xs = ctx->Xs.as<float2>();
+    b.parts = ctx->parts.as<double>();
+    return b;
+}
+
+// S inside the first batch's box, from the object: column forward FFT pass, row pass.
+fpm_status spectrum_box(fpm_context *ctx, const Plan &pl, const Twiddles &tw, float2 *O,
+                        const BatchGeom &g) {
+    ColsArgs a;
+    a.mode = kColsForward;
+    a.H = g.H;
+    a.O = O;
+    a.V = ctx->V.as<float2>();
+    a.ldV = pl.ldU;
+    a.Ru0n = g.Ru0;
+    a.rspan_n = g.rspan;
+    FPM_STAGE(ST_COLS_FORWARD, launch_big_cols(a, tw, ctx->stream));
+    FPM_STAGE(ST_ROWS_FORWARD, launch_big_rows_fwd(g.H, ctx->V.as<float2>(), pl.ldU, g.rspan,
+                                                   g.Cu0, g.cspan, ctx->Sbox.as<float2>(), tw,
+                                                   ctx->stream));
+    return FPM_OK;
+}
+
+// Low-resolution passes of one batch (Xs, loss, pupil gradient) and pass A (U).
+fpm_status lowres_and_stitch(fpm_context *ctx, const Plan &pl, const Twiddles &tw,
+                             const Inputs &in, const float2 *P, const BatchGeom &g,
+                             double *loss_slot) {
     cudaStream_t st = ctx->stream;
-    float2 *S = ctx->S.as<float2>();
-    float2 *G = ctx->G.as<float2>();
-    float2 *T1 = ctx->T1.as<float2>();
-    float2 *T2 = ctx->T2.as<float2>();
-    FPM_STAGE(ST_FFT_LARGE_FWD, ctx->fft.run(O, S, s.H, 1, kForward, st));               // K1
-    FPM_STAGE(ST_CROP, launch_crop_pupil(S, P, in.led, cur, nb, s.h, s.H, T1, st));     // K2
-    FPM_STAGE(ST_FFT_BATCH_INV, ctx->fft.run(T1, T1, s.h, nb, kInverse, st));           // K3
-    FPM_STAGE(ST_FEATURE, launch_feature_grad(T1, in.Y, cur, nb, s.h, s.pratio, T2,      // K4
-                                              ctx->parts.as<double>(), st));
-    FPM_STAGE(ST_LOSS, launch_loss_accumulate(ctx->parts.as<double>(),
-                                              nb * feature_grad_blocks_per_image(s.h),
-                                              loss_slot, st));
-    FPM_STAGE(ST_FFT_BATCH_FWD, ctx->fft.run(T2, T1, s.h, nb, kForward, st));           // K5
-    const Box box = batch_box(in.led_host, cur, nb, s.h, s.H);
-    FPM_STAGE(ST_STITCH, launch_stitch_gather(T1, P, in.led, cur, nb, s.h, s.H, box, G, st));
-    FPM_STAGE(ST_PUPIL_GRAD,
-              launch_pupil_grad(S, T1, in.led, cur, nb, s.h, s.H, ctx->dP.as<float2>(), st));
-    FPM_STAGE(ST_FFT_LARGE_INV, ctx->fft.run(G, G, s.H, 1, kInverse, st));              // K8
+    BatchBufs b = bufs_of(ctx);
+    int part_off = 0;
+    for (int l0 = 0; l0 < g.nb; l0 += pl.group) {
+        const int nl = std::min(pl.group, g.nb - l0);
+        FPM_STAGE(ST_LR_COLS_INV, launch_lr_cols_inv(g, in.led, P, b, l0, nl, tw, st));
+        FPM_STAGE(ST_LR_ROWS_INV, launch_lr_rows_inv(g, in.Y, b, l0, nl, tw, st));
+        FPM_STAGE(ST_LR_ROWS_FWD, launch_lr_rows_fwd(g, b, l0, nl, part_off, tw, st));
+        FPM_STAGE(ST_LR_COLS_FWD, launch_lr_cols_fwd(g, b, l0, nl, tw, st));
+        part_off += lr_blocks(g.h, nl);
+    }
+    FPM_STAGE(ST_LOSS, launch_loss_accumulate(b.parts, part_off, loss_slot, st));
+    FPM_STAGE(ST_PUPIL_GRAD, launch_lr_pupil_grad(g, in.led, b, ctx->dP.as<float2>(), st));
+    FPM_STAGE(ST_ROWS_INV, launch_big_rows_inv(g, in.led, P, b.Xs, ctx->U.as<float2>(), pl.ldU,
+                                               tw, st));
     return FPM_OK;
 }
 
@@ -374,21 +470,6 @@ fpm_status shape_of(fpm_context *ctx, const fpm_problem *p, Shape &s, bool need_
     s.B = need_batch ? std::min(p->batch, p->n_leds) : p->n_leds;
     s.plane = (size_t)s.h * s.h;
     s.big = (size_t)s.H * s.H;
-    return FPM_OK;
-}
-
-fpm_status alloc_common(fpm_context *ctx, const fpm_problem *p, const Shape &s) {
-    const size_t need = solve_bytes(p, s, s.B, p->memory == FPM_MEM_HOST);
-    if (ctx->mem_limit && need > ctx->mem_limit)
-        return fail(ctx, FPM_ERR_OUT_OF_MEMORY,
-                    "solve needs %zu bytes of device memory, limit is %zu", need,
-                    ctx->mem_limit);
-    FPM_CK(ctx->S.ensure(s.big * 8));
-    FPM_CK(ctx->G.ensure(s.big * 8));
-    FPM_CK(ctx->T1.ensure(s.plane * 8 * s.B));
-    FPM_CK(ctx->T2.ensure(s.plane * 8 * s.B));
-    FPM_CK(ctx->dP.ensure(s.plane * 8));
-    FPM_CK(ctx->parts.ensure(sizeof(double) * (size_t)s.B * feature_grad_blocks_per_image(s.h)));
     return FPM_OK;
 }
 
@@ -480,6 +561,28 @@ void fpm_destroy(fpm_context *ctx) {
     delete ctx;
 }
 
+// LED corners on the host (the crop boxes are planned from them), validated.
+static fpm_status fetch_leds(fpm_context *ctx, const fpm_problem *p, const Shape &s,
+                             std::vector<int32_t> &led) {
+    led.resize(2 * (size_t)s.L);
+    if (p->memory == FPM_MEM_HOST) {
+        std::memcpy(led.data(), p->led_idx, 2 * sizeof(int32_t) * s.L);
+    } else {
+        FPM_CK(cudaMemcpyAsync(led.data(), p->led_idx, 2 * sizeof(int32_t) * s.L,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        FPM_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return check_leds(ctx, led, s.L, s.H);
+}
+
+// out = fftshift(fft2(O)) (out may not alias O).
+static fpm_status centred_spectrum(fpm_context *ctx, const Shape &s, const float2 *O,
+                                   float2 *out) {
+    FPM_STAGE(ST_SPECTRUM, ctx->fft.run(O, out, s.H, 1, kForward, ctx->stream));
+    FPM_CK(launch_centre_in_place(out, s.H, ctx->stream));
+    return FPM_OK;
+}
+
 fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
     ctx->err.clear();
@@ -489,7 +592,8 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     if (rc != FPM_OK) return rc;
     fpm_result none{};
     if (!res) res = &none;
-    if (p->memory == FPM_MEM_DEVICE) {
+    const bool dev = p->memory == FPM_MEM_DEVICE;
+    if (dev) {
         void *outs[4] = {res->object, res->spectrum, res->pupil, res->loss};
         for (int i = 0; i < 4; ++i) {
             if (outs[i] && !is_device_ptr(outs[i], ctx->device))
@@ -500,16 +604,22 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
                             i);
         }
     }
-    rc = alloc_common(ctx, p, s);
+    std::vector<int32_t> led_host;
+    rc = fetch_leds(ctx, p, s, led_host);
+    if (rc != FPM_OK) return rc;
+    const Plan pl = make_plan(s, led_host, p->batch);
+    rc = alloc_pipeline(ctx, p, s, pl, res->spectrum != nullptr);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;
     ctx->prof.reset();
     Inputs in;
     rc = stage_inputs(ctx, p, s, in);
     if (rc != FPM_OK) return rc;
+    Twiddles tw;
+    rc = twiddles_of(ctx, s, tw);
+    if (rc != FPM_OK) return rc;
 
     // object and pupil: work in the caller's device outputs when given, else internal
-    const bool dev = p->memory == FPM_MEM_DEVICE;
     float2 *O, *P;
     if (dev && res->object) {
         O = reinterpret_cast<float2 *>(res->object);
@@ -548,15 +658,40 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     FPM_CK(ctx->loss.ensure(sizeof(double) * std::max(E, 1)));
     FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double) * std::max(E, 1), st));
 
+    const int nbatch = (int)pl.geoms.size();
+    if (E > 0) {
+        rc = spectrum_box(ctx, pl, tw, O, pl.geoms[0]);
+        if (rc != FPM_OK) return rc;
+    }
     float lr = p->lr;
     for (int ep = 0; ep < E; ++ep) {
-        for (int cur = 0; cur < s.L; cur += p->batch) {
-            const int nb = std::min(p->batch, s.L - cur);
-            rc = run_batch(ctx, s, in, O, P, cur, nb, ctx->loss.as<double>() + ep);
+        for (int bi = 0; bi < nbatch; ++bi) {
+            const BatchGeom &g = pl.geoms[bi];
+            const bool last = ep == E - 1 && bi == nbatch - 1;
+            const BatchGeom &gn = pl.geoms[(bi + 1) % nbatch];
+            rc = lowres_and_stitch(ctx, pl, tw, in, P, g, ctx->loss.as<double>() + ep);
             if (rc != FPM_OK) return rc;
-            FPM_STAGE(ST_RMS_OBJECT, launch_rmsprop_object(ctx->G.as<float2>(), O,
-                                                           ctx->m1.as<float>(), s.big, lr,
-                                                           p->beta, p->eps, st));
+            ColsArgs a;
+            a.mode = kColsUpdate;
+            a.H = s.H;
+            a.U = ctx->U.as<float2>();
+            a.ldU = pl.ldU;
+            a.Ru0 = g.Ru0;
+            a.rspan = g.rspan;
+            a.O = O;
+            a.m = ctx->m1.as<float>();
+            a.lr = lr;
+            a.beta = p->beta;
+            a.eps = p->eps;
+            a.V = ctx->V.as<float2>();
+            a.ldV = pl.ldU;
+            a.Ru0n = last ? 0 : gn.Ru0;
+            a.rspan_n = last ? 0 : gn.rspan;
+            FPM_STAGE(ST_COLS_UPDATE, launch_big_cols(a, tw, st));
+            if (!last)
+                FPM_STAGE(ST_ROWS_FORWARD,
+                          launch_big_rows_fwd(s.H, ctx->V.as<float2>(), pl.ldU, gn.rspan, gn.Cu0,
+                                              gn.cspan, ctx->Sbox.as<float2>(), tw, st));
             FPM_STAGE(ST_RMS_PUPIL,
                       launch_rmsprop_pupil(ctx->dP.as<float2>(), P, ctx->m2.as<float>(), P0,
                                            (int)s.plane, lr, p->beta, p->eps, p->pupil_margin,
@@ -567,14 +702,15 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
 
     // outputs
     if (res->spectrum) {
-        FPM_CK(ctx->fft.run(O, ctx->S.as<float2>(), s.H, 1, kForward, st));
-        if (dev) {
-            FPM_CK(launch_centre_spectrum(ctx->S.as<float2>(), s.H,
-                                          reinterpret_cast<float2 *>(res->spectrum), st));
-        } else {
-            FPM_CK(launch_centre_spectrum(ctx->S.as<float2>(), s.H, ctx->G.as<float2>(), st));
-            FPM_CK(cudaMemcpyAsync(res->spectrum, ctx->G.p, s.big * 8, cudaMemcpyDeviceToHost, st));
+        float2 *dst = reinterpret_cast<float2 *>(res->spectrum);
+        if (!dev) {  // stage through a full-size device buffer
+            FPM_CK(ctx->S.ensure(s.big * 8));
+            dst = ctx->S.as<float2>();
         }
+        rc = centred_spectrum(ctx, s, O, dst);
+        if (rc != FPM_OK) return rc;
+        if (!dev)
+            FPM_CK(cudaMemcpyAsync(res->spectrum, dst, s.big * 8, cudaMemcpyDeviceToHost, st));
     }
     if (!dev && res->object)
         FPM_CK(cudaMemcpyAsync(res->object, O, s.big * 8, cudaMemcpyDeviceToHost, st));
@@ -618,12 +754,19 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
         if (!dev && !is_host_ptr(outs[i]))
             return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output %d is not host memory", i);
     }
-    rc = alloc_common(ctx, p, s);
+    std::vector<int32_t> led_host;
+    rc = fetch_leds(ctx, p, s, led_host);
+    if (rc != FPM_OK) return rc;
+    const Plan pl = make_plan(s, led_host, s.L);
+    rc = alloc_pipeline(ctx, p, s, pl, true);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;
     ctx->prof.reset();
     Inputs in;
     rc = stage_inputs(ctx, p, s, in);
+    if (rc != FPM_OK) return rc;
+    Twiddles tw;
+    rc = twiddles_of(ctx, s, tw);
     if (rc != FPM_OK) return rc;
     const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     FPM_CK(ctx->O.ensure(s.big * 8));
@@ -632,15 +775,64 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
     FPM_CK(cudaMemcpyAsync(ctx->P.p, p->pupil_init, s.plane * 8, kin, st));
     FPM_CK(ctx->loss.ensure(sizeof(double)));
     FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double), st));
-    rc = run_batch(ctx, s, in, ctx->O.as<float2>(), ctx->P.as<float2>(), 0, s.L,
-                   ctx->loss.as<double>());
+    const BatchGeom &g = pl.geoms[0];
+    rc = spectrum_box(ctx, pl, tw, ctx->O.as<float2>(), g);
     if (rc != FPM_OK) return rc;
+    rc = lowres_and_stitch(ctx, pl, tw, in, ctx->P.as<float2>(), g, ctx->loss.as<double>());
+    if (rc != FPM_OK) return rc;
+    FPM_CK(ctx->S.ensure(s.big * 8));
+    float2 *gout = dev && d_object ? reinterpret_cast<float2 *>(d_object) : ctx->S.as<float2>();
+    ColsArgs a;
+    a.mode = kColsGradient;
+    a.H = s.H;
+    a.U = ctx->U.as<float2>();
+    a.ldU = pl.ldU;
+    a.Ru0 = g.Ru0;
+    a.rspan = g.rspan;
+    a.gout = gout;
+    FPM_STAGE(ST_COLS_UPDATE, launch_big_cols(a, tw, st));
     const cudaMemcpyKind kout = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    if (d_object) FPM_CK(cudaMemcpyAsync(d_object, ctx->G.p, s.big * 8, kout, st));
+    if (d_object && !dev) FPM_CK(cudaMemcpyAsync(d_object, gout, s.big * 8, kout, st));
     if (d_pupil) FPM_CK(cudaMemcpyAsync(d_pupil, ctx->dP.p, s.plane * 8, kout, st));
     if (loss) FPM_CK(cudaMemcpyAsync(loss, ctx->loss.p, sizeof(double), kout, st));
     FPM_CK(cudaStreamSynchronize(st));
     ctx->prof.collect();
+    return FPM_OK;
+}
+
+fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, int32_t count,
+                    int32_t direction, int32_t memory) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (!in || !out || count < 1 || (direction != -1 && direction != 1))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "bad fft2 arguments");
+    if (!fft_supported(n))
+        return fail(ctx, FPM_ERR_UNSUPPORTED, "n = %d: powers of two from 16 to %d", n, kMaxFftLen);
+    if (memory != FPM_MEM_DEVICE && memory != FPM_MEM_HOST)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", memory);
+    FPM_CK(cudaSetDevice(ctx->device));
+    const bool dev = memory == FPM_MEM_DEVICE;
+    const size_t bytes = (size_t)n * n * count * 8;
+    if (dev) {
+        if (!is_device_ptr(in, ctx->device) || !is_device_ptr(out, ctx->device) ||
+            ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "in/out: 16-byte aligned device memory");
+    } else if (!is_host_ptr(in) || !is_host_ptr(out)) {
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "in/out are not host memory");
+    }
+    if (ctx->mem_limit && !dev && bytes > ctx->mem_limit)
+        return fail(ctx, FPM_ERR_OUT_OF_MEMORY, "fft2 needs %zu bytes", bytes);
+    cudaStream_t st = ctx->stream;
+    const float2 *src = reinterpret_cast<const float2 *>(in);
+    float2 *dst = reinterpret_cast<float2 *>(out);
+    if (!dev) {
+        FPM_CK(ctx->spec.ensure(bytes));
+        FPM_CK(cudaMemcpyAsync(ctx->spec.p, in, bytes, cudaMemcpyHostToDevice, st));
+        src = dst = ctx->spec.as<float2>();
+    }
+    FPM_CK(ctx->fft.run(src, dst, n, count, direction < 0 ? kForward : kInverse, st));
+    if (!dev) FPM_CK(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, st));
+    FPM_CK(cudaStreamSynchronize(st));
     return FPM_OK;
 }
 

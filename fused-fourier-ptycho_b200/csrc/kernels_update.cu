@@ -111,6 +111,32 @@ cudaError_t launch_centre_spectrum(const float2 *S, int H, float2 *out, cudaStre
     return cudaGetLastError();
 }
 
+// In-place fftshift of an H x H array (even H): swaps (r, c) with
+// ((r + H/2) mod H, (c + H/2) mod H); each pair is visited once from the c < H/2 half.
+__global__ void __launch_bounds__(256) k_centre_in_place(float2 *__restrict__ S, int H) {
+    const size_t half = (size_t)H * (H / 2);
+    const int hh = H >> 1;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < half;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(q % H);
+        const int c = (int)(q / H);
+        const int r2 = r + hh >= H ? r + hh - H : r + hh;
+        const size_t a = (size_t)c * H + r, b = (size_t)(c + hh) * H + r2;
+        const float2 t = S[a];
+        S[a] = S[b];
+        S[b] = t;
+    }
+}
+
+cudaError_t launch_centre_in_place(float2 *S, int H, cudaStream_t st) {
+    const size_t half = (size_t)H * (H / 2);
+    size_t gx = (half + 255) / 256;
+    const size_t cap = (size_t)kB200SMs * 8 * 8;
+    if (gx > cap) gx = cap;
+    k_centre_in_place<<<(unsigned)gx, 256, 0, st>>>(S, H);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Initial object: MATLAB imresize(Y_1, pratio, 'bicubic') with zero phase
 // (codes_v2/main_run_FPM.m:47-48).  Output pixel u (1-based) samples input

@@ -1,0 +1,79 @@
+// Fused per-batch pipeline: low-resolution passes L1-L4 and the pruned
+// large-array passes A, B, C (see pipeline.cu for the data flow).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "engine.h"
+
+namespace fpm {
+
+// One mini-batch's crop box.  Centred rows [rlo, rlo + rspan) and columns
+// [clo, clo + cspan), modulo H; Ru0 / Cu0 are the matching un-shifted starts.
+struct BatchGeom {
+    int H = 0, h = 0, pratio = 0;
+    int z_off = 0, nb = 0;
+    int rlo = 0, rspan = 0, clo = 0, cspan = 0;
+    int Ru0 = 0, Cu0 = 0;
+};
+
+// Two-level twiddle tables (fft_core.cuh) for the low-res length h and the large length H.
+struct Twiddles {
+    const float2 *lo_hi = nullptr, *lo_lo = nullptr;  // length h
+    const float2 *hi_hi = nullptr, *hi_lo = nullptr;  // length H
+};
+
+// Workspace of one batch.
+struct BatchBufs {
+    const float2 *Sbox = nullptr;  // [cspan][rspan] spectrum inside the box (leading dim rspan)
+    float2 *T1 = nullptr;          // [group][h][h] per-LED field (group-local pages)
+    float *Rs = nullptr;           // [group][h][h] residual |z|/(h^2 p^2) - Y
+    float2 *Xs = nullptr;          // [nb][h][h] row-major fftshift'ed gradient spectrum
+    double *parts = nullptr;       // loss partials of the batch
+};
+
+bool pipeline_supported(int h, int H);
+int lr_blocks(int h, int nl);  // CTAs of one L-pass over nl LEDs
+
+// low-resolution passes over LEDs [l0, l0 + nl) of the batch (T1 / Rs group-local)
+cudaError_t launch_lr_cols_inv(const BatchGeom &g, const int2 *led, const float2 *P, BatchBufs b,
+                               int l0, int nl, const Twiddles &tw, cudaStream_t st);
+cudaError_t launch_lr_rows_inv(const BatchGeom &g, StackView Y, BatchBufs b, int l0, int nl,
+                               const Twiddles &tw, cudaStream_t st);
+cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, int part_off,
+                               const Twiddles &tw, cudaStream_t st);
+cudaError_t launch_lr_cols_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl,
+                               const Twiddles &tw, cudaStream_t st);
+cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs b, float2 *dP,
+                                 cudaStream_t st);
+
+// Pass A: gradient spectrum rows of the box -> inverse FFT along the rows -> U [H][ldU].
+cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float2 *P,
+                                const float2 *Xs, float2 *U, int ldU, const Twiddles &tw,
+                                cudaStream_t st);
+
+enum BigColsMode : int { kColsForward = 0, kColsUpdate = 1, kColsGradient = 2 };
+// Pass B over every column c:
+//   kColsForward : V[c][i] = FFT_r(O[c])[(Ru0n + i) mod H], i < rspan_n
+//   kColsUpdate  : g = IFFT_r(U[c] placed at rows Ru0 + i); RMSprop(O, m); V from FFT_r(O')
+//                  (no V when rspan_n == 0)
+//   kColsGradient: g = IFFT_r(U[c]) written to out[c]
+struct ColsArgs {
+    int mode = kColsForward;
+    int H = 0;
+    const float2 *U = nullptr;
+    int ldU = 0, Ru0 = 0, rspan = 0;
+    float2 *O = nullptr;
+    float *m = nullptr;
+    float lr = 0.f, beta = 0.f, eps = 0.f;
+    float2 *V = nullptr;
+    int ldV = 0, Ru0n = 0, rspan_n = 0;
+    float2 *gout = nullptr;
+};
+cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t st);
+
+// Pass C: rows i < rspan_n of V -> FFT along the rows -> Sbox[j][i] = row[(Cu0n + j) mod H].
+cudaError_t launch_big_rows_fwd(int H, const float2 *V, int ldV, int rspan_n, int Cu0n,
+                                int cspan_n, float2 *Sbox, const Twiddles &tw, cudaStream_t st);
+
+}  // namespace fpm

@@ -23,9 +23,9 @@ CLI = LIBDIR / "fpm_cli"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(INCLUDE),
                   "--expt-relaxed-constexpr"]
-LIBS_SOURCES = ["kernels_lowres.cu", "kernels_update.cu", "fft_cufft.cu", "fpm_api.cpp",
-                "noalloc.cu"]
-LINK_LIBS = ["-lcufft", "-lcudart"]
+LIBS_SOURCES = ["kernels_lowres.cu", "kernels_update.cu", "fft_own.cu", "fpm_api.cpp",
+                "noalloc.cu", "pipeline.cu"]
+LINK_LIBS = ["-lcudart"]
 
 
 def nvcc() -> str:

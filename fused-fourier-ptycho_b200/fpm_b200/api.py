@@ -36,7 +36,7 @@ LOSS_ANISOTROPIC = 0
 # Every symbol include/fpm.h declares.
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
-            "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc"]
+            "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2"]
 
 
 class FpmError(RuntimeError):
@@ -103,6 +103,9 @@ def load_library(path: str | Path | None = None):
     lib.fpm_set_profiling.restype = C.c_int
     lib.fpm_stage_times.argtypes = [C.c_void_p, C.POINTER(StageTime), C.c_int32]
     lib.fpm_stage_times.restype = C.c_int32
+    lib.fpm_fft2.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                             C.c_int32]
+    lib.fpm_fft2.restype = C.c_int
     lib.fpm_abi_version.argtypes = []
     lib.fpm_abi_version.restype = C.c_int32
     if path is None:
@@ -258,6 +261,25 @@ class Engine:
         self._check(self.gradients_raw(prob, op, pp, lp))
         del keep
         return o, p, float(loss[0])
+
+    def fft2(self, x, direction=-1):
+        """Unnormalised 2-D FFT of a MATLAB-order (n, n) or (n, n, count) complex64 array."""
+        if _is_torch(x):
+            import torch
+            y = x.permute(*reversed(range(x.dim()))).contiguous()
+            out = torch.empty_like(y)
+            n = int(x.shape[0])
+            cnt = int(x.shape[2]) if x.dim() == 3 else 1
+            self._check(self.lib.fpm_fft2(self._ctx, y.data_ptr(), out.data_ptr(), n, cnt,
+                                          direction, MEM_DEVICE if y.is_cuda else MEM_HOST))
+            return out.permute(*reversed(range(x.dim())))
+        a = np.asfortranarray(np.asarray(x, np.complex64))
+        out = np.empty_like(a, order="F")
+        n = a.shape[0]
+        cnt = a.shape[2] if a.ndim == 3 else 1
+        self._check(self.lib.fpm_fft2(self._ctx, a.ctypes.data, out.ctypes.data, n, cnt,
+                                      direction, MEM_HOST))
+        return out
 
     def normalise_stack(self, counts):
         """Amplitude sqrt((I-min)/(max-min)) of a uint16 stack, same shape, float32."""

@@ -22,7 +22,8 @@
  *     spectrum (MATLAB int32([kl; kt]), codes_v2/main_run_FPM.m:53-55).  A
  *     crop that runs past the spectrum edge wraps modulo H, as in v3
  *     (cuFPM_v3/cuda/kernels.cuh:43-47).  1 <= kl, kt <= H is required.
- *   - h must be even and H = h * pratio.  The caller owns every buffer.
+ *   - h and H = h * pratio must be powers of two from 16 to 16384 in this build
+ *     (FPM_ERR_UNSUPPORTED otherwise).  The caller owns every buffer.
  *   - Every function returns an fpm_status; nothing throws across the ABI.
  *   - A context is bound to one CUDA device and is not thread-safe: use one
  *     context per host thread.
@@ -144,6 +145,13 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *prob,
    precision.  Pointers follow `memory`. */
 fpm_status fpm_normalise_stack(fpm_context *ctx, const uint16_t *counts, size_t n,
                                float *amplitude, int32_t memory);
+
+/* The engine's own unnormalised 2-D FFT of `count` column-major n x n complex
+   pages (direction -1 forward, +1 inverse), the transform behind the cuFFT calls
+   of cuFPM_pure_v3.cu:135-187.  n: power of two, 16 <= n <= 16384.  in may equal
+   out.  Pointers follow `memory`. */
+fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, int32_t count,
+                    int32_t direction, int32_t memory);
 
 /* Loss-gradient stage that allocates nothing.  No counterpart in the reference.
    For callers that cannot call cudaMalloc (a mex inside MATLAB's GPU memory

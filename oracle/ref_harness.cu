@@ -40,13 +40,17 @@ struct Bufs {
 extern "C" {
 
 // Full solve (cuFPM_pure_v3 semantics).  Host arrays in, host arrays out,
-// column-major.  ms[0] = epoch-loop time, ms[1] = allocation + plans + loop.
+// column-major.  ms[0] = epoch-loop time, ms[1] = allocation + plans + loop,
+// ms[2] = number of guard bytes after the object buffer that changed (the
+// object is allocated with a 64 KiB sentinel-filled guard behind it).
 int ref_solve(int h, int H, int L, int pratio, int epochs, int batch, float lr, float beta,
               float eps, const float *O0, const float *P0c, const float *Y, const int *led,
               const float *P0, float *O_out, float *P_out, float *ms) {
     Bufs b;
     const size_t plane = (size_t)h * h, big = (size_t)H * H;
-    RCK(cudaMalloc(&b.O, big * 8));
+    const size_t guard = 64 * 1024;
+    RCK(cudaMalloc(&b.O, big * 8 + guard));
+    RCK(cudaMemset(reinterpret_cast<char *>(b.O) + big * 8, 0xA5, guard));
     RCK(cudaMalloc(&b.P, plane * 8));
     RCK(cudaMalloc(&b.Y, plane * L * 4));
     RCK(cudaMalloc(&b.P0, plane * 4));
@@ -130,6 +134,12 @@ int ref_solve(int h, int H, int L, int pratio, int epochs, int batch, float lr, 
     if (ms) {
         ms[0] = t_loop;
         ms[1] = t_all;
+        unsigned char *g = new unsigned char[guard];
+        cudaMemcpy(g, reinterpret_cast<char *>(b.O) + big * 8, guard, cudaMemcpyDeviceToHost);
+        int changed = 0;
+        for (size_t i = 0; i < guard; ++i) changed += g[i] != 0xA5;
+        delete[] g;
+        ms[2] = (float)changed;
     }
     int rc = (int)cudaGetLastError();
     if (rc == 0) {

@@ -75,7 +75,7 @@ def ref_solve(lib, O0, P0c, Y, led, P0, pratio, epochs, batch, opt):
     L = Y.shape[0]
     O = np.empty((H, H), np.complex64, order="F")
     P = np.empty((h, h), np.complex64, order="F")
-    ms = np.zeros(2, np.float32)
+    ms = np.zeros(3, np.float32)
     rc = lib.ref_solve(h, H, L, pratio, epochs, batch, opt[0], opt[1], opt[2],
                        _colmajor(O0, np.complex64).ctypes.data, _colmajor(P0c, np.complex64).ctypes.data,
                        _stack(Y).ctypes.data, np.ascontiguousarray(led, np.int32).ctypes.data,
