@@ -159,11 +159,11 @@ def stage_bytes(cfg: Cfg, led):
     H2, h2 = H * H, h * h
     boxes = batch_boxes(led, h, H, cfg.batch)
     nbatch = len(boxes)
-    group = max(1, min(cfg.batch, (96 << 20) // (h2 * 12)))
+    group = max(1, min(cfg.batch, (4 << 30) // (h2 * 12)))
     lr_launches = sum(math.ceil(nb / group) for nb, _, _ in boxes)
     tot = {k: 0.0 for k in ("lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
                             "lr_cols_forward", "pupil_grad", "rows_inverse_stitch",
-                            "cols_update", "rows_forward", "rmsprop_pupil")}
+                            "cols_update", "rows_forward", "rmsprop_pupil", "transpose")}
     for bi, (nb, rspan, cspan) in enumerate(boxes):
         _, rn, cn = boxes[(bi + 1) % nbatch]
         px = h2 * nb
@@ -176,9 +176,11 @@ def stage_bytes(cfg: Cfg, led):
         tot["cols_update"] += 8 * H * rspan + 24 * H2 + 8 * H * rn
         tot["rows_forward"] += 8 * H * rn + 8 * rn * cn
         tot["rmsprop_pupil"] += 36 * h2
+        # four transposes per batch: pupil, stitch rows, next-box rows, next-box spectrum
+        tot["transpose"] += 16 * (h2 + H * rspan + H * rn + rn * cn)
     per = {}
     for k, v in tot.items():
-        n = lr_launches if k.startswith("lr_") else nbatch
+        n = lr_launches if k.startswith("lr_") else (4 * nbatch if k == "transpose" else nbatch)
         per[k] = v / n
     nb0, r0, c0 = boxes[0]
     per["cols_forward"] = 8 * H2 + 8 * H * r0

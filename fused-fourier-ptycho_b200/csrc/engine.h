@@ -42,6 +42,9 @@ cudaError_t launch_rmsprop_pupil(const float2 *dP, float2 *P, float *m, const fl
                                  float lr, float beta, float eps, float am, cudaStream_t st);
 cudaError_t launch_centre_spectrum(const float2 *S, int H, float2 *out, cudaStream_t st);
 cudaError_t launch_centre_in_place(float2 *S, int H, cudaStream_t st);
+// out[c*ldo + r] = in[r*ldi + c] (r < rows, c < cols); conj_scale != 0 conjugates and scales.
+cudaError_t launch_transpose(const float2 *in, size_t ldi, float2 *out, size_t ldo, int rows,
+                             int cols, float conj_scale, cudaStream_t st);
 cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, cudaStream_t st);
 
 // ---- reductions and ingest ------------------------------------------------

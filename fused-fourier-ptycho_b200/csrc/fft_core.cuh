@@ -164,6 +164,71 @@ __device__ __forceinline__ void line_fft(float2 *s, const float2 *hi, const floa
     stages<N, DIR, 1>(s, hi, lo, t);
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident variant.  Thread t of a line owns the 16 elements
+// t + m*(N/16), m = 0..15, in v[m] ("canonical" layout) on entry and on exit.
+// For any radix R the butterfly j of a first stage (p = 1) reads exactly these
+// positions (i + r N/R = t + (j + r*16/R) N/16), and a last stage (p = N/R)
+// writes them, so the first stage takes its inputs from registers and the last
+// stage leaves its outputs in registers; only the exchanges between stages go
+// through shared memory (N values at s, swizzled).  Callers load v straight
+// from global memory (16 independent loads per thread) and store it back, or
+// hand it to the next computation without a shared-memory round trip.
+// ---------------------------------------------------------------------------
+template <int N, int DIR, int P>
+__device__ __forceinline__ void stages_regs(float2 (&v)[16], float2 *s, const float2 *hi,
+                                            const float2 *lo, int t) {
+    constexpr int REM = N / P;
+    constexpr int R = REM >= 16 ? 16 : REM;
+    constexpr int T = N / 16;
+    constexpr int NB = 16 / R;
+    constexpr bool FIRST = P == 1;
+    constexpr bool LAST = P * R == N;
+    if constexpr (!FIRST) {
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[j + r * NB] = s[swz(t + j * T + r * (N / R))];
+    }
+    if constexpr (!LAST) __syncthreads();   // every read of s done before it is rewritten
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        float2 u[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) u[r] = v[j + r * NB];
+        const int i = t + j * T;
+        const int k = i & (P - 1);
+        if constexpr (P > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r)
+                u[r] = cmulf(u[r], twiddle<DIR>(hi, lo, r * k * (N / (P * R))));
+        }
+        dft<R, DIR>(u);
+        if constexpr (LAST) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[j + r * NB] = u[r];
+        } else {
+            const int base = (i - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[swz(base + r * P)] = u[r];
+        }
+    }
+    if constexpr (!LAST) {
+        __syncthreads();
+        stages_regs<N, DIR, P * R>(v, s, hi, lo, t);
+    }
+}
+
+// Unnormalised DFT of a line held in canonical registers (see above).  Must be
+// reached by every thread of the block when N > 16 (it synchronises); the
+// shared-memory line s must not be in use by other threads on entry.
+template <int N, int DIR>
+__device__ __forceinline__ void line_fft_regs(float2 (&v)[16], float2 *s, const float2 *hi,
+                                              const float2 *lo, int t) {
+    static_assert(N >= 16 && (N & (N - 1)) == 0, "power-of-two length >= 16");
+    stages_regs<N, DIR, 1>(v, s, hi, lo, t);
+}
+
 // Copies the two-level twiddle table of length N into shared memory.
 // hi needs max(1, N/128) entries, lo min(N, 128).
 __device__ __forceinline__ void load_twiddles(float2 *s_hi, float2 *s_lo, const float2 *g_hi,
@@ -183,6 +248,29 @@ struct Geo {
     static constexpr int TW_BYTES = 2 * 128 * 8;
     static constexpr int NHI = N >= 128 ? N / 128 : 1;
     static constexpr int NLO = N >= 128 ? 128 : N;
+};
+
+// CTA shape for the register-resident kernels: LPC lines of length N per CTA,
+// T = N/16 threads per line, lines padded in shared memory by PAD values so that
+// the LPC lines of an interleaved warp fall on different banks.
+template <int N>
+struct LG {
+    static constexpr int T = N / 16;
+    static constexpr int LPC = (N * 8 >= 64 * 1024) ? 1 : (64 * 1024) / (N * 8);
+    static constexpr int THREADS = T * LPC;
+    static constexpr int MINB = THREADS <= 512 ? 2 : 1;      // 64 registers per thread
+    static constexpr int PAD = LPC == 1 ? 0 : (16 / LPC > 0 ? 16 / LPC : 1);
+    static constexpr int STRIDE = N + PAD;
+    static constexpr int SMEM = LPC * STRIDE * 8 + 2 * 128 * 8;
+    static constexpr int NHI = N >= 128 ? N / 128 : 1;
+    static constexpr int NLO = N >= 128 ? 128 : N;
+    // contiguous mapping: a warp walks one line
+    __device__ static int cline() { return threadIdx.x / T; }
+    __device__ static int ct() { return threadIdx.x % T; }
+    // interleaved mapping: a warp spans the LPC lines, LPC consecutive lines per element
+    __device__ static int iline() { return threadIdx.x % LPC; }
+    __device__ static int it() { return threadIdx.x / LPC; }
+    __device__ static float2 *tw_hi(float2 *smem) { return smem + LPC * STRIDE; }
 };
 
 }  // namespace fft

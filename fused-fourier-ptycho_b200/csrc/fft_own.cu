@@ -10,90 +10,75 @@ namespace fpm {
 namespace {
 
 template <int N>
-struct Geo : fft::Geo<N> {
-    static constexpr int SMEM = fft::Geo<N>::LINE_BYTES + fft::Geo<N>::TW_BYTES;
-};
+using LG = fft::LG<N>;
+
+template <class K>
+cudaError_t set_smem(K kernel, int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
+}
 
 // Lines along the contiguous axis: line L (over all pages) = elements [L*N, (L+1)*N).
 template <int N, int DIR>
-__global__ void __launch_bounds__(Geo<N>::THREADS) k_fft_contig(const float2 *__restrict__ in,
-                                                                 float2 *__restrict__ out,
-                                                                 long long n_lines,
-                                                                 const float2 *__restrict__ g_hi,
-                                                                 const float2 *__restrict__ g_lo) {
-    using G = Geo<N>;
+__global__ void __launch_bounds__(LG<N>::THREADS, LG<N>::MINB)
+    k_fft_contig(const float2 *__restrict__ in, float2 *__restrict__ out, long long n_lines,
+                 const float2 *__restrict__ g_hi, const float2 *__restrict__ g_lo) {
+    using G = LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    fft::load_twiddles(s_hi, s_lo, g_hi, g_lo, G::NHI, G::NLO);
-    const int line = threadIdx.x / G::T;
-    const int t = threadIdx.x % G::T;
-    const long long L = (long long)blockIdx.x * G::LPC + line;
-    float2 *s = smem + line * N;
-    const bool live = L < n_lines;
-    if (live) {
-        const float2 *src = in + L * N;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) s[fft::swz(t + j * G::T)] = src[t + j * G::T];
-    }
+    float2 *s_hi = G::tw_hi(smem);
+    fft::load_twiddles(s_hi, s_hi + 128, g_hi, g_lo, G::NHI, G::NLO);
     __syncthreads();
-    fft::line_fft<N, DIR>(s, s_hi, s_lo, t);
-    if (live) {
-        float2 *dst = out + L * N;
+    const int ln = G::cline(), t = G::ct();
+    const long long L = (long long)blockIdx.x * G::LPC + ln;
+    const bool live = L < n_lines;
+    const float2 *src = in + (size_t)(live ? L : 0) * N;
+    float2 v[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) dst[t + j * G::T] = s[fft::swz(t + j * G::T)];
+    for (int m = 0; m < 16; ++m) v[m] = live ? src[t + m * G::T] : make_float2(0.f, 0.f);
+    fft::line_fft_regs<N, DIR>(v, smem + ln * G::STRIDE, s_hi, s_hi + 128, t);
+    if (live) {
+        float2 *dst = out + (size_t)L * N;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) dst[t + m * G::T] = v[m];
     }
 }
 
-// Lines along the strided axis: line (p, r) = elements p*N*N + c*N + r, c = 0..N-1.
-// Lines are numbered g = p*N + r; a CTA takes LPC consecutive g (consecutive r of
-// one page when LPC <= N, whole pages when LPC > N), so each c contributes LPC*8
-// contiguous bytes per page.
+// Lines along the strided axis: line (p, r) = elements p*N*N + c*N + r, c = 0..N-1,
+// numbered g = p*N + r; a CTA takes LPC consecutive g with its warps interleaved
+// over them, so each c contributes LPC*8 contiguous bytes.
 template <int N, int DIR>
-__global__ void __launch_bounds__(Geo<N>::THREADS) k_fft_strided(const float2 *__restrict__ in,
-                                                                  float2 *__restrict__ out,
-                                                                  long long n_lines,
-                                                                  const float2 *__restrict__ g_hi,
-                                                                  const float2 *__restrict__ g_lo) {
-    using G = Geo<N>;
+__global__ void __launch_bounds__(LG<N>::THREADS, LG<N>::MINB)
+    k_fft_strided(const float2 *__restrict__ in, float2 *__restrict__ out, long long n_lines,
+                  const float2 *__restrict__ g_hi, const float2 *__restrict__ g_lo) {
+    using G = LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    fft::load_twiddles(s_hi, s_lo, g_hi, g_lo, G::NHI, G::NLO);
-    const long long g0 = (long long)blockIdx.x * G::LPC;
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int line = q % G::LPC;
-        const int c = q / G::LPC;
-        const long long g = g0 + line;
-        if (g < n_lines) {
-            const size_t addr = (size_t)(g / N) * N * N + (size_t)c * N + (size_t)(g % N);
-            smem[line * N + fft::swz(c)] = in[addr];
-        }
-    }
+    float2 *s_hi = G::tw_hi(smem);
+    fft::load_twiddles(s_hi, s_hi + 128, g_hi, g_lo, G::NHI, G::NLO);
     __syncthreads();
-    const int line = threadIdx.x / G::T;
-    fft::line_fft<N, DIR>(smem + line * N, s_hi, s_lo, threadIdx.x % G::T);
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int l2 = q % G::LPC;
-        const int c = q / G::LPC;
-        const long long g = g0 + l2;
-        if (g < n_lines) {
-            const size_t addr = (size_t)(g / N) * N * N + (size_t)c * N + (size_t)(g % N);
-            out[addr] = smem[l2 * N + fft::swz(c)];
-        }
+    const int ln = G::iline(), t = G::it();
+    const long long g = (long long)blockIdx.x * G::LPC + ln;
+    const bool live = g < n_lines;
+    const size_t base = live ? (size_t)(g / N) * N * N + (size_t)(g % N) : 0;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m)
+        v[m] = live ? in[base + (size_t)(t + m * G::T) * N] : make_float2(0.f, 0.f);
+    fft::line_fft_regs<N, DIR>(v, smem + ln * G::STRIDE, s_hi, s_hi + 128, t);
+    if (live) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) out[base + (size_t)(t + m * G::T) * N] = v[m];
     }
 }
 
 template <int N, int DIR>
 cudaError_t run_n(const float2 *in, float2 *out, int count, const float2 *hi, const float2 *lo,
                   cudaStream_t st) {
-    using G = Geo<N>;
-    // per device and cheap: set on every call rather than cached
-    cudaError_t e = cudaFuncSetAttribute(k_fft_contig<N, DIR>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    using G = LG<N>;
+    cudaError_t e = set_smem(k_fft_contig<N, DIR>, G::SMEM);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_fft_strided<N, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             G::SMEM);
+    e = set_smem(k_fft_strided<N, DIR>, G::SMEM);
     if (e != cudaSuccess) return e;
     const long long lines = (long long)count * N;
     const long long blocks = (lines + G::LPC - 1) / G::LPC;

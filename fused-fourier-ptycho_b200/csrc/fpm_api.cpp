@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstdint>
 #include <cstring>
@@ -75,13 +76,13 @@ namespace {
 enum Stage : int {
     ST_COLS_FORWARD, ST_ROWS_FORWARD, ST_LR_COLS_INV, ST_LR_ROWS_INV, ST_LR_ROWS_FWD,
     ST_LR_COLS_FWD, ST_LOSS, ST_PUPIL_GRAD, ST_ROWS_INV, ST_COLS_UPDATE, ST_RMS_PUPIL,
-    ST_SPECTRUM, ST_COUNT
+    ST_SPECTRUM, ST_TRANSPOSE, ST_COUNT
 };
 const char *const kStageName[ST_COUNT] = {
     "cols_forward", "rows_forward", "lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
     "lr_cols_forward", "loss_reduce", "pupil_grad", "rows_inverse_stitch", "cols_update",
-    "rmsprop_pupil", "spectrum_fft2"};
-const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    "rmsprop_pupil", "spectrum_fft2", "transpose"};
+const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
 
 struct Profiler {
     bool on = false;
@@ -151,7 +152,8 @@ struct fpm_context {
     std::string err;
     FftEngine fft;
     // work buffers, kept between calls
-    DevBuf O, m1, S, P, m2, P0, dP, T1, Rs, Xs, Sbox, U, V, Y, led, parts, loss, minmax, spec;
+    DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
+        minmax, spec;
 };
 
 namespace {
@@ -364,9 +366,15 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch) {
         pl.ldU = std::max(pl.ldU, g.rspan);
         pl.sbox = std::max(pl.sbox, (size_t)g.rspan * g.cspan);
     }
-    // keep a group's field + residual (12 B/px) within ~96 MiB so they stay in L2
+    // LEDs per low-resolution launch: the whole batch (measured fastest: large
+    // grids, no tails; the field + residual of 26 LEDs of 2048^2 take 1.3 GB), capped
+    // at 4 GiB of field + residual; FPM_LR_GROUP overrides it (tuning).
     const size_t per = s.plane * 12;
-    pl.group = (int)std::max<size_t>(1, std::min<size_t>(s.B, (96u << 20) / per));
+    pl.group = (int)std::max<size_t>(1, std::min<size_t>(s.B, (4ull << 30) / per));
+    if (const char *env = std::getenv("FPM_LR_GROUP")) {
+        const int v = std::atoi(env);
+        if (v > 0) pl.group = std::min(v, s.B);
+    }
     int parts = 0;
     for (int l0 = 0; l0 < s.B; l0 += pl.group) parts += lr_blocks(s.h, std::min(pl.group, s.B - l0));
     pl.parts = parts;
@@ -376,11 +384,11 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch) {
 size_t solve_bytes(const fpm_problem *p, const Shape &s, const Plan &pl, bool host, bool spec) {
     size_t b = 0;
     b += s.big * 8 + s.big * 4;                       // O, m1
-    b += (size_t)s.H * pl.ldU * 8 * 2;                // U, V
-    b += pl.sbox * 8;                                 // Sbox
+    b += (size_t)s.H * pl.ldU * 8 * 3;                // U, V and their row-major twin
+    b += pl.sbox * 8 * 2;                             // Sbox and its row-major twin
     b += s.plane * 8 * s.B;                           // Xs
     b += s.plane * 12 * pl.group;                     // T1, Rs
-    b += s.plane * (8 * 3 + 4 * 2);                   // P, dP, m2, P0
+    b += s.plane * (8 * 4 + 4 * 2);                   // P, dP, Pt, m2, P0
     if (spec) b += s.big * 8;                         // spectrum / gradient staging
     if (host) b += s.plane * s.L * (p->stack_type == FPM_STACK_U16_COUNTS ? 2 : 4);
     return b;
@@ -395,7 +403,10 @@ fpm_status alloc_pipeline(fpm_context *ctx, const fpm_problem *p, const Shape &s
                     ctx->mem_limit);
     FPM_CK(ctx->U.ensure((size_t)s.H * pl.ldU * 8));
     FPM_CK(ctx->V.ensure((size_t)s.H * pl.ldU * 8));
+    FPM_CK(ctx->W.ensure((size_t)s.H * pl.ldU * 8));
     FPM_CK(ctx->Sbox.ensure(pl.sbox * 8));
+    FPM_CK(ctx->Sboxr.ensure(pl.sbox * 8));
+    FPM_CK(ctx->Pt.ensure(s.plane * 8));
     FPM_CK(ctx->Xs.ensure(s.plane * 8 * s.B));
     FPM_CK(ctx->T1.ensure(s.plane * 8 * pl.group));
     FPM_CK(ctx->Rs.ensure(s.plane * 4 * pl.group));
@@ -420,6 +431,22 @@ BatchBufs bufs_of(fpm_context *ctx) {
     return b;
 }
 
+// Row pass of the next box: V (column-major) -> Vr (row-major, in W) -> row FFTs ->
+// Sboxr (row-major) -> Sbox (column-major), every access coalesced.
+fpm_status rows_forward(fpm_context *ctx, const Plan &pl, const Twiddles &tw,
+                        const BatchGeom &gn) {
+    cudaStream_t st = ctx->stream;
+    float2 *W = ctx->W.as<float2>();
+    FPM_STAGE(ST_TRANSPOSE, launch_transpose(ctx->V.as<float2>(), pl.ldU, W, gn.H, gn.H, gn.rspan,
+                                             0.f, st));
+    FPM_STAGE(ST_ROWS_FORWARD, launch_big_rows_fwd(gn.H, W, gn.rspan, gn.Cu0, gn.cspan,
+                                                   ctx->Sboxr.as<float2>(), tw, st));
+    FPM_STAGE(ST_TRANSPOSE, launch_transpose(ctx->Sboxr.as<float2>(), gn.cspan,
+                                             ctx->Sbox.as<float2>(), gn.rspan, gn.rspan, gn.cspan,
+                                             0.f, st));
+    return FPM_OK;
+}
+
 // S inside the first batch's box, from the object: column forward FFT pass, row pass.
 fpm_status spectrum_box(fpm_context *ctx, const Plan &pl, const Twiddles &tw, float2 *O,
                         const BatchGeom &g) {
@@ -432,10 +459,7 @@ fpm_status spectrum_box(fpm_context *ctx, const Plan &pl, const Twiddles &tw, fl
     a.Ru0n = g.Ru0;
     a.rspan_n = g.rspan;
     FPM_STAGE(ST_COLS_FORWARD, launch_big_cols(a, tw, ctx->stream));
-    FPM_STAGE(ST_ROWS_FORWARD, launch_big_rows_fwd(g.H, ctx->V.as<float2>(), pl.ldU, g.rspan,
-                                                   g.Cu0, g.cspan, ctx->Sbox.as<float2>(), tw,
-                                                   ctx->stream));
-    return FPM_OK;
+    return rows_forward(ctx, pl, tw, g);
 }
 
 // Low-resolution passes of one batch (Xs, loss, pupil gradient) and pass A (U).
@@ -455,8 +479,13 @@ fpm_status lowres_and_stitch(fpm_context *ctx, const Plan &pl, const Twiddles &t
     }
     FPM_STAGE(ST_LOSS, launch_loss_accumulate(b.parts, part_off, loss_slot, st));
     FPM_STAGE(ST_PUPIL_GRAD, launch_lr_pupil_grad(g, in.led, b, ctx->dP.as<float2>(), st));
-    FPM_STAGE(ST_ROWS_INV, launch_big_rows_inv(g, in.led, P, b.Xs, ctx->U.as<float2>(), pl.ldU,
-                                               tw, st));
+    // conj(P) / H^2, row-major, for coalesced pupil reads in the stitch
+    FPM_STAGE(ST_TRANSPOSE, launch_transpose(P, g.h, ctx->Pt.as<float2>(), g.h, g.h, g.h,
+                                             (float)(1.0 / ((double)g.H * g.H)), st));
+    float2 *W = ctx->W.as<float2>();
+    FPM_STAGE(ST_ROWS_INV, launch_big_rows_inv(g, in.led, ctx->Pt.as<float2>(), b.Xs, W, tw, st));
+    FPM_STAGE(ST_TRANSPOSE, launch_transpose(W, g.H, ctx->U.as<float2>(), pl.ldU, g.rspan, g.H,
+                                             0.f, st));
     return FPM_OK;
 }
 
@@ -688,10 +717,10 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
             a.Ru0n = last ? 0 : gn.Ru0;
             a.rspan_n = last ? 0 : gn.rspan;
             FPM_STAGE(ST_COLS_UPDATE, launch_big_cols(a, tw, st));
-            if (!last)
-                FPM_STAGE(ST_ROWS_FORWARD,
-                          launch_big_rows_fwd(s.H, ctx->V.as<float2>(), pl.ldU, gn.rspan, gn.Cu0,
-                                              gn.cspan, ctx->Sbox.as<float2>(), tw, st));
+            if (!last) {
+                rc = rows_forward(ctx, pl, tw, gn);
+                if (rc != FPM_OK) return rc;
+            }
             FPM_STAGE(ST_RMS_PUPIL,
                       launch_rmsprop_pupil(ctx->dP.as<float2>(), P, ctx->m2.as<float>(), P0,
                                            (int)s.plane, lr, p->beta, p->eps, p->pupil_margin,

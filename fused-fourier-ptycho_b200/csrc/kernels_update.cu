@@ -296,3 +296,44 @@ cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *mm, fl
 }
 
 }  // namespace fpm
+
+namespace fpm {
+
+// ---------------------------------------------------------------------------
+// Tiled transpose of a complex matrix: out[c * ldo + r] = in[r * ldi + c] for
+// r < rows, c < cols (32 x 32 tiles through shared memory, both sides coalesced).
+// With `conj_scale` != 0 the values are conjugated and multiplied by it.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_transpose_c(const float2 *__restrict__ in, size_t ldi,
+                                                      float2 *__restrict__ out, size_t ldo,
+                                                      int rows, int cols, float conj_scale) {
+    __shared__ float2 tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = r0 + ty + 8 * k, c = c0 + tx;
+        if (r < rows && c < cols) tile[ty + 8 * k][tx] = in[(size_t)r * ldi + c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int c = c0 + ty + 8 * k, r = r0 + tx;
+        if (r < rows && c < cols) {
+            float2 v = tile[tx][ty + 8 * k];
+            if (conj_scale != 0.f) v = make_float2(v.x * conj_scale, -v.y * conj_scale);
+            out[(size_t)c * ldo + r] = v;
+        }
+    }
+}
+
+cudaError_t launch_transpose(const float2 *in, size_t ldi, float2 *out, size_t ldo, int rows,
+                             int cols, float conj_scale, cudaStream_t st) {
+    if (rows <= 0 || cols <= 0) return cudaSuccess;
+    const dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+    if (grid.y > 65535u) return cudaErrorInvalidValue;
+    k_transpose_c<<<grid, 256, 0, st>>>(in, ldi, out, ldo, rows, cols, conj_scale);
+    return cudaGetLastError();
+}
+
+}  // namespace fpm

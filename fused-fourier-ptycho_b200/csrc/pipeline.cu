@@ -12,12 +12,13 @@
 //  L4 cols_fwd   X = FFT_r(T1); Xs[l][r][c] = X(fftshift(r, c)) row-major
 //  pupil grad    dP = sum_l conj(sub_l) Xs_l, LED order, Kahan (kernels.cuh:118-128)
 //  A rows_inv    per box row: stitch conj(P) Xs / H^2 of the covering LEDs (LED order,
-//                Kahan; kernels.cuh:95-116 as a gather), IFFT along the row -> U
+//                Kahan; kernels.cuh:95-116 as a gather), IFFT along the row -> Ur
+//                (row-major; a tiled transpose makes it U, column-major)
 //  B cols        per column: IFFT along r of U (zero outside the box rows) -> object
 //                gradient; RMSprop of O and m (kernels.cuh:364-382); FFT along r of the
 //                updated column, kept only on the next batch's box rows -> V
-//  C rows_fwd    per next-box row: FFT along the row of V, kept on the next box columns
-//                -> the next batch's Sbox
+//  C rows_fwd    per next-box row (V transposed to Vr first): FFT along the row,
+//                kept on the next box columns -> Sboxr, transposed into the next Sbox
 //
 // Only the box rows / columns of the gradient spectrum are non-zero and only the
 // next box is read, so passes A and C touch rspan lines instead of H, and U, V
@@ -30,7 +31,6 @@
 
 namespace fpm {
 
-using fft::Geo;
 using fft::swz;
 
 namespace {
@@ -49,12 +49,15 @@ __device__ __forceinline__ int box_index(int offset, int i, int H) {
 
 template <int N>
 constexpr int smem_bytes() {
-    return Geo<N>::LINE_BYTES + Geo<N>::TW_BYTES;
+    return fft::LG<N>::SMEM;
 }
 
 template <class K>
 cudaError_t set_smem(K kernel, int bytes) {
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
 }
 
 template <int TYPE>
@@ -64,45 +67,54 @@ __device__ __forceinline__ float amplitude(const StackView &Y, size_t idx, float
     return range > 0.f ? sqrtf(x / range) : sqrtf(x);
 }
 
+// Shared set-up of every pass kernel: twiddles into shared memory.
+template <int N>
+__device__ __forceinline__ void setup(float2 *smem, const float2 *thi, const float2 *tlo) {
+    using G = fft::LG<N>;
+    float2 *s_hi = G::tw_hi(smem);
+    fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, G::NHI, G::NLO);
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // L1: crop x pupil, ifftshift, inverse FFT along r (contiguous column lines)
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Geo<N>::THREADS)
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     k_lr_cols_inv(const float2 *__restrict__ Sbox, const float2 *__restrict__ P,
                   const int2 *__restrict__ led, BatchGeom g, int l0, int nl,
                   float2 *__restrict__ T1, const float2 *__restrict__ thi,
                   const float2 *__restrict__ tlo) {
-    using G = Geo<N>;
+    using G = fft::LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    fft::load_twiddles(s_hi, s_lo, thi, tlo, G::NHI, G::NLO);
-    const long long total = (long long)nl * N;
-    const long long g0 = (long long)blockIdx.x * G::LPC;
+    setup<N>(smem, thi, tlo);
+    const int ln = G::cline(), t = G::ct();
+    const long long gl = (long long)blockIdx.x * G::LPC + ln;
+    const bool live = gl < (long long)nl * N;
     constexpr int hh = N / 2;
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q / N;
-        const int e = q % N;
-        const long long gl = g0 + ln;
-        if (gl < total) {
-            const int lloc = (int)(gl / N);
-            const int cq = (int)(gl % N);
-            const int2 ab = led_box_offset(led, l0 + lloc, g);
+    float2 v[16];
+    if (live) {
+        const int lloc = (int)(gl / N);
+        const int cq = (int)(gl % N);
+        const int2 ab = led_box_offset(led, l0 + lloc, g);
+        const int c = cq + hh >= N ? cq + hh - N : cq + hh;
+        const float2 *scol = Sbox + (size_t)box_index(ab.y, c, g.H) * g.rspan;
+        const float2 *pcol = P + (size_t)c * N;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int e = t + m * G::T;
             const int r = e + hh >= N ? e + hh - N : e + hh;
-            const int c = cq + hh >= N ? cq + hh - N : cq + hh;
-            const float2 s = Sbox[(size_t)box_index(ab.y, c, g.H) * g.rspan +
-                                  box_index(ab.x, r, g.H)];
-            smem[ln * N + swz(e)] = cmul(s, P[(size_t)c * N + r]);
+            v[m] = cmul(scol[box_index(ab.x, r, g.H)], pcol[r]);
         }
+    } else {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[m] = make_float2(0.f, 0.f);
     }
-    __syncthreads();
-    fft::line_fft<N, +1>(smem + (threadIdx.x / G::T) * N, s_hi, s_lo, threadIdx.x % G::T);
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q / N;
-        const int e = q % N;
-        const long long gl = g0 + ln;
-        if (gl < total) T1[(size_t)gl * N + e] = smem[ln * N + swz(e)];
+    fft::line_fft_regs<N, +1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    if (live) {
+        float2 *dst = T1 + (size_t)gl * N;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) dst[t + m * G::T] = v[m];
     }
 }
 
@@ -110,47 +122,42 @@ __global__ void __launch_bounds__(Geo<N>::THREADS)
 // L2: inverse FFT along c (strided row lines) -> z (in place) and the residual
 // ---------------------------------------------------------------------------
 template <int N, int TYPE>
-__global__ void __launch_bounds__(Geo<N>::THREADS)
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     k_lr_rows_inv(StackView Y, BatchGeom g, int l0, int nl, float2 *__restrict__ T1,
                   float *__restrict__ Rs, const float2 *__restrict__ thi,
                   const float2 *__restrict__ tlo) {
-    using G = Geo<N>;
+    using G = fft::LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    fft::load_twiddles(s_hi, s_lo, thi, tlo, G::NHI, G::NLO);
-    const long long total = (long long)nl * N;
-    const long long g0 = (long long)blockIdx.x * G::LPC;
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q % G::LPC;
-        const int c = q / G::LPC;
-        const long long gl = g0 + ln;
-        if (gl < total) {
-            const size_t idx = ((size_t)(gl / N) * N + c) * N + (size_t)(gl % N);
-            smem[ln * N + swz(c)] = T1[idx];
-        }
-    }
-    __syncthreads();
-    fft::line_fft<N, +1>(smem + (threadIdx.x / G::T) * N, s_hi, s_lo, threadIdx.x % G::T);
+    setup<N>(smem, thi, tlo);
+    const int ln = G::iline(), t = G::it();
+    const long long gl = (long long)blockIdx.x * G::LPC + ln;
+    const bool live = gl < (long long)nl * N;
+    const int lloc = live ? (int)(gl / N) : 0;
+    const int r = live ? (int)(gl % N) : 0;
+    float2 *page = T1 + (size_t)lloc * N * N + r;   // element c at page[c * N]
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m)
+        v[m] = live ? page[(size_t)(t + m * G::T) * N] : make_float2(0.f, 0.f);
+    fft::line_fft_regs<N, +1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    if (!live) return;
     float mn = 0.f, range = 0.f;
     if (TYPE == kStackU16) {
         mn = (float)Y.minmax[0];
         range = (float)(Y.minmax[1] - Y.minmax[0]);
     }
     const float ratio = (float)((double)N * N * g.pratio * g.pratio);
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q % G::LPC;
-        const int c = q / G::LPC;
-        const long long gl = g0 + ln;
-        if (gl < total) {
-            const int lloc = (int)(gl / N);
-            const int r = (int)(gl % N);
-            const size_t idx = ((size_t)lloc * N + c) * N + r;
-            const float2 z = smem[ln * N + swz(c)];
-            T1[idx] = z;
-            const size_t ypix = (size_t)(g.z_off + l0 + lloc) * N * N + (size_t)c * N + r;
-            Rs[idx] = sqrtf(z.x * z.x + z.y * z.y) / ratio - amplitude<TYPE>(Y, ypix, mn, range);
-        }
+    const size_t ypage = (size_t)(g.z_off + l0 + lloc) * N * N + r;
+    float *rs = Rs + (size_t)lloc * N * N + r;
+    float y[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) y[m] = amplitude<TYPE>(Y, ypage + (size_t)(t + m * G::T) * N, mn, range);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const size_t off = (size_t)(t + m * G::T) * N;
+        const float2 z = v[m];
+        page[off] = z;
+        rs[off] = sqrtf(z.x * z.x + z.y * z.y) / ratio - y[m];
     }
 }
 
@@ -158,30 +165,31 @@ __global__ void __launch_bounds__(Geo<N>::THREADS)
 // L3: sign stencil of the residual, phase, forward FFT along c (strided rows)
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Geo<N>::THREADS)
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     k_lr_rows_fwd(BatchGeom g, int nl, float2 *__restrict__ T1, const float *__restrict__ Rs,
                   double *__restrict__ parts, const float2 *__restrict__ thi,
                   const float2 *__restrict__ tlo) {
-    using G = Geo<N>;
+    using G = fft::LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
     __shared__ double s_red[32];
-    fft::load_twiddles(s_hi, s_lo, thi, tlo, G::NHI, G::NLO);
-    const long long total = (long long)nl * N;
-    const long long g0 = (long long)blockIdx.x * G::LPC;
+    setup<N>(smem, thi, tlo);
+    const int ln = G::iline(), t = G::it();
+    const long long gl = (long long)blockIdx.x * G::LPC + ln;
+    const bool live = gl < (long long)nl * N;
+    const int lloc = live ? (int)(gl / N) : 0;
+    const int r = live ? (int)(gl % N) : 0;
     const float gscale = (float)(g.pratio * g.pratio);
+    const float *rp = Rs + (size_t)lloc * N * N;
+    float2 *page = T1 + (size_t)lloc * N * N + r;
+    const int rpp = r + 1 == N ? 0 : r + 1, rmm = r == 0 ? N - 1 : r - 1;
     double lsum = 0.0;
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q % G::LPC;
-        const int c = q / G::LPC;
-        const long long gl = g0 + ln;
-        if (gl < total) {
-            const int lloc = (int)(gl / N);
-            const int r = (int)(gl % N);
-            const float *rp = Rs + (size_t)lloc * N * N;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int c = t + m * G::T;
+        float2 o = make_float2(0.f, 0.f);
+        if (live) {
             const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
-            const int rpp = r + 1 == N ? 0 : r + 1, rmm = r == 0 ? N - 1 : r - 1;
             const float a = rp[(size_t)c * N + r];
             const float rx = rp[(size_t)cp * N + r] - a;     // res(r, c+1) - res(r, c)
             const float ry = rp[(size_t)c * N + rpp] - a;    // res(r+1, c) - res(r, c)
@@ -189,16 +197,15 @@ __global__ void __launch_bounds__(Geo<N>::THREADS)
             const float oym = sign1(a - rp[(size_t)c * N + rmm]);
             const float d = (oxm - sign1(rx) + oym - sign1(ry)) * gscale;
             lsum += (double)fabsf(rx) + (double)fabsf(ry);
-            const float2 z = T1[((size_t)lloc * N + c) * N + r];
+            const float2 z = page[(size_t)c * N];
             const float mag = sqrtf(z.x * z.x + z.y * z.y);
-            float2 o = make_float2(0.f, 0.f);
             if (mag > 0.f) {
                 const float inv = 1.0f / mag;
                 o.x = z.x * inv * d;
                 o.y = z.y * inv * d;
             }
-            smem[ln * N + swz(c)] = o;
         }
+        v[m] = o;
     }
     // fixed-order block reduction of the loss partial
 #pragma unroll
@@ -206,56 +213,47 @@ __global__ void __launch_bounds__(Geo<N>::THREADS)
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = lsum;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < G::THREADS / 32; ++w) t += s_red[w];
-        parts[blockIdx.x] = t;
+        double tot = 0.0;
+        for (int w = 0; w < G::THREADS / 32; ++w) tot += s_red[w];
+        parts[blockIdx.x] = tot;
     }
-    fft::line_fft<N, -1>(smem + (threadIdx.x / G::T) * N, s_hi, s_lo, threadIdx.x % G::T);
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q % G::LPC;
-        const int c = q / G::LPC;
-        const long long gl = g0 + ln;
-        if (gl < total) {
-            const size_t idx = ((size_t)(gl / N) * N + c) * N + (size_t)(gl % N);
-            T1[idx] = smem[ln * N + swz(c)];
-        }
+    fft::line_fft_regs<N, -1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    if (live) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) page[(size_t)(t + m * G::T) * N] = v[m];
     }
 }
 
 // ---------------------------------------------------------------------------
-// L4: forward FFT along r (contiguous columns) -> fftshift'ed row-major Xs
+// L4: forward FFT along r (column lines, interleaved so the row-major store of
+// the fftshift'ed Xs writes LPC consecutive columns per row)
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Geo<N>::THREADS)
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     k_lr_cols_fwd(int l0, int nl, const float2 *__restrict__ T1, float2 *__restrict__ Xs,
                   const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
-    using G = Geo<N>;
+    using G = fft::LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    fft::load_twiddles(s_hi, s_lo, thi, tlo, G::NHI, G::NLO);
-    const long long total = (long long)nl * N;
-    const long long g0 = (long long)blockIdx.x * G::LPC;
+    setup<N>(smem, thi, tlo);
+    const int ln = G::iline(), t = G::it();
+    const long long gl = (long long)blockIdx.x * G::LPC + ln;
+    const bool live = gl < (long long)nl * N;
     constexpr int hh = N / 2;
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q / N;
-        const int e = q % N;
-        const long long gl = g0 + ln;
-        if (gl < total) smem[ln * N + swz(e)] = T1[(size_t)gl * N + e];
-    }
-    __syncthreads();
-    fft::line_fft<N, -1>(smem + (threadIdx.x / G::T) * N, s_hi, s_lo, threadIdx.x % G::T);
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q % G::LPC;
-        const int r = q / G::LPC;
-        const long long gl = g0 + ln;
-        if (gl < total) {
-            const int lloc = (int)(gl / N);
-            const int cf = (int)(gl % N);
-            const int c = cf + hh >= N ? cf + hh - N : cf + hh;
-            const int rf = r + hh >= N ? r + hh - N : r + hh;
-            Xs[((size_t)(l0 + lloc) * N + r) * N + c] = smem[ln * N + swz(rf)];
-        }
+    const float2 *src = T1 + (size_t)(live ? gl : 0) * N;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = live ? src[t + m * G::T] : make_float2(0.f, 0.f);
+    fft::line_fft_regs<N, -1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    if (!live) return;
+    const int lloc = (int)(gl / N);
+    const int cf = (int)(gl % N);
+    const int c = cf + hh >= N ? cf + hh - N : cf + hh;
+    float2 *xs = Xs + (size_t)(l0 + lloc) * N * N + c;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int e = t + m * G::T;                  // frequency row of X
+        const int r = e + hh >= N ? e + hh - N : e + hh;
+        xs[(size_t)r * N] = v[m];
     }
 }
 
@@ -302,130 +300,141 @@ __global__ void __launch_bounds__(256) k_lr_pupil_grad(const float2 *__restrict_
 // Pass A: stitch the box rows of the gradient spectrum, inverse FFT along the row
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Geo<N>::THREADS)
-    k_big_rows_inv(BatchGeom g, const int2 *__restrict__ led, const float2 *__restrict__ P,
-                   const float2 *__restrict__ Xs, float2 *__restrict__ U, int ldU,
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
+    k_big_rows_inv(BatchGeom g, const int2 *__restrict__ led, const float2 *__restrict__ Pt,
+                   const float2 *__restrict__ Xs, float2 *__restrict__ Ur,
                    const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
-    using G = Geo<N>;
+    using G = fft::LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    int2 *s_ab = reinterpret_cast<int2 *>(s_lo + 128);
-    fft::load_twiddles(s_hi, s_lo, thi, tlo, G::NHI, G::NLO);
+    int2 *s_ab = reinterpret_cast<int2 *>(G::tw_hi(smem) + 256);
     for (int l = threadIdx.x; l < g.nb; l += G::THREADS) s_ab[l] = led_box_offset(led, l, g);
-    const int ln = threadIdx.x / G::T;
-    const int t = threadIdx.x % G::T;
+    setup<N>(smem, thi, tlo);
+    const int ln = G::cline(), t = G::ct();
     const int i = blockIdx.x * G::LPC + ln;     // box row of this line
-    float2 *line = smem + ln * N;
-    for (int e = t; e < N; e += G::T) line[swz(e)] = make_float2(0.f, 0.f);
-    __syncthreads();
+    const bool live = i < g.rspan;
     const int h = g.h;
-    const float inv_H2 = 1.0f / (float)((double)N * N);
-    if (i < g.rspan) {
-        // thread t owns box columns j = t + k*T; four per chunk
-        for (int j0 = 0; j0 < g.cspan; j0 += 4 * G::T) {
-            KahanC acc[4];
+    float2 v[16];
+    // four elements per LED sweep: four independent gathers in flight per thread
+#pragma unroll
+    for (int m0 = 0; m0 < 16; m0 += 4) {
+        int jj[4];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int j = t + (m0 + k) * G::T - g.Cu0;     // box column of element e
+            if (j < 0) j += N;
+            jj[k] = (live && j < g.cspan) ? j : -1;
+            any |= jj[k] >= 0;
+        }
+        KahanC acc[4];
+        if (__any_sync(0xffffffffu, any)) {
             for (int l = 0; l < g.nb; ++l) {
                 const int2 ab = s_ab[l];
                 int rr = i - ab.x;
                 if (rr < 0) rr += N;
-                if (rr >= h) continue;
+                if (rr >= h) continue;               // uniform per line
                 const float2 *xrow = Xs + ((size_t)l * h + rr) * h;
+                const float2 *prow = Pt + (size_t)rr * h;
+                float2 x[4], pp[4];
+                bool in[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    int c = j0 + t + k * G::T - ab.y;
+                    int c = jj[k] - ab.y;
                     if (c < 0) c += N;
-                    if (c < h && j0 + t + k * G::T < g.cspan) {
-                        float2 v = cmul_conj(xrow[c], P[(size_t)c * h + rr]);
-                        v.x *= inv_H2;
-                        v.y *= inv_H2;
-                        acc[k].add(v);
-                    }
+                    in[k] = jj[k] >= 0 && c < h;
+                    x[k] = in[k] ? xrow[c] : make_float2(0.f, 0.f);
+                    pp[k] = in[k] ? prow[c] : make_float2(0.f, 0.f);
                 }
-            }
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int j = j0 + t + k * G::T;
-                if (j < g.cspan) {
-                    int pos = g.Cu0 + j;
-                    pos = pos >= N ? pos - N : pos;
-                    line[swz(pos)] = acc[k].s;
+                for (int k = 0; k < 4; ++k) {
+                    if (in[k]) acc[k].add(cmul(x[k], pp[k]));
                 }
             }
         }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[m0 + k] = acc[k].s;
     }
-    __syncthreads();
-    fft::line_fft<N, +1>(line, s_hi, s_lo, t);
-    if (i < g.rspan)
-        for (int e = t; e < N; e += G::T) U[(size_t)e * ldU + i] = line[swz(e)];
+    fft::line_fft_regs<N, +1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    if (live) {
+        float2 *row = Ur + (size_t)i * N;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) row[t + m * G::T] = v[m];
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Pass B: columns (contiguous): IFFT of the gradient, RMSprop, FFT of the update
+// Pass B: columns (contiguous): IFFT of the gradient, RMSprop in registers,
+// FFT of the updated column; the IFFT's last stage hands its registers to the
+// RMSprop and the FFT's first stage without a shared-memory round trip.
 // ---------------------------------------------------------------------------
 template <int N, int MODE>
-__global__ void __launch_bounds__(Geo<N>::THREADS)
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     k_big_cols(ColsArgs a, const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
-    using G = Geo<N>;
+    using G = fft::LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    fft::load_twiddles(s_hi, s_lo, thi, tlo, G::NHI, G::NLO);
-    const int ln = threadIdx.x / G::T;
-    const int t = threadIdx.x % G::T;
+    setup<N>(smem, thi, tlo);
+    const int ln = G::cline(), t = G::ct();
     const int c = blockIdx.x * G::LPC + ln;    // column; c >= N only when N < LPC
     const bool live = c < N;
-    float2 *line = smem + ln * N;
+    float2 *line = smem + ln * G::STRIDE;
+    const float2 *s_hi = G::tw_hi(smem);
     const size_t col = (size_t)(live ? c : 0) * N;
+    float2 v[16];
     if (MODE == kColsForward) {
-        for (int e = t; e < N; e += G::T)
-            line[swz(e)] = live ? a.O[col + e] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[m] = live ? a.O[col + t + m * G::T] : make_float2(0.f, 0.f);
     } else {
-        for (int e = t; e < N; e += G::T) line[swz(e)] = make_float2(0.f, 0.f);
-        __syncthreads();
-        if (live) {
-            const float2 *u = a.U + (size_t)c * a.ldU;
-            for (int i = t; i < a.rspan; i += G::T) {
-                int pos = a.Ru0 + i;
-                pos = pos >= N ? pos - N : pos;
-                line[swz(pos)] = u[i];
-            }
+        const float2 *u = a.U + (size_t)(live ? c : 0) * a.ldU;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            int i = t + m * G::T - a.Ru0;          // box row of element e
+            if (i < 0) i += N;
+            v[m] = (live && i < a.rspan) ? u[i] : make_float2(0.f, 0.f);
         }
-    }
-    __syncthreads();
-    if (MODE != kColsForward) {
-        fft::line_fft<N, +1>(line, s_hi, s_lo, t);
+        fft::line_fft_regs<N, +1>(v, line, s_hi, s_hi + 128, t);
         if (MODE == kColsGradient) {
-            if (live)
-                for (int e = t; e < N; e += G::T) a.gout[col + e] = line[swz(e)];
+            if (live) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) a.gout[col + t + m * G::T] = v[m];
+            }
             return;
         }
         // RMSprop on the column (constrained_RMSprop_both, kernels.cuh:364-382)
         const float omb = 1.0f - a.beta;
         if (live) {
-            for (int e = t; e < N; e += G::T) {
-                const float2 gv = line[swz(e)];
-                float2 w = a.O[col + e];
-                float mu = gv.x * gv.x + gv.y * gv.y;
-                mu = a.beta * a.m[col + e] + omb * mu;
-                const float sq = a.lr / (sqrtf(mu) + a.eps);
-                w.x -= gv.x * sq;
-                w.y -= gv.y * sq;
-                a.O[col + e] = w;
-                a.m[col + e] = mu;
-                line[swz(e)] = w;
+#pragma unroll
+            for (int m0 = 0; m0 < 16; m0 += 4) {
+                float2 w[4];
+                float mv[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    w[k] = a.O[col + t + (m0 + k) * G::T];
+                    mv[k] = a.m[col + t + (m0 + k) * G::T];
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float2 gv = v[m0 + k];
+                    float mu = gv.x * gv.x + gv.y * gv.y;
+                    mu = a.beta * mv[k] + omb * mu;
+                    const float sq = a.lr / (sqrtf(mu) + a.eps);
+                    w[k].x -= gv.x * sq;
+                    w[k].y -= gv.y * sq;
+                    a.O[col + t + (m0 + k) * G::T] = w[k];
+                    a.m[col + t + (m0 + k) * G::T] = mu;
+                    v[m0 + k] = w[k];
+                }
             }
         }
         if (a.rspan_n == 0) return;   // uniform over the grid: no next batch
-        __syncthreads();
     }
-    fft::line_fft<N, -1>(line, s_hi, s_lo, t);
+    fft::line_fft_regs<N, -1>(v, line, s_hi, s_hi + 128, t);
     if (live) {
-        float2 *v = a.V + (size_t)c * a.ldV;
-        for (int i = t; i < a.rspan_n; i += G::T) {
-            int pos = a.Ru0n + i;
-            pos = pos >= N ? pos - N : pos;
-            v[i] = line[swz(pos)];
+        float2 *vv = a.V + (size_t)c * a.ldV;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            int i = t + m * G::T - a.Ru0n;
+            if (i < 0) i += N;
+            if (i < a.rspan_n) vv[i] = v[m];
         }
     }
 }
@@ -434,30 +443,27 @@ __global__ void __launch_bounds__(Geo<N>::THREADS)
 // Pass C: rows of V (strided) -> FFT along the row -> the next batch's Sbox
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(Geo<N>::THREADS)
-    k_big_rows_fwd(const float2 *__restrict__ V, int ldV, int rspan_n, int Cu0n, int cspan_n,
-                   float2 *__restrict__ Sbox, const float2 *__restrict__ thi,
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
+    k_big_rows_fwd(const float2 *__restrict__ Vr, int rspan_n, int Cu0n, int cspan_n,
+                   float2 *__restrict__ Sboxr, const float2 *__restrict__ thi,
                    const float2 *__restrict__ tlo) {
-    using G = Geo<N>;
+    using G = fft::LG<N>;
     extern __shared__ float2 smem[];
-    float2 *s_hi = smem + G::LPC * N;
-    float2 *s_lo = s_hi + 128;
-    fft::load_twiddles(s_hi, s_lo, thi, tlo, G::NHI, G::NLO);
-    const int i0 = blockIdx.x * G::LPC;
-    for (int q = threadIdx.x; q < G::LPC * N; q += G::THREADS) {
-        const int ln = q % G::LPC;
-        const int e = q / G::LPC;
-        if (i0 + ln < rspan_n) smem[ln * N + swz(e)] = V[(size_t)e * ldV + i0 + ln];
-    }
-    __syncthreads();
-    fft::line_fft<N, -1>(smem + (threadIdx.x / G::T) * N, s_hi, s_lo, threadIdx.x % G::T);
-    for (int q = threadIdx.x; q < G::LPC * cspan_n; q += G::THREADS) {
-        const int ln = q % G::LPC;
-        const int j = q / G::LPC;
-        if (i0 + ln < rspan_n) {
-            int pos = Cu0n + j;
-            pos = pos >= N ? pos - N : pos;
-            Sbox[(size_t)j * rspan_n + i0 + ln] = smem[ln * N + swz(pos)];
+    setup<N>(smem, thi, tlo);
+    const int ln = G::cline(), t = G::ct();
+    const int i = blockIdx.x * G::LPC + ln;
+    const bool live = i < rspan_n;
+    const float2 *row = Vr + (size_t)(live ? i : 0) * N;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = live ? row[t + m * G::T] : make_float2(0.f, 0.f);
+    fft::line_fft_regs<N, -1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    if (live) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            int j = t + m * G::T - Cu0n;
+            if (j < 0) j += N;
+            if (j < cspan_n) Sboxr[(size_t)i * cspan_n + j] = v[m];
         }
     }
 }
@@ -503,7 +509,7 @@ bool pipeline_supported(int h, int H) {
         default: return cudaErrorInvalidValue; \
     }
 
-static int lpc_of(int n) { return (n * 8 >= 64 * 1024) ? 1 : (64 * 1024) / (n * 8); }
+static int lpc_of(int n) { return (n * 8 >= 64 * 1024) ? 1 : (64 * 1024) / (n * 8); }  // fft::LG<n>::LPC
 
 int lr_blocks(int h, int nl) {
     const long long lines = (long long)nl * h;
@@ -518,7 +524,7 @@ cudaError_t launch_lr_cols_inv(const BatchGeom &g, const int2 *led, const float2
 #define F(N)                                                                              \
     e = set_smem(k_lr_cols_inv<N>, smem_bytes<N>());                                      \
     if (e != cudaSuccess) return e;                                                       \
-    k_lr_cols_inv<N><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(                   \
+    k_lr_cols_inv<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                   \
         b.Sbox, P, led, g, l0, nl, b.T1, tw.lo_hi, tw.lo_lo);
     FPM_DISPATCH_LR(g.h, F)
 #undef F
@@ -533,12 +539,12 @@ cudaError_t launch_lr_rows_inv(const BatchGeom &g, StackView Y, BatchBufs b, int
     if (Y.type == kStackU16) {                                                            \
         e = set_smem(k_lr_rows_inv<N, kStackU16>, smem_bytes<N>());                       \
         if (e != cudaSuccess) return e;                                                   \
-        k_lr_rows_inv<N, kStackU16><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(    \
+        k_lr_rows_inv<N, kStackU16><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(    \
             Y, g, l0, nl, b.T1, b.Rs, tw.lo_hi, tw.lo_lo);                                \
     } else {                                                                              \
         e = set_smem(k_lr_rows_inv<N, kStackF32>, smem_bytes<N>());                       \
         if (e != cudaSuccess) return e;                                                   \
-        k_lr_rows_inv<N, kStackF32><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(    \
+        k_lr_rows_inv<N, kStackF32><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(    \
             Y, g, l0, nl, b.T1, b.Rs, tw.lo_hi, tw.lo_lo);                                \
     }
     FPM_DISPATCH_LR(g.h, F)
@@ -554,7 +560,7 @@ cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, 
 #define F(N)                                                                              \
     e = set_smem(k_lr_rows_fwd<N>, smem_bytes<N>());                                      \
     if (e != cudaSuccess) return e;                                                       \
-    k_lr_rows_fwd<N><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(                   \
+    k_lr_rows_fwd<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                   \
         g, nl, b.T1, b.Rs, b.parts + part_off, tw.lo_hi, tw.lo_lo);
     FPM_DISPATCH_LR(g.h, F)
 #undef F
@@ -568,7 +574,7 @@ cudaError_t launch_lr_cols_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl,
 #define F(N)                                                                              \
     e = set_smem(k_lr_cols_fwd<N>, smem_bytes<N>());                                      \
     if (e != cudaSuccess) return e;                                                       \
-    k_lr_cols_fwd<N><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(                   \
+    k_lr_cols_fwd<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                   \
         l0, nl, b.T1, b.Xs, tw.lo_hi, tw.lo_lo);
     FPM_DISPATCH_LR(g.h, F)
 #undef F
@@ -582,17 +588,17 @@ cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs 
     return cudaGetLastError();
 }
 
-cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float2 *P,
-                                const float2 *Xs, float2 *U, int ldU, const Twiddles &tw,
+cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float2 *Pt,
+                                const float2 *Xs, float2 *Ur, const Twiddles &tw,
                                 cudaStream_t st) {
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                                  \
     {                                                                                         \
         const int smem = smem_bytes<N>() + g.nb * (int)sizeof(int2);                          \
-        const int blocks = (g.rspan + Geo<N>::LPC - 1) / Geo<N>::LPC;                          \
+        const int blocks = (g.rspan + fft::LG<N>::LPC - 1) / fft::LG<N>::LPC;                          \
         e = set_smem(k_big_rows_inv<N>, smem);                                                \
         if (e != cudaSuccess) return e;                                                       \
-        k_big_rows_inv<N><<<blocks, Geo<N>::THREADS, smem, st>>>(g, led, P, Xs, U, ldU,       \
+        k_big_rows_inv<N><<<blocks, fft::LG<N>::THREADS, smem, st>>>(g, led, Pt, Xs, Ur,          \
                                                                  tw.hi_hi, tw.hi_lo);         \
     }
     FPM_DISPATCH_BIG(g.H, F)
@@ -604,21 +610,21 @@ cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t 
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                                  \
     {                                                                                         \
-        const int blocks = (N + Geo<N>::LPC - 1) / Geo<N>::LPC;                               \
+        const int blocks = (N + fft::LG<N>::LPC - 1) / fft::LG<N>::LPC;                               \
         if (a.mode == kColsForward) {                                                         \
             e = set_smem(k_big_cols<N, kColsForward>, smem_bytes<N>());                       \
             if (e != cudaSuccess) return e;                                                   \
-            k_big_cols<N, kColsForward><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(    \
+            k_big_cols<N, kColsForward><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(    \
                 a, tw.hi_hi, tw.hi_lo);                                                       \
         } else if (a.mode == kColsUpdate) {                                                   \
             e = set_smem(k_big_cols<N, kColsUpdate>, smem_bytes<N>());                        \
             if (e != cudaSuccess) return e;                                                   \
-            k_big_cols<N, kColsUpdate><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(     \
+            k_big_cols<N, kColsUpdate><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(     \
                 a, tw.hi_hi, tw.hi_lo);                                                       \
         } else {                                                                              \
             e = set_smem(k_big_cols<N, kColsGradient>, smem_bytes<N>());                      \
             if (e != cudaSuccess) return e;                                                   \
-            k_big_cols<N, kColsGradient><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(   \
+            k_big_cols<N, kColsGradient><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(   \
                 a, tw.hi_hi, tw.hi_lo);                                                       \
         }                                                                                     \
     }
@@ -627,16 +633,16 @@ cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t 
     return cudaGetLastError();
 }
 
-cudaError_t launch_big_rows_fwd(int H, const float2 *V, int ldV, int rspan_n, int Cu0n,
-                                int cspan_n, float2 *Sbox, const Twiddles &tw, cudaStream_t st) {
+cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, int cspan_n,
+                                float2 *Sboxr, const Twiddles &tw, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                                  \
     {                                                                                         \
-        const int blocks = (rspan_n + Geo<N>::LPC - 1) / Geo<N>::LPC;                          \
+        const int blocks = (rspan_n + fft::LG<N>::LPC - 1) / fft::LG<N>::LPC;                          \
         e = set_smem(k_big_rows_fwd<N>, smem_bytes<N>());                                     \
         if (e != cudaSuccess) return e;                                                       \
-        k_big_rows_fwd<N><<<blocks, Geo<N>::THREADS, smem_bytes<N>(), st>>>(                  \
-            V, ldV, rspan_n, Cu0n, cspan_n, Sbox, tw.hi_hi, tw.hi_lo);                        \
+        k_big_rows_fwd<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                  \
+            Vr, rspan_n, Cu0n, cspan_n, Sboxr, tw.hi_hi, tw.hi_lo);                           \
     }
     FPM_DISPATCH_BIG(H, F)
 #undef F

@@ -47,9 +47,11 @@ cudaError_t launch_lr_cols_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl,
 cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs b, float2 *dP,
                                  cudaStream_t st);
 
-// Pass A: gradient spectrum rows of the box -> inverse FFT along the rows -> U [H][ldU].
-cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float2 *P,
-                                const float2 *Xs, float2 *U, int ldU, const Twiddles &tw,
+// Pass A: gradient spectrum rows of the box -> inverse FFT along the rows ->
+// Ur [rspan][H] (row-major).  Pt is the conjugated pupil transposed to row-major
+// and scaled by 1/H^2: Pt[r*h + c] = conj(P[c*h + r]) / H^2.
+cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float2 *Pt,
+                                const float2 *Xs, float2 *Ur, const Twiddles &tw,
                                 cudaStream_t st);
 
 enum BigColsMode : int { kColsForward = 0, kColsUpdate = 1, kColsGradient = 2 };
@@ -72,8 +74,9 @@ struct ColsArgs {
 };
 cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t st);
 
-// Pass C: rows i < rspan_n of V -> FFT along the rows -> Sbox[j][i] = row[(Cu0n + j) mod H].
-cudaError_t launch_big_rows_fwd(int H, const float2 *V, int ldV, int rspan_n, int Cu0n,
-                                int cspan_n, float2 *Sbox, const Twiddles &tw, cudaStream_t st);
+// Pass C: rows i < rspan_n of Vr [rspan_n][H] -> FFT along the rows ->
+// Sboxr[i][j] = row[(Cu0n + j) mod H] (row-major, leading dim cspan_n).
+cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, int cspan_n,
+                                float2 *Sboxr, const Twiddles &tw, cudaStream_t st);
 
 }  // namespace fpm
