@@ -159,10 +159,10 @@ def stage_bytes(cfg: Cfg, led):
     H2, h2 = H * H, h * h
     boxes = batch_boxes(led, h, H, cfg.batch)
     nbatch = len(boxes)
-    group = max(1, min(cfg.batch, (4 << 30) // (h2 * 12)))
+    group = max(1, min(cfg.batch, (4 << 30) // (h2 * 16)))
     lr_launches = sum(math.ceil(nb / group) for nb, _, _ in boxes)
     tot = {k: 0.0 for k in ("lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
-                            "lr_cols_forward", "pupil_grad", "rows_inverse_stitch",
+                            "lr_rows_fused", "lr_cols_forward", "pupil_grad", "rows_inverse_stitch",
                             "cols_update", "rows_forward", "rmsprop_pupil", "transpose")}
     for bi, (nb, rspan, cspan) in enumerate(boxes):
         _, rn, cn = boxes[(bi + 1) % nbatch]
@@ -170,6 +170,7 @@ def stage_bytes(cfg: Cfg, led):
         tot["lr_cols_inverse"] += 16 * px      # crop of the spectrum box r8, field w8
         tot["lr_rows_inverse"] += 22 * px      # field r8 w8, residual w4, stack r2
         tot["lr_rows_forward"] += 20 * px      # residual r4, field r8 w8
+        tot["lr_rows_fused"] += 18 * px        # field r8, stack r2, field w8 (halo re-reads not counted)
         tot["lr_cols_forward"] += 16 * px      # field r8, gradient spectrum w8
         tot["pupil_grad"] += 16 * px + 8 * h2  # spectrum box r8 + gradient spectrum r8 per LED px
         tot["rows_inverse_stitch"] += 8 * px + 8 * H * rspan

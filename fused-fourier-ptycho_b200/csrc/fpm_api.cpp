@@ -76,13 +76,13 @@ namespace {
 enum Stage : int {
     ST_COLS_FORWARD, ST_ROWS_FORWARD, ST_LR_COLS_INV, ST_LR_ROWS_INV, ST_LR_ROWS_FWD,
     ST_LR_COLS_FWD, ST_LOSS, ST_PUPIL_GRAD, ST_ROWS_INV, ST_COLS_UPDATE, ST_RMS_PUPIL,
-    ST_SPECTRUM, ST_TRANSPOSE, ST_COUNT
+    ST_SPECTRUM, ST_TRANSPOSE, ST_LR_ROWS_FUSED, ST_COUNT
 };
 const char *const kStageName[ST_COUNT] = {
     "cols_forward", "rows_forward", "lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
     "lr_cols_forward", "loss_reduce", "pupil_grad", "rows_inverse_stitch", "cols_update",
-    "rmsprop_pupil", "spectrum_fft2", "transpose"};
-const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    "rmsprop_pupil", "spectrum_fft2", "transpose", "lr_rows_fused"};
+const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
 
 struct Profiler {
     bool on = false;
@@ -152,7 +152,7 @@ struct fpm_context {
     std::string err;
     FftEngine fft;
     // work buffers, kept between calls
-    DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
+    DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
         minmax, spec;
 };
 
@@ -343,7 +343,9 @@ struct Plan {
     size_t sbox = 0;    // max box rows x cols
     int group = 1;      // LEDs per low-resolution launch group
     int parts = 0;      // loss partial slots of the largest batch
+    bool fused_rows = false;  // L2 + L3 as one pass (T2 instead of Rs)
 };
+
 
 Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch) {
     Plan pl;
@@ -369,14 +371,20 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch) {
     // LEDs per low-resolution launch: the whole batch (measured fastest: large
     // grids, no tails; the field + residual of 26 LEDs of 2048^2 take 1.3 GB), capped
     // at 4 GiB of field + residual; FPM_LR_GROUP overrides it (tuning).
-    const size_t per = s.plane * 12;
+    const size_t per = s.plane * 16;
     pl.group = (int)std::max<size_t>(1, std::min<size_t>(s.B, (4ull << 30) / per));
     if (const char *env = std::getenv("FPM_LR_GROUP")) {
         const int v = std::atoi(env);
         if (v > 0) pl.group = std::min(v, s.B);
     }
+    // fused L2 + L3 where its CTA shape exists; FPM_LR_FUSED=0 keeps the separate passes
+    pl.fused_rows = lr_rows_fused_supported(s.h);
+    if (const char *env = std::getenv("FPM_LR_FUSED")) pl.fused_rows = pl.fused_rows && std::atoi(env) != 0;
     int parts = 0;
-    for (int l0 = 0; l0 < s.B; l0 += pl.group) parts += lr_blocks(s.h, std::min(pl.group, s.B - l0));
+    for (int l0 = 0; l0 < s.B; l0 += pl.group) {
+        const int nl = std::min(pl.group, s.B - l0);
+        parts += pl.fused_rows ? lr_rows_fused_blocks(s.h, nl) : lr_blocks(s.h, nl);
+    }
     pl.parts = parts;
     return pl;
 }
@@ -387,7 +395,7 @@ size_t solve_bytes(const fpm_problem *p, const Shape &s, const Plan &pl, bool ho
     b += (size_t)s.H * pl.ldU * 8 * 3;                // U, V and their row-major twin
     b += pl.sbox * 8 * 2;                             // Sbox and its row-major twin
     b += s.plane * 8 * s.B;                           // Xs
-    b += s.plane * 12 * pl.group;                     // T1, Rs
+    b += s.plane * (pl.fused_rows ? 16 : 12) * pl.group;   // T1 and T2 or Rs
     b += s.plane * (8 * 4 + 4 * 2);                   // P, dP, Pt, m2, P0
     if (spec) b += s.big * 8;                         // spectrum / gradient staging
     if (host) b += s.plane * s.L * (p->stack_type == FPM_STACK_U16_COUNTS ? 2 : 4);
@@ -409,7 +417,10 @@ fpm_status alloc_pipeline(fpm_context *ctx, const fpm_problem *p, const Shape &s
     FPM_CK(ctx->Pt.ensure(s.plane * 8));
     FPM_CK(ctx->Xs.ensure(s.plane * 8 * s.B));
     FPM_CK(ctx->T1.ensure(s.plane * 8 * pl.group));
-    FPM_CK(ctx->Rs.ensure(s.plane * 4 * pl.group));
+    if (pl.fused_rows)
+        FPM_CK(ctx->T2.ensure(s.plane * 8 * pl.group));
+    else
+        FPM_CK(ctx->Rs.ensure(s.plane * 4 * pl.group));
     FPM_CK(ctx->dP.ensure(s.plane * 8));
     FPM_CK(ctx->parts.ensure(sizeof(double) * (size_t)std::max(pl.parts, 1)));
     return FPM_OK;
@@ -426,6 +437,7 @@ BatchBufs bufs_of(fpm_context *ctx) {
     b.Sbox = ctx->Sbox.as<float2>();
     b.T1 = ctx->T1.as<float2>();
     b.Rs = ctx->Rs.as<float>();
+    b.T2 = ctx->T2.as<float2>();
     b.Xs = ctx->Xs.as<float2>();
     b.parts = ctx->parts.as<double>();
     return b;
@@ -472,10 +484,17 @@ fpm_status lowres_and_stitch(fpm_context *ctx, const Plan &pl, const Twiddles &t
     for (int l0 = 0; l0 < g.nb; l0 += pl.group) {
         const int nl = std::min(pl.group, g.nb - l0);
         FPM_STAGE(ST_LR_COLS_INV, launch_lr_cols_inv(g, in.led, P, b, l0, nl, tw, st));
-        FPM_STAGE(ST_LR_ROWS_INV, launch_lr_rows_inv(g, in.Y, b, l0, nl, tw, st));
-        FPM_STAGE(ST_LR_ROWS_FWD, launch_lr_rows_fwd(g, b, l0, nl, part_off, tw, st));
-        FPM_STAGE(ST_LR_COLS_FWD, launch_lr_cols_fwd(g, b, l0, nl, tw, st));
-        part_off += lr_blocks(g.h, nl);
+        if (pl.fused_rows) {
+            FPM_STAGE(ST_LR_ROWS_FUSED,
+                      launch_lr_rows_fused(g, in.Y, b, l0, nl, part_off, tw, st));
+            FPM_STAGE(ST_LR_COLS_FWD, launch_lr_cols_fwd(g, b.T2, b, l0, nl, tw, st));
+            part_off += lr_rows_fused_blocks(g.h, nl);
+        } else {
+            FPM_STAGE(ST_LR_ROWS_INV, launch_lr_rows_inv(g, in.Y, b, l0, nl, tw, st));
+            FPM_STAGE(ST_LR_ROWS_FWD, launch_lr_rows_fwd(g, b, l0, nl, part_off, tw, st));
+            FPM_STAGE(ST_LR_COLS_FWD, launch_lr_cols_fwd(g, b.T1, b, l0, nl, tw, st));
+            part_off += lr_blocks(g.h, nl);
+        }
     }
     FPM_STAGE(ST_LOSS, launch_loss_accumulate(b.parts, part_off, loss_slot, st));
     FPM_STAGE(ST_PUPIL_GRAD, launch_lr_pupil_grad(g, in.led, b, ctx->dP.as<float2>(), st));

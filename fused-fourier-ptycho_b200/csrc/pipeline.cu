@@ -225,6 +225,117 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 }
 
 // ---------------------------------------------------------------------------
+// L2 + L3 fused: a CTA of 1024 threads takes LIN consecutive row lines r0-1 ..
+// r0+LOUT (modulo h) of one LED, runs their inverse FFTs, keeps the residuals of
+// all LIN lines in shared memory and finishes the LOUT central lines (stencil,
+// phase, forward FFT).  The two halo lines supply res(r -/+ 1, c); their inverse
+// FFTs are recomputed by the neighbouring CTAs.  The output goes to a second
+// buffer because neighbours still read the halo rows of the input.
+// ---------------------------------------------------------------------------
+template <int N>
+struct L23 {
+    static constexpr int T = N / 16;
+    static constexpr int LIN = 1024 / T;              // lines per CTA, halo included
+    static constexpr int LOUT = LIN - 2;              // central lines per CTA
+    static constexpr int PAD = 16 / LIN > 0 ? 16 / LIN : 1;
+    static constexpr int STRIDE = N + PAD;            // FFT exchange line stride (float2)
+    // residual line stride (float): the 32 (line, t) pairs of a warp on 32 banks
+    static constexpr int RSTRIDE = N + (LIN >= 32 ? 1 : 32 / LIN);
+    static constexpr int SMEM = LIN * STRIDE * 8 + LIN * RSTRIDE * 4 + 2 * 128 * 8;
+    static constexpr int CTAS_PER_LED = (N + LOUT - 1) / LOUT;
+    static constexpr int NHI = N >= 128 ? N / 128 : 1;
+    static constexpr int NLO = N >= 128 ? 128 : N;
+    static_assert(LIN >= 8 && LIN % 2 == 0, "fused row pass needs T <= 128");
+};
+
+template <int N, int TYPE>
+__global__ void __launch_bounds__(1024, 1)
+    k_lr_rows_fused(StackView Y, BatchGeom g, int l0, const float2 *__restrict__ T1,
+                    float2 *__restrict__ T2, double *__restrict__ parts,
+                    const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
+    using F = L23<N>;
+    constexpr int T = F::T;
+    extern __shared__ float2 smem[];
+    __shared__ double s_red[32];
+    float *res = reinterpret_cast<float *>(smem + F::LIN * F::STRIDE);
+    float2 *s_hi = reinterpret_cast<float2 *>(res + F::LIN * F::RSTRIDE);
+    fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, F::NHI, F::NLO);
+    __syncthreads();
+    const int k = threadIdx.x % F::LIN, t = threadIdx.x / F::LIN;
+    const int lloc = blockIdx.x / F::CTAS_PER_LED;
+    const int r0 = (blockIdx.x % F::CTAS_PER_LED) * F::LOUT;
+    int r = r0 - 1 + k;
+    r = r < 0 ? r + N : (r >= N ? r - N : r);          // r0 - 1 + k < 2N
+    const bool central = k >= 1 && k <= F::LOUT && r0 + k - 1 < N;
+    const float2 *page = T1 + (size_t)lloc * N * N + r;   // element c at page[c * N]
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = page[(size_t)(t + m * T) * N];
+    float2 *line = smem + k * F::STRIDE;
+    fft::line_fft_regs<N, +1>(v, line, s_hi, s_hi + 128, t);
+    float mn = 0.f, range = 0.f;
+    if (TYPE == kStackU16) {
+        mn = (float)Y.minmax[0];
+        range = (float)(Y.minmax[1] - Y.minmax[0]);
+    }
+    const float ratio = (float)((double)N * N * g.pratio * g.pratio);
+    const size_t ypage = (size_t)(g.z_off + l0 + lloc) * N * N + r;
+    float *rk = res + k * F::RSTRIDE;
+    {
+        float y[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m)
+            y[m] = amplitude<TYPE>(Y, ypage + (size_t)(t + m * T) * N, mn, range);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const float2 z = v[m];
+            rk[t + m * T] = sqrtf(z.x * z.x + z.y * z.y) / ratio - y[m];
+        }
+    }
+    __syncthreads();
+    const float gscale = (float)(g.pratio * g.pratio);
+    double lsum = 0.0;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int c = t + m * T;
+        float2 o = make_float2(0.f, 0.f);
+        if (central) {
+            const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
+            const float a = rk[c];
+            const float rx = rk[cp] - a;                    // res(r, c+1) - res(r, c)
+            const float ry = rk[F::RSTRIDE + c] - a;        // res(r+1, c) - res(r, c)
+            const float oxm = sign1(a - rk[cm]);
+            const float oym = sign1(a - rk[c - F::RSTRIDE]);
+            const float d = (oxm - sign1(rx) + oym - sign1(ry)) * gscale;
+            lsum += (double)fabsf(rx) + (double)fabsf(ry);
+            const float2 z = v[m];
+            const float mag = sqrtf(z.x * z.x + z.y * z.y);
+            if (mag > 0.f) {
+                const float inv = 1.0f / mag;
+                o.x = z.x * inv * d;
+                o.y = z.y * inv * d;
+            }
+        }
+        v[m] = o;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = lsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < 32; ++w) tot += s_red[w];
+        parts[blockIdx.x] = tot;
+    }
+    fft::line_fft_regs<N, -1>(v, line, s_hi, s_hi + 128, t);
+    if (central) {
+        float2 *dst = T2 + (size_t)lloc * N * N + r;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) dst[(size_t)(t + m * T) * N] = v[m];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // L4: forward FFT along r (column lines, interleaved so the row-major store of
 // the fftshift'ed Xs writes LPC consecutive columns per row)
 // ---------------------------------------------------------------------------
@@ -567,15 +678,57 @@ cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_lr_cols_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl,
-                               const Twiddles &tw, cudaStream_t st) {
+bool lr_rows_fused_supported(int h) { return h >= 128 && h <= 2048 && (h & (h - 1)) == 0; }
+
+static int ctas_per_led_fused(int h) {   // L23<h>::CTAS_PER_LED
+    const int lout = 1024 / (h / 16) - 2;
+    return (h + lout - 1) / lout;
+}
+
+int lr_rows_fused_blocks(int h, int nl) { return nl * ctas_per_led_fused(h); }
+
+#define FPM_DISPATCH_FUSED(n, F) \
+    switch (n) {                 \
+        case 128: F(128); break;  \
+        case 256: F(256); break;  \
+        case 512: F(512); break;  \
+        case 1024: F(1024); break; \
+        case 2048: F(2048); break; \
+        default: return cudaErrorInvalidValue; \
+    }
+
+cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, BatchBufs b, int l0, int nl,
+                                 int part_off, const Twiddles &tw, cudaStream_t st) {
+    const int blocks = lr_rows_fused_blocks(g.h, nl);
+    cudaError_t e = cudaSuccess;
+#define F(N)                                                                              \
+    static_assert(L23<N>::CTAS_PER_LED == (N + 1024 / (N / 16) - 3) / (1024 / (N / 16) - 2), \
+                  "host CTA count");                                                      \
+    if (Y.type == kStackU16) {                                                            \
+        e = set_smem(k_lr_rows_fused<N, kStackU16>, L23<N>::SMEM);                        \
+        if (e != cudaSuccess) return e;                                                   \
+        k_lr_rows_fused<N, kStackU16><<<blocks, 1024, L23<N>::SMEM, st>>>(                \
+            Y, g, l0, b.T1, b.T2, b.parts + part_off, tw.lo_hi, tw.lo_lo);           \
+    } else {                                                                              \
+        e = set_smem(k_lr_rows_fused<N, kStackF32>, L23<N>::SMEM);                        \
+        if (e != cudaSuccess) return e;                                                   \
+        k_lr_rows_fused<N, kStackF32><<<blocks, 1024, L23<N>::SMEM, st>>>(                \
+            Y, g, l0, b.T1, b.T2, b.parts + part_off, tw.lo_hi, tw.lo_lo);           \
+    }
+    FPM_DISPATCH_FUSED(g.h, F)
+#undef F
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs b, int l0,
+                               int nl, const Twiddles &tw, cudaStream_t st) {
     const int blocks = lr_blocks(g.h, nl);
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                              \
     e = set_smem(k_lr_cols_fwd<N>, smem_bytes<N>());                                      \
     if (e != cudaSuccess) return e;                                                       \
     k_lr_cols_fwd<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                   \
-        l0, nl, b.T1, b.Xs, tw.lo_hi, tw.lo_lo);
+        l0, nl, src, b.Xs, tw.lo_hi, tw.lo_lo);
     FPM_DISPATCH_LR(g.h, F)
 #undef F
     return cudaGetLastError();
@@ -598,8 +751,8 @@ cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float
         const int blocks = (g.rspan + fft::LG<N>::LPC - 1) / fft::LG<N>::LPC;                          \
         e = set_smem(k_big_rows_inv<N>, smem);                                                \
         if (e != cudaSuccess) return e;                                                       \
-        k_big_rows_inv<N><<<blocks, fft::LG<N>::THREADS, smem, st>>>(g, led, Pt, Xs, Ur,          \
-                                                                 tw.hi_hi, tw.hi_lo);         \
+        k_big_rows_inv<N><<<blocks, fft::LG<N>::THREADS, smem, st>>>(                           \
+            g, led, Pt, Xs, Ur, tw.hi_hi, tw.hi_lo);                                                                        \
     }
     FPM_DISPATCH_BIG(g.H, F)
 #undef F

@@ -27,7 +27,8 @@ struct Twiddles {
 struct BatchBufs {
     const float2 *Sbox = nullptr;  // [cspan][rspan] spectrum inside the box (leading dim rspan)
     float2 *T1 = nullptr;          // [group][h][h] per-LED field (group-local pages)
-    float *Rs = nullptr;           // [group][h][h] residual |z|/(h^2 p^2) - Y
+    float *Rs = nullptr;           // [group][h][h] residual |z|/(h^2 p^2) - Y (separate L2, L3)
+    float2 *T2 = nullptr;          // [group][h][h] output of the fused L2 + L3 pass
     float2 *Xs = nullptr;          // [nb][h][h] row-major fftshift'ed gradient spectrum
     double *parts = nullptr;       // loss partials of the batch
 };
@@ -42,8 +43,15 @@ cudaError_t launch_lr_rows_inv(const BatchGeom &g, StackView Y, BatchBufs b, int
                                const Twiddles &tw, cudaStream_t st);
 cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, int part_off,
                                const Twiddles &tw, cudaStream_t st);
-cudaError_t launch_lr_cols_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl,
-                               const Twiddles &tw, cudaStream_t st);
+// L2 + L3 in one pass (h in [128, 2048]): T1 -> T2, loss partials at parts + part_off,
+// lr_rows_fused_blocks(h, nl) of them.
+bool lr_rows_fused_supported(int h);
+int lr_rows_fused_blocks(int h, int nl);
+cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, BatchBufs b, int l0, int nl,
+                                 int part_off, const Twiddles &tw, cudaStream_t st);
+// L4 over src (T1 after separate L2, L3; T2 after the fused pass) -> Xs
+cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs b, int l0,
+                               int nl, const Twiddles &tw, cudaStream_t st);
 cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs b, float2 *dP,
                                  cudaStream_t st);
 

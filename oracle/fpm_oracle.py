@@ -346,3 +346,88 @@ def imresize_bicubic(img, scale: int):
     t = (img[ir, :] * wr[:, :, None]).sum(axis=1)            # (n_out_r, n_c)
     out = (t[:, ic] * wc[None, :, :]).sum(axis=2)            # (n_out_r, n_out_c)
     return out
+
+
+# ---------------------------------------------------------------------------
+# LED illumination geometry (restated for checking the device helper)
+# ---------------------------------------------------------------------------
+
+def spiral_grid_order(n: int):
+    """1-based (i, j) grid positions in the centre-out visiting order.
+
+    ``codes_v2/func_ware/init_environment_rgb.m:111-133``: start at the centre
+    ((n+1)/2, (n+1)/2); at every step, if the cell one turn further
+    (direction + 1, with (sin, cos)(pi/2 * direction) giving (di, dj)) is
+    unvisited, take that direction; then step once in the current direction.
+    ``n`` must be odd (the centre index is fractional otherwise).
+    """
+    import math
+    seen = np.zeros((n + 1, n + 1), bool)          # 1-based
+    i = j = (n + 1) // 2
+    seen[i, j] = True
+    order = [(i, j)]
+    d = 0
+    while len(order) < n * n:
+        d2 = d + 1
+        i2 = int(round(i + math.sin(math.pi / 2 * d2)))
+        j2 = int(round(j + math.cos(math.pi / 2 * d2)))
+        if not seen[i2, j2]:
+            d = d2
+        i = int(round(i + math.sin(math.pi / 2 * d)))
+        j = int(round(j + math.cos(math.pi / 2 * d)))
+        seen[i, j] = True
+        order.append((i, j))
+    return order
+
+
+def led_geometry(grid: int, h: int, pratio: int, wavelength_um: float, led_pitch_um: float,
+                 led_height_um: float, camera_pixel_um: float, magnification: float,
+                 sample_dx_um: float = -0.0, sample_dy_um: float = -0.0):
+    """ledIdx (L, 2) int32 rows (kl, kt) in spiral order, plus the (i, j) order.
+
+    Python floats are IEEE doubles and are evaluated one operation at a time in
+    MATLAB's left-to-right order (no fused multiply-add):
+
+    * ``init_environment_rgb.m:15-21,31-46``: D_pixel = pixel_size / mag, the
+      high-res frequency axis ``(k - NN/2) ./ (N * D_pixel) .* (2*pi)``;
+    * ``:64-68,82-90``: per grid cell (i, j), ``a = -vled(i)*D_led + objdx``,
+      ``b = -hled(j)*D_led + objdy``, ``den = sqrt(a^2 + b^2 + h^2)``,
+      ``v = a/den``, ``u = -b/den``, then u and v swapped;
+    * ``:98-106``: uo / vo = first index of the minimum of
+      ``|F - k_lamuda * u|`` / ``|F - k_lamuda * v|`` (``find(x == min(x))``,
+      first on ties), with ``k_lamuda = 2*pi/lamuda``;
+    * ``main_run_FPM.m:21-31,51-55``: LEDs in spiral order,
+      ``kl = uo - N/2``, ``kt = vo - M/2``.
+    """
+    import math
+    NN = h * pratio
+    D_pixel = camera_pixel_um / magnification
+    ND = h * D_pixel
+    two_pi = 2 * math.pi
+    F = [((k - NN // 2) / ND) * two_pi for k in range(NN)]
+    k_lamuda = two_pi / wavelength_um
+    cen = (grid - 1) / 2
+
+    def nearest(x):
+        best, bi = None, 0
+        for k, f in enumerate(F):
+            d = abs(f - x)
+            if best is None or d < best:
+                best, bi = d, k
+        return bi + 1
+
+    order = spiral_grid_order(grid)
+    out = []
+    for (i, j) in order:
+        vv = (i - 1) - cen
+        hh = (j - 1) - cen
+        a = (-vv) * led_pitch_um + sample_dx_um
+        b = (-hh) * led_pitch_um + sample_dy_um
+        den = math.sqrt(a * a + b * b + led_height_um * led_height_um)
+        v0 = a / den
+        u0 = (-b) / den
+        u, v = v0, u0
+        uo = nearest(k_lamuda * u)
+        vo = nearest(k_lamuda * v)
+        out.append((uo - h // 2, vo - h // 2))
+    return np.asarray(out, np.int32), np.asarray(order, np.int32)

@@ -233,6 +233,29 @@ def test_fft2_large_lines_device(engine):
         assert np.abs(got - ref).max() < 1e-4 * np.abs(vals).sum(), n
 
 
+def test_fft2_dense_separable_16384(engine):
+    """Every output of a dense 16384 x 16384 transform: a separable input a b^T has the
+    separable transform fft(a) fft(b)^T (numpy, FP64), compared on the device."""
+    import torch
+    n = 16384
+    rng = np.random.default_rng(7)
+    a = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    for sign, A, B in ((-1, np.fft.fft(a), np.fft.fft(b)),
+                       (+1, np.fft.ifft(a) * n, np.fft.ifft(b) * n)):
+        x = torch.outer(torch.from_numpy(a.astype(np.complex64)).cuda(),
+                        torch.from_numpy(b.astype(np.complex64)).cuda())
+        y = engine.fft2(x, sign)
+        del x
+        ref = torch.outer(torch.from_numpy(A.astype(np.complex64)).cuda(),
+                          torch.from_numpy(B.astype(np.complex64)).cuda())
+        err = (torch.linalg.vector_norm(torch.view_as_real(y - ref), dtype=torch.float64)
+               / torch.linalg.vector_norm(torch.view_as_real(ref), dtype=torch.float64)).item()
+        del y, ref
+        torch.cuda.empty_cache()
+        assert err < 2e-6 * np.log2(n) / 8, (sign, err)
+
+
 def test_unsupported_sizes_are_refused(engine):
     rng = np.random.default_rng(1)
     h = 48

@@ -185,6 +185,31 @@ def test_led_indices_centre_led():
     assert led.min() >= 1 and (led + 127).max() <= H
 
 
+def test_geometry_restatements_agree():
+    """The oracle's statement-by-statement geometry against the generator's."""
+    assert orc.spiral_grid_order(3) == [(2, 2), (3, 2), (3, 1), (2, 1), (1, 1), (1, 2), (1, 3),
+                                        (2, 3), (3, 3)]
+    for n in (5, 11, 19):
+        assert orc.spiral_grid_order(n) == synth.spiral_order(n)
+    for grid, h, p in ((5, 64, 2), (11, 128, 4), (19, 256, 8)):
+        o = synth.Optics(led_grid=grid)
+        led, order = orc.led_geometry(grid, h, p, o.wavelength_um, o.led_pitch_mm * 1000,
+                                      o.led_height_mm * 1000, o.camera_pixel_um, o.magnification)
+        np.testing.assert_array_equal(led, synth.led_indices(h, p, o))
+        assert order.shape == (grid * grid, 2)
+
+
+def test_geometry_off_axis_sample_area():
+    """objdx / objdy shift every illumination angle: the centre LED's crop moves off centre."""
+    o = synth.Optics(led_grid=5)
+    args = (5, 128, 4, o.wavelength_um, o.led_pitch_mm * 1000, o.led_height_mm * 1000,
+            o.camera_pixel_um, o.magnification)
+    c, _ = orc.led_geometry(*args)
+    s, _ = orc.led_geometry(*args, sample_dx_um=3000.0, sample_dy_um=-2000.0)
+    assert tuple(c[0]) == (512 // 2 + 1 - 64, 512 // 2 + 1 - 64)
+    assert s[0, 0] > c[0, 0] and s[0, 1] > c[0, 1]   # u <- +dx, v <- -(-dy) after the swap
+
+
 def test_bicubic_restatements_agree_and_keep_constants():
     rng = np.random.default_rng(7)
     img = rng.random((12, 12))
