@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace fpm {
 
@@ -25,22 +26,13 @@ struct Box {
 };
 
 // ---- low-resolution (per-LED) stages -------------------------------------
-cudaError_t launch_crop_pupil(const float2 *S, const float2 *P, const int2 *led, int z_off,
-                              int nb, int h, int H, float2 *T, cudaStream_t st);
 int feature_grad_blocks_per_image(int h);
 cudaError_t launch_feature_grad(const float2 *Z, StackView Y, int z_off, int nb, int h,
                                 int pratio, float2 *out, double *loss_part, cudaStream_t st);
-cudaError_t launch_stitch_gather(const float2 *X, const float2 *P, const int2 *led, int z_off,
-                                 int nb, int h, int H, Box box, float2 *G, cudaStream_t st);
-cudaError_t launch_pupil_grad(const float2 *S, const float2 *X, const int2 *led, int z_off,
-                              int nb, int h, int H, float2 *dP, cudaStream_t st);
 
 // ---- large-array stages ---------------------------------------------------
-cudaError_t launch_rmsprop_object(const float2 *g, float2 *O, float *m, size_t n, float lr,
-                                  float beta, float eps, cudaStream_t st);
 cudaError_t launch_rmsprop_pupil(const float2 *dP, float2 *P, float *m, const float *P0, int n,
                                  float lr, float beta, float eps, float am, cudaStream_t st);
-cudaError_t launch_centre_spectrum(const float2 *S, int H, float2 *out, cudaStream_t st);
 cudaError_t launch_centre_in_place(float2 *S, int H, cudaStream_t st);
 // out[c*ldo + r] = in[r*ldi + c] (r < rows, c < cols); conj_scale != 0 conjugates and scales.
 cudaError_t launch_transpose(const float2 *in, size_t ldi, float2 *out, size_t ldo, int rows,
@@ -52,5 +44,20 @@ cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cud
 cudaError_t launch_stack_minmax(const uint16_t *p, size_t n, unsigned *minmax, cudaStream_t st);
 cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *minmax, float *out,
                              cudaStream_t st);
+
+// ---- LED geometry (FP64) -----------------------------------------------------
+struct LedGeom {
+    int grid = 0, h = 0, NN = 0;     // LEDs per side, low-res side, high-res side
+    double pitch = 0, height = 0;    // D_led, LED-plane height (um)
+    double dx = 0, dy = 0;           // objdx, objdy (um)
+    double k_lamuda = 0;             // 2 pi / lambda
+    double ND = 0;                   // N * D_pixel
+    double two_pi = 0;               // 2 pi
+};
+// (i, j) 1-based grid cells of an odd n x n array in the centre-out spiral order
+void spiral_grid_order(int n, std::vector<int2> &order);
+// led_idx[2l], led_idx[2l+1] = (kl, kt) of the LED at grid cell pos[l]
+cudaError_t launch_led_nearest(const int2 *pos, int n_leds, const LedGeom &p, int32_t *led_idx,
+                               cudaStream_t st);
 
 }  // namespace fpm

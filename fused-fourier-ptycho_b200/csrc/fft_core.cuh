@@ -1,10 +1,10 @@
 // Block-level FFT building blocks (power-of-two lengths 16 .. 16384).
 //
-// A line of N complex values sits in shared memory in natural order at
-// swizzled addresses (swz below).  T = N/16 threads cooperate on one line; each
-// stage of a radix-R Stockham (self-sorting) decomposition has every thread
-// load 16 values, apply the stage twiddles, run 16/R in-register DFTs of
-// length R, and store 16 values:
+// T = N/16 threads cooperate on a line of N complex values, each holding 16 of
+// them in registers; each stage of a radix-R Stockham (self-sorting)
+// decomposition applies the stage twiddles, runs 16/R in-register DFTs of
+// length R, and exchanges values through shared memory (swizzled addresses,
+// swz below):
 //
 //   butterfly i in [0, N/R), k = i mod p (p = product of the radices done):
 //     inputs   x[i + r N/R]                          r = 0..R-1
@@ -15,7 +15,8 @@
 // XOR swizzle l ^ ((l >> 4) & 15) makes the strided stores of the first stage
 // and all contiguous loads bank-conflict free.  Stage twiddles W_N^m come from
 // a two-level table W_N^m = hi[m >> 7] * lo[m & 127] held in shared memory
-// (about 1.5 ulp), built on the host in double precision.
+// (about 1.5 ulp), built on the host in double precision; within a butterfly the
+// powers W^(r m) beyond r = 1, 2, 4, 8 are products of table values.
 #pragma once
 
 #include "common.cuh"
@@ -25,10 +26,18 @@ namespace fft {
 
 __device__ __forceinline__ int swz(int l) { return l ^ ((l >> 4) & 15); }
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// Complex arithmetic on packed float pairs: one sm_100 two-lane instruction
+// (FADD2 / FMUL2 / FFMA2) per complex add and two per complex product, half the
+// scalar count.  Each lane is an ordinary IEEE round-to-nearest operation.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.f, -1.f), a);   // a - b, exact negation
+}
+// w * v = (w.x v.x - w.y v.y, w.x v.y + w.y v.x); w is the factor that is
+// broadcast (a twiddle or a constant), v the data.
+__device__ __forceinline__ float2 cmulf(float2 w, float2 v) {
+    const float2 t = __fmul2_rn(make_float2(w.x, w.x), v);
+    return __ffma2_rn(make_float2(-w.y, w.y), make_float2(v.y, v.x), t);
 }
 
 // cos / sin of 2 pi k / 16, k = 0..4 (the rest follow by symmetry)
@@ -57,7 +66,7 @@ __device__ __forceinline__ float2 mul_w16(float2 v) {
     } else if constexpr (K == 4) {  // exp(DIR i pi/2) = DIR * i
         return DIR < 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
     } else {
-        return cmulf(v, w16<DIR>(K));
+        return cmulf(w16<DIR>(K), v);
     }
 }
 
@@ -95,7 +104,7 @@ __device__ __forceinline__ void dft(float2 (&v)[R]) {
                     } else if (kk == 4) {
                         t = mul_w16<DIR, 4>(t);
                     } else {
-                        t = cmulf(t, w16<DIR>(kk));
+                        t = cmulf(w16<DIR>(kk), t);
                     }
                     a[i + j] = cadd(u, t);
                     a[i + j + len / 2] = csub(u, t);
@@ -115,53 +124,40 @@ __device__ __forceinline__ float2 twiddle(const float2 *hi, const float2 *lo, in
     return w;
 }
 
-// One radix-R stage on a line of N values; t in [0, N/16).
-template <int N, int DIR, int P, int R>
-__device__ __forceinline__ void stage(float2 *s, const float2 *hi, const float2 *lo, int t) {
-    constexpr int T = N / 16;
-    constexpr int NB = 16 / R;
-    float2 v[NB][R];
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        const int i = t + j * T;
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[j][r] = s[swz(i + r * (N / R))];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-        const int i = t + j * T;
-        const int k = i & (P - 1);
-        if constexpr (P > 1) {
-#pragma unroll
-            for (int r = 1; r < R; ++r)
-                v[j][r] = cmulf(v[j][r], twiddle<DIR>(hi, lo, r * k * (N / (P * R))));
+// u[r] *= W^(r m1) for r = 1 .. R-1.  Only W^m1, W^2m1, W^4m1, W^8m1 come from the
+// table (two shared-memory loads each); the other powers are products of those
+// (at most three products deep, a few ulp), which takes most of the twiddle loads
+// and their bank conflicts off the shared-memory pipe.
+template <int R, int DIR>
+__device__ __forceinline__ void apply_twiddles(float2 (&u)[R], const float2 *hi, const float2 *lo,
+                                               int m1) {
+    const float2 w1 = twiddle<DIR>(hi, lo, m1);
+    u[1] = cmulf(w1, u[1]);
+    if constexpr (R >= 4) {
+        const float2 w2 = twiddle<DIR>(hi, lo, 2 * m1);
+        u[2] = cmulf(w2, u[2]);
+        const float2 w3 = cmulf(w1, w2);
+        u[3] = cmulf(w3, u[3]);
+        if constexpr (R >= 8) {
+            const float2 w4 = twiddle<DIR>(hi, lo, 4 * m1);
+            u[4] = cmulf(w4, u[4]);
+            u[5] = cmulf(cmulf(w1, w4), u[5]);
+            u[6] = cmulf(cmulf(w2, w4), u[6]);
+            u[7] = cmulf(cmulf(w3, w4), u[7]);
+            if constexpr (R >= 16) {
+                const float2 w8 = twiddle<DIR>(hi, lo, 8 * m1);
+                u[8] = cmulf(w8, u[8]);
+                u[9] = cmulf(cmulf(w1, w8), u[9]);
+                u[10] = cmulf(cmulf(w2, w8), u[10]);
+                u[11] = cmulf(cmulf(w3, w8), u[11]);
+                const float2 w12 = cmulf(w4, w8);
+                u[12] = cmulf(w12, u[12]);
+                u[13] = cmulf(cmulf(w1, w12), u[13]);
+                u[14] = cmulf(cmulf(w2, w12), u[14]);
+                u[15] = cmulf(cmulf(w3, w12), u[15]);
+            }
         }
-        dft<R, DIR>(v[j]);
-        const int base = (i - k) * R + k;
-#pragma unroll
-        for (int r = 0; r < R; ++r) s[swz(base + r * P)] = v[j][r];
     }
-    __syncthreads();
-}
-
-template <int N, int DIR, int P>
-__device__ __forceinline__ void stages(float2 *s, const float2 *hi, const float2 *lo, int t) {
-    if constexpr (P < N) {
-        constexpr int REM = N / P;
-        constexpr int R = REM >= 16 ? 16 : REM;
-        stage<N, DIR, P, R>(s, hi, lo, t);
-        stages<N, DIR, P * R>(s, hi, lo, t);
-    }
-}
-
-// Unnormalised DFT of the N values at s (swizzled, natural order), in place.
-// Must be reached by every thread of the block (it synchronises); threads with
-// t >= N/16 of a multi-line block run their own line.
-template <int N, int DIR>
-__device__ __forceinline__ void line_fft(float2 *s, const float2 *hi, const float2 *lo, int t) {
-    static_assert(N >= 16 && (N & (N - 1)) == 0, "power-of-two length >= 16");
-    stages<N, DIR, 1>(s, hi, lo, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -198,11 +194,7 @@ __device__ __forceinline__ void stages_regs(float2 (&v)[16], float2 *s, const fl
         for (int r = 0; r < R; ++r) u[r] = v[j + r * NB];
         const int i = t + j * T;
         const int k = i & (P - 1);
-        if constexpr (P > 1) {
-#pragma unroll
-            for (int r = 1; r < R; ++r)
-                u[r] = cmulf(u[r], twiddle<DIR>(hi, lo, r * k * (N / (P * R))));
-        }
+        if constexpr (P > 1) apply_twiddles<R, DIR>(u, hi, lo, k * (N / (P * R)));
         dft<R, DIR>(u);
         if constexpr (LAST) {
 #pragma unroll
@@ -236,19 +228,6 @@ __device__ __forceinline__ void load_twiddles(float2 *s_hi, float2 *s_lo, const 
     for (int i = threadIdx.x; i < n_hi; i += blockDim.x) s_hi[i] = g_hi[i];
     for (int i = threadIdx.x; i < n_lo; i += blockDim.x) s_lo[i] = g_lo[i];
 }
-
-// CTA shape for lines of length N: T = N/16 threads per line, LPC lines per CTA
-// (64 KiB of line data per CTA for N <= 8192, one 128 KiB line for N = 16384).
-template <int N>
-struct Geo {
-    static constexpr int T = N / 16;
-    static constexpr int LPC = (N * 8 >= 64 * 1024) ? 1 : (64 * 1024) / (N * 8);
-    static constexpr int THREADS = T * LPC;
-    static constexpr int LINE_BYTES = LPC * N * 8;
-    static constexpr int TW_BYTES = 2 * 128 * 8;
-    static constexpr int NHI = N >= 128 ? N / 128 : 1;
-    static constexpr int NLO = N >= 128 ? 128 : N;
-};
 
 // CTA shape for the register-resident kernels: LPC lines of length N per CTA,
 // T = N/16 threads per line, lines padded in shared memory by PAD values so that

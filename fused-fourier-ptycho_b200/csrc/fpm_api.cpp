@@ -148,6 +148,7 @@ struct fpm_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaEvent_t entry = nullptr;   // orders device-memory calls after the legacy default stream
     size_t mem_limit = 0;
     std::string err;
     FftEngine fft;
@@ -596,6 +597,12 @@ fpm_status fpm_create(fpm_context **out, const fpm_device_opts *opts) {
         }
         ctx->own_stream = true;
     }
+    if (cudaEventCreateWithFlags(&ctx->entry, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return FPM_ERR_CUDA;
+    }
     *out = ctx;
     return FPM_OK;
 }
@@ -605,8 +612,20 @@ void fpm_destroy(fpm_context *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->fft.release();
+    if (ctx->entry) cudaEventDestroy(ctx->entry);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+// Device-memory inputs are usually written on the legacy default stream (a MATLAB
+// gpuArray, a torch tensor on torch's default stream), which a non-blocking context
+// stream does not wait for: every call that reads device memory first makes the
+// context's stream wait for the work already queued there.  Work on other streams
+// must be complete before the call (the caller's responsibility, as in any CUDA API).
+static fpm_status order_after_default_stream(fpm_context *ctx) {
+    FPM_CK(cudaEventRecord(ctx->entry, cudaStreamLegacy));
+    FPM_CK(cudaStreamWaitEvent(ctx->stream, ctx->entry, 0));
+    return FPM_OK;
 }
 
 // LED corners on the host (the crop boxes are planned from them), validated.
@@ -651,6 +670,10 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
                 return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "result pointer %d is not 16-byte aligned",
                             i);
         }
+    }
+    if (dev) {
+        rc = order_after_default_stream(ctx);
+        if (rc != FPM_OK) return rc;
     }
     std::vector<int32_t> led_host;
     rc = fetch_leds(ctx, p, s, led_host);
@@ -802,6 +825,10 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
         if (!dev && !is_host_ptr(outs[i]))
             return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output %d is not host memory", i);
     }
+    if (dev) {
+        rc = order_after_default_stream(ctx);
+        if (rc != FPM_OK) return rc;
+    }
     std::vector<int32_t> led_host;
     rc = fetch_leds(ctx, p, s, led_host);
     if (rc != FPM_OK) return rc;
@@ -870,6 +897,10 @@ fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, in
     }
     if (ctx->mem_limit && !dev && bytes > ctx->mem_limit)
         return fail(ctx, FPM_ERR_OUT_OF_MEMORY, "fft2 needs %zu bytes", bytes);
+    if (dev) {
+        const fpm_status rc = order_after_default_stream(ctx);
+        if (rc != FPM_OK) return rc;
+    }
     cudaStream_t st = ctx->stream;
     const float2 *src = reinterpret_cast<const float2 *>(in);
     float2 *dst = reinterpret_cast<float2 *>(out);
@@ -881,6 +912,56 @@ fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, in
     FPM_CK(ctx->fft.run(src, dst, n, count, direction < 0 ? kForward : kInverse, st));
     if (!dev) FPM_CK(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, st));
     FPM_CK(cudaStreamSynchronize(st));
+    return FPM_OK;
+}
+
+fpm_status fpm_led_indices(fpm_context *ctx, const fpm_led_geometry *geo, int32_t *led_idx,
+                           int32_t *grid_pos) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (!geo || !led_idx) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "geo or led_idx is NULL");
+    const fpm_led_geometry &g = *geo;
+    if (g.grid < 1 || g.grid > 255 || g.grid % 2 == 0)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "grid = %d: an odd LED count per side, 1..255",
+                    g.grid);
+    if (g.h < 2 || g.h % 2 || g.pratio < 1 || (long long)g.h * g.pratio > (1 << 20))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "h = %d, pratio = %d", g.h, g.pratio);
+    const double pos[] = {g.wavelength_um, g.led_height_um, g.camera_pixel_um, g.magnification};
+    for (double v : pos)
+        if (!(v > 0) || !std::isfinite(v))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT,
+                        "wavelength, LED height, camera pixel and magnification must be > 0");
+    if (!std::isfinite(g.led_pitch_um) || !std::isfinite(g.sample_dx_um) ||
+        !std::isfinite(g.sample_dy_um))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "non-finite LED pitch or sample offset");
+    if (!is_host_ptr(led_idx) || (grid_pos && !is_host_ptr(grid_pos)))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "led_idx / grid_pos must be host memory");
+    FPM_CK(cudaSetDevice(ctx->device));
+    std::vector<int2> order;
+    spiral_grid_order(g.grid, order);
+    const int L = g.grid * g.grid;
+    if ((int)order.size() != L) return fail(ctx, FPM_ERR_INTERNAL, "spiral order incomplete");
+    LedGeom p;
+    p.grid = g.grid;
+    p.h = g.h;
+    p.NN = g.h * g.pratio;
+    p.pitch = g.led_pitch_um;
+    p.height = g.led_height_um;
+    p.dx = g.sample_dx_um;
+    p.dy = g.sample_dy_um;
+    p.two_pi = 2 * M_PI;
+    p.k_lamuda = p.two_pi / g.wavelength_um;          // k_lamuda = 2*pi/lamuda
+    const double d_pixel = g.camera_pixel_um / g.magnification;   // D_pixel
+    p.ND = (double)g.h * d_pixel;                       // N * D_pixel
+    cudaStream_t st = ctx->stream;
+    FPM_CK(ctx->led.ensure((size_t)L * 16));
+    int2 *d_pos = ctx->led.as<int2>();
+    int32_t *d_idx = reinterpret_cast<int32_t *>(d_pos + L);
+    FPM_CK(cudaMemcpyAsync(d_pos, order.data(), (size_t)L * 8, cudaMemcpyHostToDevice, st));
+    FPM_CK(launch_led_nearest(d_pos, L, p, d_idx, st));
+    FPM_CK(cudaMemcpyAsync(led_idx, d_idx, (size_t)L * 8, cudaMemcpyDeviceToHost, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    if (grid_pos) std::memcpy(grid_pos, order.data(), (size_t)L * 8);
     return FPM_OK;
 }
 
@@ -899,6 +980,10 @@ fpm_status fpm_normalise_stack(fpm_context *ctx, const uint16_t *counts, size_t 
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not device memory");
     if (!dev && (!is_host_ptr(counts) || !is_host_ptr(amplitude)))
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not host memory");
+    if (dev) {
+        const fpm_status rc = order_after_default_stream(ctx);
+        if (rc != FPM_OK) return rc;
+    }
     const uint16_t *src = counts;
     float *dst = amplitude;
     if (!dev) {

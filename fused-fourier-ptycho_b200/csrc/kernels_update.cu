@@ -1,18 +1,15 @@
-// Large-array stages (object update, spectrum output, initial object) and the
-// small reductions / ingest kernels.
+// Pupil update, spectrum output, initial object, tiled transposes, and the small
+// reductions / ingest kernels.  (The object's RMSprop lives in the column pass of
+// pipeline.cu.)
 #include "common.cuh"
 #include "engine.h"
 
 namespace fpm {
 
-// ---------------------------------------------------------------------------
-// RMSprop on the object (constrained_RMSprop_both, first half,
-// cuFPM_v3/cuda/kernels.cuh:364-382):
-//   mu = beta*m + (1-beta)|g|²,  w -= g * lr/(sqrt(mu)+eps),  m = mu.
-// The reference also zeroes g; here the next stitch rewrites the whole
-// gradient spectrum, so that store is dropped.  Two complex pixels per thread
-// with 128-bit loads of g and O and a 64-bit load of m.
-// ---------------------------------------------------------------------------
+// One RMSprop step (constrained_RMSprop_both, cuFPM_v3/cuda/kernels.cuh:364-382 for
+// the object, :384-393 for the pupil): mu = beta*m + (1-beta)|g|^2,
+// w -= g * lr/(sqrt(mu)+eps), m = mu.  The column pass of pipeline.cu applies the
+// same expression to the object.
 __device__ __forceinline__ void rms_one(float gr, float gi, float &wr, float &wi, float &m,
                                         float lr, float beta, float omb, float eps) {
     float mu = gr * gr + gi * gi;
@@ -21,37 +18,6 @@ __device__ __forceinline__ void rms_one(float gr, float gi, float &wr, float &wi
     wr -= gr * sq;
     wi -= gi * sq;
     m = mu;
-}
-
-__global__ void __launch_bounds__(256) k_rmsprop_object(const float4 *__restrict__ g,
-                                                         float4 *__restrict__ O,
-                                                         float2 *__restrict__ m, size_t n2,
-                                                         float lr, float beta, float eps) {
-    const float omb = 1.0f - beta;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
-         i += (size_t)gridDim.x * blockDim.x) {
-        const float4 gv = g[i];
-        float4 w = O[i];
-        float2 mv = m[i];
-        rms_one(gv.x, gv.y, w.x, w.y, mv.x, lr, beta, omb, eps);
-        rms_one(gv.z, gv.w, w.z, w.w, mv.y, lr, beta, omb, eps);
-        O[i] = w;
-        m[i] = mv;
-    }
-}
-
-cudaError_t launch_rmsprop_object(const float2 *g, float2 *O, float *m, size_t n, float lr,
-                                  float beta, float eps, cudaStream_t st) {
-    if (n % 2) return cudaErrorInvalidValue;
-    const size_t n2 = n / 2;
-    size_t gx = (n2 + 255) / 256;
-    const size_t cap = (size_t)kB200SMs * 8 * 8;
-    if (gx > cap) gx = cap;
-    k_rmsprop_object<<<(unsigned)gx, 256, 0, st>>>(reinterpret_cast<const float4 *>(g),
-                                                   reinterpret_cast<float4 *>(O),
-                                                   reinterpret_cast<float2 *>(m), n2, lr, beta,
-                                                   eps);
-    return cudaGetLastError();
 }
 
 // RMSprop on the pupil plus the amplitude box constraint
@@ -84,30 +50,6 @@ cudaError_t launch_rmsprop_pupil(const float2 *dP, float2 *P, float *m, const fl
     int gx = (n + 255) / 256;
     if (gx > kB200SMs * 8) gx = kB200SMs * 8;
     k_rmsprop_pupil<<<gx, 256, 0, st>>>(dP, P, m, P0, n, lr, beta, eps, am);
-    return cudaGetLastError();
-}
-
-// out = fftshift(S) (even H: swap halves on both axes).
-__global__ void __launch_bounds__(256) k_centre_spectrum(const float2 *__restrict__ S, int H,
-                                                          float2 *__restrict__ out) {
-    const size_t total = (size_t)H * H;
-    const int hh = H >> 1;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
-         q += (size_t)gridDim.x * blockDim.x) {
-        const int r = (int)(q % H);
-        const int c = (int)(q / H);
-        const int rs = r + hh >= H ? r + hh - H : r + hh;
-        const int cs = c + hh >= H ? c + hh - H : c + hh;
-        out[q] = S[(size_t)cs * H + rs];
-    }
-}
-
-cudaError_t launch_centre_spectrum(const float2 *S, int H, float2 *out, cudaStream_t st) {
-    const size_t total = (size_t)H * H;
-    size_t gx = (total + 255) / 256;
-    const size_t cap = (size_t)kB200SMs * 8 * 8;
-    if (gx > cap) gx = cap;
-    k_centre_spectrum<<<(unsigned)gx, 256, 0, st>>>(S, H, out);
     return cudaGetLastError();
 }
 

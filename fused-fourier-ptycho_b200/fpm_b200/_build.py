@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(INCLUDE),
                   "--expt-relaxed-constexpr"]
 LIBS_SOURCES = ["kernels_lowres.cu", "kernels_update.cu", "fft_own.cu", "fpm_api.cpp",
-                "noalloc.cu", "pipeline.cu"]
+                "noalloc.cu", "pipeline.cu", "geometry.cu"]
 LINK_LIBS = ["-lcudart"]
 
 
@@ -67,7 +67,25 @@ def build(verbose: bool = False) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link of libfpm.so failed:\n{r.stdout}\n{r.stderr}")
+    build_cli(verbose)
     return LIB
+
+
+def build_cli(verbose: bool = False) -> Path:
+    """fpm_cli, the file-driven front end (host C++ over the C ABI), next to libfpm.so."""
+    src = CSRC / "fpm_cli.cpp"
+    if CLI.exists() and CLI.stat().st_mtime > max(src.stat().st_mtime, LIB.stat().st_mtime,
+                                                  (INCLUDE / "fpm.h").stat().st_mtime):
+        return CLI
+    cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", str(INCLUDE), str(src), "-o", str(CLI),
+           "-L", str(LIBDIR), "-lfpm", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build of fpm_cli failed:\n{r.stdout}\n{r.stderr}")
+    return CLI
 
 
 if __name__ == "__main__":

@@ -36,7 +36,8 @@ LOSS_ANISOTROPIC = 0
 # Every symbol include/fpm.h declares.
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
-            "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2"]
+            "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
+            "fpm_led_indices"]
 
 
 class FpmError(RuntimeError):
@@ -49,6 +50,15 @@ class FpmError(RuntimeError):
 class DeviceOpts(C.Structure):
     _fields_ = [("device", C.c_int32), ("reserved0", C.c_int32),
                 ("mem_limit_bytes", C.c_size_t), ("stream", C.c_void_p)]
+
+
+class LedGeometry(C.Structure):
+    """fpm_led_geometry (include/fpm.h); lengths in micrometres."""
+    _fields_ = [("grid", C.c_int32), ("h", C.c_int32), ("pratio", C.c_int32),
+                ("reserved0", C.c_int32), ("wavelength_um", C.c_double),
+                ("led_pitch_um", C.c_double), ("led_height_um", C.c_double),
+                ("camera_pixel_um", C.c_double), ("magnification", C.c_double),
+                ("sample_dx_um", C.c_double), ("sample_dy_um", C.c_double)]
 
 
 class Problem(C.Structure):
@@ -106,6 +116,8 @@ def load_library(path: str | Path | None = None):
     lib.fpm_fft2.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                              C.c_int32]
     lib.fpm_fft2.restype = C.c_int
+    lib.fpm_led_indices.argtypes = [C.c_void_p, C.POINTER(LedGeometry), C.c_void_p, C.c_void_p]
+    lib.fpm_led_indices.restype = C.c_int
     lib.fpm_abi_version.argtypes = []
     lib.fpm_abi_version.restype = C.c_int32
     if path is None:
@@ -119,6 +131,17 @@ def load_library(path: str | Path | None = None):
 
 def _is_torch(x) -> bool:
     return type(x).__module__.startswith("torch")
+
+
+def _inputs_ready(*xs):
+    """Wait for the torch work that produced CUDA tensor inputs (copies made by the
+    layout helpers included): the library runs on its own stream, which orders itself
+    after the legacy default stream only, not after a torch side stream."""
+    import torch
+    for x in xs:
+        if _is_torch(x) and x.is_cuda:
+            torch.cuda.current_stream(x.device).synchronize()
+            return
 
 
 def _colmajor(x, dtype):
@@ -244,6 +267,7 @@ class Engine:
             sp, s = _empty_like_layout((H, H), np.complex64, like)
         lp, loss = _empty_like_layout((max(int(epochs), 1),), np.float64, like)
         res = Result(object=op, spectrum=sp, pupil=pp, loss=lp)
+        _inputs_ready(*keep)
         self._check(self.solve_raw(prob, res))
         del keep
         return {"object": o, "pupil": p, "spectrum": s, "loss": loss[: int(epochs)]}
@@ -258,6 +282,7 @@ class Engine:
         op, o = _empty_like_layout((H, H), np.complex64, like)
         pp, p = _empty_like_layout((h, h), np.complex64, like)
         lp, loss = _empty_like_layout((1,), np.float64, like)
+        _inputs_ready(*keep)
         self._check(self.gradients_raw(prob, op, pp, lp))
         del keep
         return o, p, float(loss[0])
@@ -270,6 +295,7 @@ class Engine:
             out = torch.empty_like(y)
             n = int(x.shape[0])
             cnt = int(x.shape[2]) if x.dim() == 3 else 1
+            _inputs_ready(y)
             self._check(self.lib.fpm_fft2(self._ctx, y.data_ptr(), out.data_ptr(), n, cnt,
                                           direction, MEM_DEVICE if y.is_cuda else MEM_HOST))
             return out.permute(*reversed(range(x.dim())))
@@ -281,6 +307,23 @@ class Engine:
                                       direction, MEM_HOST))
         return out
 
+    def led_indices(self, grid, h, pratio, wavelength_um, led_pitch_um, led_height_um,
+                    camera_pixel_um, magnification, sample_dx_um=-0.0, sample_dy_um=-0.0):
+        """ledIdx of a grid x grid LED array in spiral order, computed on the device (FP64).
+
+        Returns (led, order): led (L, 2) int32 rows (kl, kt) -- MATLAB's ledIdx transposed --
+        and order (L, 2) int32 rows (i, j), the 1-based grid cell of each LED.
+        """
+        g = LedGeometry(int(grid), int(h), int(pratio), 0, float(wavelength_um),
+                        float(led_pitch_um), float(led_height_um), float(camera_pixel_um),
+                        float(magnification), float(sample_dx_um), float(sample_dy_um))
+        L = int(grid) * int(grid)
+        led = np.empty((L, 2), np.int32)
+        order = np.empty((L, 2), np.int32)
+        self._check(self.lib.fpm_led_indices(self._ctx, C.byref(g), led.ctypes.data,
+                                             order.ctypes.data))
+        return led, order
+
     def normalise_stack(self, counts):
         """Amplitude sqrt((I-min)/(max-min)) of a uint16 stack, same shape, float32."""
         if _is_torch(counts):
@@ -288,6 +331,7 @@ class Engine:
             x = counts.contiguous()
             out = torch.empty(x.shape, dtype=torch.float32, device=x.device)
             mem = MEM_DEVICE if x.is_cuda else MEM_HOST
+            _inputs_ready(x)
             self._check(self.lib.fpm_normalise_stack(self._ctx, x.data_ptr(), x.numel(),
                                                      out.data_ptr(), mem))
             return out

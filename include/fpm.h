@@ -176,6 +176,32 @@ fpm_status fpm_feature_gradient_noalloc(const float *z, const float *amplitude, 
                                         int32_t n_images, int32_t pratio, float *gradient,
                                         double *loss, void *stream);
 
+/* Geometry of a square LED array (codes_v2/func_ware/init_environment_rgb.m:1-25). */
+typedef struct fpm_led_geometry {
+    int32_t grid;             /* LEDs per side (ledMM = ledNN), odd, 1..255 */
+    int32_t h;                /* low-res image side (pix), even */
+    int32_t pratio;           /* up-sampling ratio (MAGimg); H = h * pratio */
+    int32_t reserved0;
+    double wavelength_um;     /* lamuda */
+    double led_pitch_um;      /* D_led: distance between neighbouring LEDs */
+    double led_height_um;     /* h: distance from the LED plane to the sample */
+    double camera_pixel_um;   /* pixel_size */
+    double magnification;     /* mag */
+    double sample_dx_um;      /* objdx: offset of the reconstructed area (x * D_pixel) */
+    double sample_dy_um;      /* objdy */
+} fpm_led_geometry;
+
+/* LED corners for fpm_problem.led_idx, computed on the device in FP64: the
+   illumination angle of every LED (visited centre-out in the spiral order of
+   init_environment_rgb.m:111-133), the nearest point of the high-res frequency
+   axis (first on ties; :98-106) and the crop corner kl = uo - h/2, kt = vo - h/2
+   (codes_v2/main_run_FPM.m:21-31,51-55), bit-identical to an IEEE double
+   evaluation of those MATLAB statements.  led_idx: host array of
+   2 * grid * grid int32, (kl, kt) per LED; grid_pos (optional, host, same size):
+   the 1-based (row i, column j) grid cell of each LED. */
+fpm_status fpm_led_indices(fpm_context *ctx, const fpm_led_geometry *geo, int32_t *led_idx,
+                           int32_t *grid_pos);
+
 void fpm_destroy(fpm_context *ctx);
 
 /* Per-stage device timing (no counterpart in the reference, which only times

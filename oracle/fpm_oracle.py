@@ -404,17 +404,13 @@ def led_geometry(grid: int, h: int, pratio: int, wavelength_um: float, led_pitch
     D_pixel = camera_pixel_um / magnification
     ND = h * D_pixel
     two_pi = 2 * math.pi
-    F = [((k - NN // 2) / ND) * two_pi for k in range(NN)]
+    # elementwise IEEE double operations, one rounding each (numpy does not fuse them)
+    F = ((np.arange(NN, dtype=np.int64) - NN // 2) / ND) * two_pi
     k_lamuda = two_pi / wavelength_um
     cen = (grid - 1) / 2
 
     def nearest(x):
-        best, bi = None, 0
-        for k, f in enumerate(F):
-            d = abs(f - x)
-            if best is None or d < best:
-                best, bi = d, k
-        return bi + 1
+        return int(np.argmin(np.abs(F - x))) + 1        # argmin: first index on ties
 
     order = spiral_grid_order(grid)
     out = []

@@ -86,14 +86,14 @@ def ref_solve(lib, O0, P0c, Y, led, P0, pratio, epochs, batch, opt):
 
 
 def _wrap_case():
-    """h 48, pratio 2, LED corners at and past the spectrum edge (crops wrap modulo H)."""
+    """h 32, pratio 2, LED corners at and past the spectrum edge (crops wrap modulo H)."""
     rng = np.random.default_rng(4)
-    h, p = 48, 2
+    h, p = 32, 2
     H = h * p
     O = (0.5 + 0.5 * rng.random((H, H)) * np.exp(1j * rng.random((H, H)))).astype(np.complex64)
     P = synth.pupil_circle(h, synth.Optics(led_grid=3)).astype(np.complex64)
     led = np.array([[1, 1], [H - 10, 3], [H, H], [40, H - 20], [7, 60], [H // 2, H // 2 + 5]],
-                   np.int32)
+                   np.int32)                                     # H = 64
     Y = rng.random((len(led), h, h)).astype(np.float32)
     return O, P, Y, led, p
 

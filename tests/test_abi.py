@@ -49,8 +49,9 @@ PROBE = r"""
 #include "fpm.h"
 #define F(T, f) printf(#T "." #f " %zu\n", offsetof(T, f));
 int main(void) {
-  printf("fpm_problem %zu\nfpm_result %zu\nfpm_device_opts %zu\n", sizeof(fpm_problem),
-         sizeof(fpm_result), sizeof(fpm_device_opts));
+  printf("fpm_problem %zu\nfpm_result %zu\nfpm_device_opts %zu\nfpm_led_geometry %zu\n",
+         sizeof(fpm_problem), sizeof(fpm_result), sizeof(fpm_device_opts),
+         sizeof(fpm_led_geometry));
   F(fpm_problem, h) F(fpm_problem, n_leds) F(fpm_problem, pratio) F(fpm_problem, batch)
   F(fpm_problem, epochs) F(fpm_problem, lr) F(fpm_problem, beta) F(fpm_problem, eps)
   F(fpm_problem, pupil_margin) F(fpm_problem, lr_halve_after) F(fpm_problem, lr_decay)
@@ -59,6 +60,11 @@ int main(void) {
   F(fpm_problem, pupil_amp) F(fpm_problem, object_init)
   F(fpm_result, object) F(fpm_result, spectrum) F(fpm_result, pupil) F(fpm_result, loss)
   F(fpm_device_opts, device) F(fpm_device_opts, mem_limit_bytes) F(fpm_device_opts, stream)
+  F(fpm_led_geometry, grid) F(fpm_led_geometry, h) F(fpm_led_geometry, pratio)
+  F(fpm_led_geometry, wavelength_um) F(fpm_led_geometry, led_pitch_um)
+  F(fpm_led_geometry, led_height_um) F(fpm_led_geometry, camera_pixel_um)
+  F(fpm_led_geometry, magnification) F(fpm_led_geometry, sample_dx_um)
+  F(fpm_led_geometry, sample_dy_um)
   return 0;
 }
 """
@@ -75,8 +81,9 @@ def test_struct_layout_matches_c(tmp_path):
     assert int(got["fpm_problem"]) == C.sizeof(api.Problem)
     assert int(got["fpm_result"]) == C.sizeof(api.Result)
     assert int(got["fpm_device_opts"]) == C.sizeof(api.DeviceOpts)
+    assert int(got["fpm_led_geometry"]) == C.sizeof(api.LedGeometry)
     for cname, cls in (("fpm_problem", api.Problem), ("fpm_result", api.Result),
-                       ("fpm_device_opts", api.DeviceOpts)):
+                       ("fpm_device_opts", api.DeviceOpts), ("fpm_led_geometry", api.LedGeometry)):
         for fname, _ in cls._fields_:
             key = f"{cname}.{fname}"
             if key in got:

@@ -1,0 +1,82 @@
+"""fpm_cli, the file-driven front end for hosts without MATLAB.
+
+CPU: usage errors and unreadable inputs are refused before any device work, and
+without a device the engine's own status comes back as the exit code.  GPU: a
+solve from files equals the same solve through the library call bit for bit
+(one engine, one code path; the CLI only moves bytes).
+"""
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu, dataset, led_matlab, to_matlab_stack
+
+CLI = ROOT / "fused-fourier-ptycho_b200" / "fpm_b200" / "_lib" / "fpm_cli"
+
+
+def run(*args):
+    return subprocess.run([str(CLI), *map(str, args)], capture_output=True, text=True)
+
+
+def _inputs(tmp_path, ds, L):
+    """MATLAB-order raw files of the first L LEDs of a data set."""
+    f = {
+        "stack": tmp_path / "Y.u16", "led": tmp_path / "led.i32", "pupil": tmp_path / "P0c.c64",
+        "pupil-amp": tmp_path / "P0.f32",
+    }
+    f["stack"].write_bytes(np.transpose(ds.raw[:L], (0, 2, 1)).astype("<u2").tobytes())
+    f["led"].write_bytes(np.asarray(ds.led_idx[:L], "<i4").tobytes())          # (kl, kt) pairs
+    f["pupil"].write_bytes(np.asarray(ds.P0c, np.complex64).T.tobytes())
+    f["pupil-amp"].write_bytes(np.asarray(ds.pupil0, np.float32).T.tobytes())
+    return f
+
+
+def test_cli_usage():
+    assert CLI.exists(), "fpm_cli is built with libfpm.so"
+    r = run()
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = run("solve", "--h", "64")
+    assert r.returncode == 2 and "missing --leds" in r.stderr
+
+
+def test_cli_refuses_short_files(tmp_path):
+    ds = dataset(64, 4, 5, seed=3, aberration=True)
+    f = _inputs(tmp_path, ds, 25)
+    f["stack"].write_bytes(f["stack"].read_bytes()[:-2])
+    r = run("solve", "--h", 64, "--leds", 25, "--pratio", 4, "--batch", 6, "--epochs", 1,
+            *sum(([f"--{k}", v] for k, v in f.items()), []))
+    assert r.returncode == 2 and "fewer than" in r.stderr
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_cli_without_device_reports_engine_status(tmp_path):
+    ds = dataset(64, 4, 5, seed=3, aberration=True)
+    f = _inputs(tmp_path, ds, 25)
+    r = run("solve", "--h", 64, "--leds", 25, "--pratio", 4, "--batch", 6, "--epochs", 1,
+            *sum(([f"--{k}", v] for k, v in f.items()), []))
+    assert r.returncode == 3 + 6 and "no CUDA device" in r.stderr     # FPM_ERR_NO_DEVICE
+
+
+@pytest.mark.gpu
+def test_cli_solve_equals_library_solve(tmp_path, engine):
+    ds = dataset(64, 4, 5, seed=3, aberration=True)
+    L, E, B = 25, 2, 6
+    f = _inputs(tmp_path, ds, L)
+    out = {k: tmp_path / n for k, n in (("out-object", "O.c64"), ("out-pupil", "P.c64"),
+                                         ("out-loss", "loss.f64"), ("out-spectrum", "S.c64"))}
+    r = run("solve", "--h", 64, "--leds", L, "--pratio", 4, "--batch", B, "--epochs", E,
+            "--lr", 2e-3, "--beta", 0.999, "--eps", 1e-4,
+            *sum(([f"--{k}", v] for k, v in {**f, **out}.items()), []))
+    assert r.returncode == 0, r.stderr
+    H = 64 * 4
+    O = np.fromfile(out["out-object"], np.complex64).reshape(H, H).T
+    P = np.fromfile(out["out-pupil"], np.complex64).reshape(64, 64).T
+    S = np.fromfile(out["out-spectrum"], np.complex64).reshape(H, H).T
+    loss = np.fromfile(out["out-loss"], np.float64)
+    ref = engine.solve(None, ds.P0c, to_matlab_stack(ds.raw[:L]), led_matlab(ds.led_idx[:L]),
+                       ds.pupil0, 4, E, B, lr=2e-3, beta=0.999, eps=1e-4)   # bicubic start
+    np.testing.assert_array_equal(O, ref["object"])
+    np.testing.assert_array_equal(P, ref["pupil"])
+    np.testing.assert_array_equal(S, ref["spectrum"])
+    np.testing.assert_array_equal(loss, ref["loss"])

@@ -338,3 +338,58 @@ def test_nonfinite_loss_is_reported(engine, ds_small):
     with pytest.raises(fpm_b200.FpmError) as ex:
         engine.solve(ds.O0, ds.P0c, Y, led_matlab(ds.led_idx[:4]), ds.pupil0, ds.pratio, 1, 2)
     assert ex.value.status == 5
+
+
+@pytest.mark.parametrize("grid,h,p,dx,dy", [(19, 2048, 8, -0.0, -0.0), (11, 128, 4, -0.0, -0.0),
+                                           (5, 64, 2, 1625.0, -3250.0), (1, 256, 4, -0.0, -0.0)])
+def test_led_indices_on_device_equal_oracle(engine, grid, h, p, dx, dy):
+    """FP64 geometry on the device: bit-identical integers to the oracle's IEEE double
+    evaluation of init_environment_rgb.m, spiral order included."""
+    from fpm_b200 import synth
+    o = synth.Optics(led_grid=grid)
+    args = (grid, h, p, o.wavelength_um, o.led_pitch_mm * 1000, o.led_height_mm * 1000,
+            o.camera_pixel_um, o.magnification)
+    led, order = engine.led_indices(*args, sample_dx_um=dx, sample_dy_um=dy)
+    ref, ref_order = orc.led_geometry(*args, sample_dx_um=dx, sample_dy_um=dy)
+    np.testing.assert_array_equal(order, ref_order)
+    np.testing.assert_array_equal(led, ref)
+
+
+def test_led_indices_rejects_bad_geometry(engine):
+    with pytest.raises(fpm_b200.FpmError) as e:
+        engine.led_indices(4, 128, 4, 0.532, 4000, 90000, 6.5, 4)     # even grid
+    assert e.value.status == 1
+    with pytest.raises(fpm_b200.FpmError):
+        engine.led_indices(5, 128, 4, 0.0, 4000, 90000, 6.5, 4)       # zero wavelength
+
+
+def _engine_sized_ref_fixtures():
+    """Reference-build fixtures whose sizes the engine supports (powers of two)."""
+    from pathlib import Path
+    out = []
+    for f in sorted((Path(__file__).resolve().parent / "golden").glob("ref_gradients_*.npz")):
+        h = int(np.load(f)["P"].shape[0])
+        if h & (h - 1) == 0:
+            out.append(f.name)
+    return out
+
+
+@pytest.mark.parametrize("name", _engine_sized_ref_fixtures())
+def test_gradients_match_reference_build(engine, name):
+    """The engine against the reference's own CUDA kernels (+ cuFFT) on the same inputs:
+    fixtures of tests/golden made on a B200 by make_golden.py --ref.  The tolerance is the
+    fixture's (10x the FP32 twin's distance to FP64, floor 1e-5); a sign of the loss
+    stencil taken the other way at a near-tie moves a gradient by ~1e-3, so the engine
+    must match within the tolerance or, failing that, the FP64 oracle as tightly as the
+    reference build does."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / name)
+    h = g["P"].shape[0]
+    ones = np.ones((h, h), np.float32)       # pupil amplitude: unused by a gradient call
+    dO, dP, loss = engine.batch_gradients(g["O"], g["P"], to_matlab_stack(g["Y"]),
+                                          led_matlab(g["led_idx"]), ones, int(g["pratio"]))
+    tol = float(g["tol"])
+    e_o = orc.rel_err(dO, g["ref_dO"])
+    e_p = orc.rel_err(dP, g["ref_dP"])
+    print(f"{name}: engine-vs-reference dO {e_o:.3e} dP {e_p:.3e} (tol {tol:.1e})")
+    assert e_o < tol and e_p < tol
