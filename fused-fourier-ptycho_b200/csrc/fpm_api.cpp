@@ -154,7 +154,7 @@ struct fpm_context {
     FftEngine fft;
     // work buffers, kept between calls
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
-        minmax, spec;
+        minmax, spec, flag;
 };
 
 namespace {
@@ -297,6 +297,7 @@ fpm_status check_leds(fpm_context *ctx, const std::vector<int32_t> &led, int L, 
 
 struct Inputs {
     StackView Y;
+    int stack_pages = 0;
     const int2 *led = nullptr;
     std::vector<int32_t> led_host;
 };
@@ -304,6 +305,7 @@ struct Inputs {
 // Brings every input to the device (or adopts device pointers) and fills `in`.
 fpm_status stage_inputs(fpm_context *ctx, const fpm_problem *p, const Shape &s, Inputs &in) {
     cudaStream_t st = ctx->stream;
+    in.stack_pages = s.L;
     const size_t ybytes = s.plane * s.L * (p->stack_type == FPM_STACK_U16_COUNTS ? 2 : 4);
     in.led_host.resize(2 * (size_t)s.L);
     if (p->memory == FPM_MEM_HOST) {
@@ -424,6 +426,8 @@ fpm_status alloc_pipeline(fpm_context *ctx, const fpm_problem *p, const Shape &s
         FPM_CK(ctx->Rs.ensure(s.plane * 4 * pl.group));
     FPM_CK(ctx->dP.ensure(s.plane * 8));
     FPM_CK(ctx->parts.ensure(sizeof(double) * (size_t)std::max(pl.parts, 1)));
+    FPM_CK(ctx->flag.ensure(sizeof(int)));
+    FPM_CK(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), ctx->stream));
     return FPM_OK;
 }
 
@@ -439,6 +443,7 @@ BatchBufs bufs_of(fpm_context *ctx) {
     b.T1 = ctx->T1.as<float2>();
     b.Rs = ctx->Rs.as<float>();
     b.T2 = ctx->T2.as<float2>();
+    b.flag = ctx->flag.as<int>();
     b.Xs = ctx->Xs.as<float2>();
     b.parts = ctx->parts.as<double>();
     return b;
@@ -487,7 +492,7 @@ fpm_status lowres_and_stitch(fpm_context *ctx, const Plan &pl, const Twiddles &t
         FPM_STAGE(ST_LR_COLS_INV, launch_lr_cols_inv(g, in.led, P, b, l0, nl, tw, st));
         if (pl.fused_rows) {
             FPM_STAGE(ST_LR_ROWS_FUSED,
-                      launch_lr_rows_fused(g, in.Y, b, l0, nl, part_off, tw, st));
+                      launch_lr_rows_fused(g, in.Y, in.stack_pages, b, l0, nl, part_off, tw, st));
             FPM_STAGE(ST_LR_COLS_FWD, launch_lr_cols_fwd(g, b.T2, b, l0, nl, tw, st));
             part_off += lr_rows_fused_blocks(g.h, nl);
         } else {
@@ -625,6 +630,16 @@ void fpm_destroy(fpm_context *ctx) {
 static fpm_status order_after_default_stream(fpm_context *ctx) {
     FPM_CK(cudaEventRecord(ctx->entry, cudaStreamLegacy));
     FPM_CK(cudaStreamWaitEvent(ctx->stream, ctx->entry, 0));
+    return FPM_OK;
+}
+
+// A kernel whose bounded wait on an asynchronous copy gave up sets the context's
+// device flag and skips its work; the call then fails instead of returning
+// results computed from incomplete data.
+static fpm_status check_device_flag(fpm_context *ctx) {
+    int f = 0;
+    FPM_CK(cudaMemcpy(&f, ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) return fail(ctx, FPM_ERR_INTERNAL, "a device-side wait for a tile copy timed out");
     return FPM_OK;
 }
 
@@ -796,6 +811,10 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     FPM_CK(cudaStreamSynchronize(st));
     FPM_CK(cudaGetLastError());
     ctx->prof.collect();
+    {
+        const fpm_status fr = check_device_flag(ctx);
+        if (fr != FPM_OK) return fr;
+    }
     if (res->loss && !dev) std::memcpy(res->loss, loss_h.data(), sizeof(double) * E);
     for (int ep = 0; ep < E; ++ep)
         if (!std::isfinite(loss_h[ep]))
@@ -872,6 +891,10 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
     if (loss) FPM_CK(cudaMemcpyAsync(loss, ctx->loss.p, sizeof(double), kout, st));
     FPM_CK(cudaStreamSynchronize(st));
     ctx->prof.collect();
+    {
+        const fpm_status fr = check_device_flag(ctx);
+        if (fr != FPM_OK) return fr;
+    }
     return FPM_OK;
 }
 

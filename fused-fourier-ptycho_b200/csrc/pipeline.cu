@@ -28,6 +28,9 @@
 #include "engine.h"
 #include "fft_core.cuh"
 #include "pipeline.h"
+#include "tma.cuh"
+
+#include <cudaTypedefs.h>
 
 namespace fpm {
 
@@ -231,6 +234,13 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 // phase, forward FFT).  The two halo lines supply res(r -/+ 1, c); their inverse
 // FFTs are recomputed by the neighbouring CTAs.  The output goes to a second
 // buffer because neighbours still read the halo rows of the input.
+//
+// The row lines are strided in memory (element c of row r at c*h + r): instead of
+// 16 scattered 8-byte loads per thread, the TMA unit copies the CTA's tile of
+// rows [r0-2, r0-2+XR) x all columns into shared memory (boxes of XR x 256) and
+// the threads pick their values there; the stack tile of the same rows (uint16)
+// follows by TMA while the inverse FFTs run.  Lines whose row wraps past the
+// image edge (first and last CTA of an LED) read global memory directly.
 // ---------------------------------------------------------------------------
 template <int N>
 struct L23 {
@@ -241,36 +251,85 @@ struct L23 {
     static constexpr int STRIDE = N + PAD;            // FFT exchange line stride (float2)
     // residual line stride (float): the 32 (line, t) pairs of a warp on 32 banks
     static constexpr int RSTRIDE = N + (LIN >= 32 ? 1 : 32 / LIN);
-    static constexpr int SMEM = LIN * STRIDE * 8 + LIN * RSTRIDE * 4 + 2 * 128 * 8;
+    static constexpr int LINE_BYTES = LIN * STRIDE * 8;
+    static constexpr int RES_BYTES = LIN * RSTRIDE * 4;
+    static constexpr int CB = N < 256 ? N : 256;      // TMA box width along c
+    static constexpr int XR = LIN == 8 ? 12 : LIN + 2;   // field tile rows (even; 12: no bank conflicts)
+    static constexpr int YR = LIN + 8;                // stack tile rows (uint16, 16-byte aligned start)
+    static constexpr int SMEM = LINE_BYTES + RES_BYTES + 2 * 128 * 8 + 16;
     static constexpr int CTAS_PER_LED = (N + LOUT - 1) / LOUT;
     static constexpr int NHI = N >= 128 ? N / 128 : 1;
     static constexpr int NLO = N >= 128 ? 128 : N;
-    static_assert(LIN >= 8 && LIN % 2 == 0, "fused row pass needs T <= 128");
+    static_assert(LIN >= 8 && LIN % 8 == 0, "fused row pass needs T <= 128");
+    static_assert(XR * N * 8 <= LINE_BYTES + RES_BYTES, "field tile fits the line + residual areas");
+    static_assert(YR * N * 2 <= RES_BYTES, "stack tile fits the residual area");
+    static_assert(LINE_BYTES % 128 == 0, "residual area 128-byte aligned for TMA");
 };
 
 template <int N, int TYPE>
 __global__ void __launch_bounds__(1024, 1)
     k_lr_rows_fused(StackView Y, BatchGeom g, int l0, const float2 *__restrict__ T1,
-                    float2 *__restrict__ T2, double *__restrict__ parts,
-                    const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
+                    float2 *__restrict__ T2, double *__restrict__ parts, int *__restrict__ flag,
+                    const __grid_constant__ CUtensorMap tm_field,
+                    const __grid_constant__ CUtensorMap tm_stack, const float2 *__restrict__ thi,
+                    const float2 *__restrict__ tlo) {
     using F = L23<N>;
     constexpr int T = F::T;
-    extern __shared__ float2 smem[];
+    extern __shared__ __align__(128) float2 smem[];
     __shared__ double s_red[32];
     float *res = reinterpret_cast<float *>(smem + F::LIN * F::STRIDE);
     float2 *s_hi = reinterpret_cast<float2 *>(res + F::LIN * F::RSTRIDE);
-    fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, F::NHI, F::NLO);
-    __syncthreads();
+    uint64_t *bar = reinterpret_cast<uint64_t *>(s_hi + 256);          // [0] field, [1] stack
+    const float2 *tile = smem;                                          // [c][XR] field tile
+    const uint16_t *ytile = reinterpret_cast<const uint16_t *>(res);    // [c][YR] stack tile
     const int k = threadIdx.x % F::LIN, t = threadIdx.x / F::LIN;
     const int lloc = blockIdx.x / F::CTAS_PER_LED;
     const int r0 = (blockIdx.x % F::CTAS_PER_LED) * F::LOUT;
-    int r = r0 - 1 + k;
-    r = r < 0 ? r + N : (r >= N ? r - N : r);          // r0 - 1 + k < 2N
-    const bool central = k >= 1 && k <= F::LOUT && r0 + k - 1 < N;
-    const float2 *page = T1 + (size_t)lloc * N * N + r;   // element c at page[c * N]
+    const int x0 = r0 - 2;                      // first tile row (even: 16-byte TMA rule)
+    const int y0 = (r0 - 1) & ~7;               // first stack tile row (8 x 2 bytes)
+    const int zpage = g.z_off + l0 + lloc;
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_barrier_init();
+        tma::arrive_expect_tx(&bar[0], F::XR * N * 8);
+#pragma unroll 1
+        for (int q = 0; q < N / F::CB; ++q)
+            tma::load_3d(smem + q * F::CB * F::XR, &tm_field, x0, q * F::CB, lloc, &bar[0]);
+    }
+    fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, F::NHI, F::NLO);
+    __syncthreads();                                    // barriers initialised before any wait
+    const int rraw = r0 - 1 + k;                        // row before the wrap
+    const bool wrapped = rraw < 0 || rraw >= N;
+    const int r = rraw < 0 ? rraw + N : (rraw >= N ? rraw - N : rraw);
+    const bool central = k >= 1 && k <= F::LOUT && rraw < N;
     float2 v[16];
+    if (wrapped) {   // first / last CTA of an LED: the wrapped halo row from global memory
+        const float2 *page = T1 + (size_t)lloc * N * N + r;
 #pragma unroll
-    for (int m = 0; m < 16; ++m) v[m] = page[(size_t)(t + m * T) * N];
+        for (int m = 0; m < 16; ++m) v[m] = page[(size_t)(t + m * T) * N];
+    }
+    bool bad = !tma::mbar_wait(&bar[0], 0);
+    if (__syncthreads_or(bad)) {   // a tile load never completed: flag it, drain, leave
+        if (threadIdx.x == 0) {
+            atomicExch(flag, 1);
+            tma::mbar_wait(&bar[0], 0);
+        }
+        return;
+    }
+    if (!wrapped) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[m] = tile[(t + m * T) * F::XR + (rraw - x0)];
+    }
+    __syncthreads();                                    // the tile area becomes FFT scratch
+    if (TYPE == kStackU16 && threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        tma::arrive_expect_tx(&bar[1], F::YR * N * 2);
+#pragma unroll 1
+        for (int q = 0; q < N / F::CB; ++q)
+            tma::load_3d(const_cast<uint16_t *>(ytile) + q * F::CB * F::YR, &tm_stack, y0,
+                         q * F::CB, zpage, &bar[1]);
+    }
     float2 *line = smem + k * F::STRIDE;
     fft::line_fft_regs<N, +1>(v, line, s_hi, s_hi + 128, t);
     float mn = 0.f, range = 0.f;
@@ -279,13 +338,33 @@ __global__ void __launch_bounds__(1024, 1)
         range = (float)(Y.minmax[1] - Y.minmax[0]);
     }
     const float ratio = (float)((double)N * N * g.pratio * g.pratio);
-    const size_t ypage = (size_t)(g.z_off + l0 + lloc) * N * N + r;
+    const size_t ypage = (size_t)zpage * N * N + r;
     float *rk = res + k * F::RSTRIDE;
     {
         float y[16];
+        if (TYPE == kStackU16) {
+            bad = !tma::mbar_wait(&bar[1], 0);
+            if (__syncthreads_or(bad)) {
+                if (threadIdx.x == 0) {
+                    atomicExch(flag, 1);
+                    tma::mbar_wait(&bar[1], 0);
+                }
+                return;
+            }
 #pragma unroll
-        for (int m = 0; m < 16; ++m)
-            y[m] = amplitude<TYPE>(Y, ypage + (size_t)(t + m * T) * N, mn, range);
+            for (int m = 0; m < 16; ++m) {
+                const int c = t + m * T;
+                const uint16_t raw = wrapped ? static_cast<const uint16_t *>(Y.ptr)[ypage + (size_t)c * N]
+                                             : ytile[c * F::YR + (rraw - y0)];
+                const float x = (float)raw - mn;
+                y[m] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+            }
+            __syncthreads();                            // the stack tile area becomes residuals
+        } else {
+#pragma unroll
+            for (int m = 0; m < 16; ++m)
+                y[m] = amplitude<TYPE>(Y, ypage + (size_t)(t + m * T) * N, mn, range);
+        }
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const float2 z = v[m];
@@ -697,23 +776,65 @@ int lr_rows_fused_blocks(int h, int nl) { return nl * ctas_per_led_fused(h); }
         default: return cudaErrorInvalidValue; \
     }
 
-cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, BatchBufs b, int l0, int nl,
-                                 int part_off, const Twiddles &tw, cudaStream_t st) {
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (the library links the runtime only).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// 3-D tile map over pages of n x n column-major images (x = row, y = column, z = page).
+static cudaError_t page_tile_map(CUtensorMap *map, CUtensorMapDataType type, size_t esz,
+                                 const void *base, int n, int pages, int box_rows, int box_cols) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)pages};
+    const cuuint64_t strides[2] = {(cuuint64_t)n * esz, (cuuint64_t)n * n * esz};
+    const cuuint32_t box[3] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(map, type, 3, const_cast<void *>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_pages, BatchBufs b,
+                                 int l0, int nl, int part_off, const Twiddles &tw,
+                                 cudaStream_t st) {
     const int blocks = lr_rows_fused_blocks(g.h, nl);
     cudaError_t e = cudaSuccess;
+    CUtensorMap tm_field{}, tm_stack{};
 #define F(N)                                                                              \
     static_assert(L23<N>::CTAS_PER_LED == (N + 1024 / (N / 16) - 3) / (1024 / (N / 16) - 2), \
                   "host CTA count");                                                      \
+    e = page_tile_map(&tm_field, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, b.T1, N, nl,          \
+                      L23<N>::XR, L23<N>::CB);                                            \
+    if (e != cudaSuccess) return e;                                                       \
     if (Y.type == kStackU16) {                                                            \
+        e = page_tile_map(&tm_stack, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, Y.ptr, N,         \
+                          stack_pages, L23<N>::YR, L23<N>::CB);                           \
+        if (e != cudaSuccess) return e;                                                   \
         e = set_smem(k_lr_rows_fused<N, kStackU16>, L23<N>::SMEM);                        \
         if (e != cudaSuccess) return e;                                                   \
         k_lr_rows_fused<N, kStackU16><<<blocks, 1024, L23<N>::SMEM, st>>>(                \
-            Y, g, l0, b.T1, b.T2, b.parts + part_off, tw.lo_hi, tw.lo_lo);           \
+            Y, g, l0, b.T1, b.T2, b.parts + part_off, b.flag, tm_field, tm_stack,         \
+            tw.lo_hi, tw.lo_lo);                                                          \
     } else {                                                                              \
         e = set_smem(k_lr_rows_fused<N, kStackF32>, L23<N>::SMEM);                        \
         if (e != cudaSuccess) return e;                                                   \
         k_lr_rows_fused<N, kStackF32><<<blocks, 1024, L23<N>::SMEM, st>>>(                \
-            Y, g, l0, b.T1, b.T2, b.parts + part_off, tw.lo_hi, tw.lo_lo);           \
+            Y, g, l0, b.T1, b.T2, b.parts + part_off, b.flag, tm_field, tm_stack,         \
+            tw.lo_hi, tw.lo_lo);                                                          \
     }
     FPM_DISPATCH_FUSED(g.h, F)
 #undef F

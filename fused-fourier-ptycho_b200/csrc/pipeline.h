@@ -31,6 +31,7 @@ struct BatchBufs {
     float2 *T2 = nullptr;          // [group][h][h] output of the fused L2 + L3 pass
     float2 *Xs = nullptr;          // [nb][h][h] row-major fftshift'ed gradient spectrum
     double *parts = nullptr;       // loss partials of the batch
+    int *flag = nullptr;           // set by a kernel whose bounded wait gave up
 };
 
 bool pipeline_supported(int h, int H);
@@ -47,8 +48,9 @@ cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, 
 // lr_rows_fused_blocks(h, nl) of them.
 bool lr_rows_fused_supported(int h);
 int lr_rows_fused_blocks(int h, int nl);
-cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, BatchBufs b, int l0, int nl,
-                                 int part_off, const Twiddles &tw, cudaStream_t st);
+cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_pages, BatchBufs b,
+                                 int l0, int nl, int part_off, const Twiddles &tw,
+                                 cudaStream_t st);
 // L4 over src (T1 after separate L2, L3; T2 after the fused pass) -> Xs
 cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs b, int l0,
                                int nl, const Twiddles &tw, cudaStream_t st);
