@@ -139,25 +139,48 @@ def make_workload_gpu(cfg: Cfg, dev):
 # ---------------------------------------------------------------------------
 # algorithmic bytes per launch of each stage (documented in DESIGN.md)
 # ---------------------------------------------------------------------------
-def batch_boxes(led, h, H, batch):
-    """Crop box (rspan, cspan) of every mini-batch, as the engine plans them."""
+def pupil_support(circ):
+    """Rows / columns [lo, hi) of the pupil's non-zero pixels (the engine prunes to them)."""
+    rows = np.flatnonzero(np.any(circ != 0, axis=1))
+    cols = np.flatnonzero(np.any(circ != 0, axis=0))
+    return int(rows[0]), int(rows[-1]) + 1, int(cols[0]), int(cols[-1]) + 1
+
+
+def _support_of(wl):
+    """The support the engine prunes to (none with FPM_PUPIL_SUPPORT=0)."""
+    if os.environ.get("FPM_PUPIL_SUPPORT", "1") == "0":
+        return None
+    return pupil_support(wl["circ"])
+
+
+def batch_boxes(led, h, H, batch, sup=None):
+    """Spectrum box (rspan, cspan) of every mini-batch, as the engine plans them: the union of
+    the batch's crops restricted to the pupil support."""
+    r_lo, r_hi, c_lo, c_hi = sup if sup is not None else (0, h, 0, h)
     out = []
     L = len(led)
     for cur in range(0, L, batch):
         sl = led[cur:cur + batch]
         kt = sl[:, 1] - 1
         kl = sl[:, 0] - 1
-        rspan = min(int((kt + h).max() - kt.min()), H)
-        cspan = min(int((kl + h).max() - kl.min()), H)
+        rspan = min(int((kt + r_hi).max() - (kt + r_lo).min()), H)
+        cspan = min(int((kl + c_hi).max() - (kl + c_lo).min()), H)
         out.append((len(sl), rspan, cspan))
     return out
 
 
-def stage_bytes(cfg: Cfg, led):
-    """Average algorithmic bytes per launch of each stage over one epoch."""
+def stage_bytes(cfg: Cfg, led, sup=None):
+    """Average algorithmic bytes per launch of each stage over one epoch.
+
+    fr, fc: fractions of crop rows / columns inside the pupil support; the passes read
+    and write only what the pruned algorithm needs (zero columns of the first field
+    are still written)."""
     H, h = cfg.H, cfg.h
     H2, h2 = H * H, h * h
-    boxes = batch_boxes(led, h, H, cfg.batch)
+    sup = sup if sup is not None else (0, h, 0, h)
+    fr = (sup[1] - sup[0]) / h
+    fc = (sup[3] - sup[2]) / h
+    boxes = batch_boxes(led, h, H, cfg.batch, sup)
     nbatch = len(boxes)
     group = max(1, min(cfg.batch, (4 << 30) // (h2 * 16)))
     lr_launches = sum(math.ceil(nb / group) for nb, _, _ in boxes)
@@ -167,13 +190,13 @@ def stage_bytes(cfg: Cfg, led):
     for bi, (nb, rspan, cspan) in enumerate(boxes):
         _, rn, cn = boxes[(bi + 1) % nbatch]
         px = h2 * nb
-        tot["lr_cols_inverse"] += 16 * px      # crop of the spectrum box r8, field w8
+        tot["lr_cols_inverse"] += (8 * fr * fc + 8) * px   # support crop r8, field w8
         tot["lr_rows_inverse"] += 22 * px      # field r8 w8, residual w4, stack r2
         tot["lr_rows_forward"] += 20 * px      # residual r4, field r8 w8
-        tot["lr_rows_fused"] += 18 * px        # field r8, stack r2, field w8 (halo re-reads not counted)
-        tot["lr_cols_forward"] += 16 * px      # field r8, gradient spectrum w8
-        tot["pupil_grad"] += 16 * px + 8 * h2  # spectrum box r8 + gradient spectrum r8 per LED px
-        tot["rows_inverse_stitch"] += 8 * px + 8 * H * rspan
+        tot["lr_rows_fused"] += (10 + 8 * fc) * px   # field r8, stack r2, support columns w8
+        tot["lr_cols_forward"] += 16 * fc * px        # support columns r8, gradient spectrum w8
+        tot["pupil_grad"] += 16 * fr * fc * px + 8 * h2
+        tot["rows_inverse_stitch"] += 8 * fr * fc * px + 8 * H * rspan
         tot["cols_update"] += 8 * H * rspan + 24 * H2 + 8 * H * rn
         tot["rows_forward"] += 8 * H * rn + 8 * rn * cn
         tot["rmsprop_pupil"] += 36 * h2
@@ -367,7 +390,7 @@ def run_ours(args, cfg: Cfg):
     # e2e: the full 10-epoch job through the C ABI with pinned host buffers
     if args.no_e2e:
         return _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, None,
-                       wl["led_np"]), wl, rank, world
+                       wl["led_np"], _support_of(wl)), wl, rank, world
     pin = lambda x: x.cpu().pin_memory()
     hs, hl, hp, ha = pin(wl["stack"]), pin(wl["led"]), pin(wl["P0c"]), pin(wl["P0"])
     hO = torch.empty((H, H), dtype=torch.complex64).pin_memory()
@@ -395,16 +418,17 @@ def run_ours(args, cfg: Cfg):
            "note": "one 10-epoch job per step through fpm_solve with pinned host buffers; "
                    "stack/LEDs/pupil in, object+spectrum+pupil+loss out"}
     out = _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e,
-                  wl["led_np"])
+                  wl["led_np"], _support_of(wl))
     eng.close()
     return out, wl, rank, world
 
 
-def _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e, wl_led):
+def _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e, wl_led,
+            sup=None):
     out = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        sb = stage_bytes(cfg, wl_led)
+        sb = stage_bytes(cfg, wl_led, sup)
         st_rep = {}
         for name, (n, tms, own) in stages.items():
             avg = tms / n

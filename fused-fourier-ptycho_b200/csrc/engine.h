@@ -45,6 +45,10 @@ cudaError_t launch_stack_minmax(const uint16_t *p, size_t n, unsigned *minmax, c
 cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *minmax, float *out,
                              cudaStream_t st);
 
+// box = {min row, max row, min col, max col} of the non-zero pixels of P (complex) or A
+// (real), either may be NULL; {h, -1, h, -1} when none
+cudaError_t launch_support_box(const float2 *P, const float *A, int h, int *box, cudaStream_t st);
+
 // ---- LED geometry (FP64) -----------------------------------------------------
 struct LedGeom {
     int grid = 0, h = 0, NN = 0;     // LEDs per side, low-res side, high-res side

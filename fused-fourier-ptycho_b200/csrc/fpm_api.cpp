@@ -211,14 +211,22 @@ bool is_host_ptr(const void *p) {
 }
 
 // crop box of one batch in centred coordinates, taken modulo H
-Box batch_box(const std::vector<int32_t> &led, int first, int nb, int h, int H) {
+// Pupil support: crop rows / columns [r_lo, r_hi) x [c_lo, c_hi) outside which the
+// pupil is zero for the whole solve.
+struct Support {
+    int r_lo = 0, r_hi = 0, c_lo = 0, c_hi = 0;
+};
+
+// Centred-spectrum box of one batch: the union of its LEDs' crops restricted to the
+// pupil support (the only part of a crop the batch reads or writes).
+Box batch_box(const std::vector<int32_t> &led, int first, int nb, const Support &sup, int H) {
     int rlo = 1 << 30, rhi = -(1 << 30), clo = 1 << 30, chi = -(1 << 30);
     for (int i = first; i < first + nb; ++i) {
         const int kl = led[2 * i], kt = led[2 * i + 1];
-        rlo = std::min(rlo, kt - 1);
-        rhi = std::max(rhi, kt - 1 + h);
-        clo = std::min(clo, kl - 1);
-        chi = std::max(chi, kl - 1 + h);
+        rlo = std::min(rlo, kt - 1 + sup.r_lo);
+        rhi = std::max(rhi, kt - 1 + sup.r_hi);
+        clo = std::min(clo, kl - 1 + sup.c_lo);
+        chi = std::max(chi, kl - 1 + sup.c_hi);
     }
     Box b;
     b.r_lo = rlo;
@@ -339,6 +347,43 @@ fpm_status stage_inputs(fpm_context *ctx, const fpm_problem *p, const Shape &s, 
     return FPM_OK;
 }
 
+// Pupil support of a solve: the amplitude clamp (|P| <- P0 clamp(|P|, P0 -/+ am))
+// keeps the pupil at zero wherever P0 is zero, so after the initial pupil P0c the
+// pupil is non-zero only inside supp(P0c) u supp(P0).  FPM_PUPIL_SUPPORT=0 keeps whole
+// crops (measurements).
+fpm_status pupil_support(fpm_context *ctx, const fpm_problem *p, const Shape &s, Support &sup) {
+    sup.r_lo = sup.c_lo = 0;
+    sup.r_hi = sup.c_hi = s.h;
+    if (const char *env = std::getenv("FPM_PUPIL_SUPPORT"))
+        if (std::atoi(env) == 0) return FPM_OK;
+    int box[4] = {s.h, -1, s.h, -1};
+    if (p->memory == FPM_MEM_HOST) {
+        const float *P = p->pupil_init, *A = p->pupil_amp;
+        for (int c = 0; c < s.h; ++c)
+            for (int r = 0; r < s.h; ++r) {
+                const size_t i = (size_t)c * s.h + r;
+                if (!(P[2 * i] == 0.f && P[2 * i + 1] == 0.f) || !(A[i] == 0.f)) {
+                    box[0] = std::min(box[0], r);
+                    box[1] = std::max(box[1], r);
+                    box[2] = std::min(box[2], c);
+                    box[3] = std::max(box[3], c);
+                }
+            }
+    } else {
+        FPM_CK(ctx->flag.ensure(sizeof(int) * 4));
+        FPM_CK(launch_support_box(reinterpret_cast<const float2 *>(p->pupil_init), p->pupil_amp,
+                                  s.h, ctx->flag.as<int>(), ctx->stream));
+        FPM_CK(cudaMemcpyAsync(box, ctx->flag.p, sizeof(box), cudaMemcpyDeviceToHost, ctx->stream));
+        FPM_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    if (box[1] < 0) return FPM_OK;   // an all-zero pupil: keep whole crops
+    sup.r_lo = box[0];
+    sup.r_hi = box[1] + 1;
+    sup.c_lo = box[2];
+    sup.c_hi = box[3] + 1;
+    return FPM_OK;
+}
+
 // Crop boxes of every mini-batch of an epoch (the same every epoch).
 struct Plan {
     std::vector<BatchGeom> geoms;
@@ -350,11 +395,11 @@ struct Plan {
 };
 
 
-Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch) {
+Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const Support &sup) {
     Plan pl;
     for (int cur = 0; cur < s.L; cur += batch) {
         const int nb = std::min(batch, s.L - cur);
-        const Box b = batch_box(led, cur, nb, s.h, s.H);
+        const Box b = batch_box(led, cur, nb, sup, s.H);
         BatchGeom g;
         g.H = s.H;
         g.h = s.h;
@@ -367,6 +412,10 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch) {
         g.cspan = b.c_span;
         g.Ru0 = (g.rlo + s.H / 2) % s.H;
         g.Cu0 = (g.clo + s.H / 2) % s.H;
+        g.pr_lo = sup.r_lo;
+        g.pr_hi = sup.r_hi;
+        g.pc_lo = sup.c_lo;
+        g.pc_hi = sup.c_hi;
         pl.geoms.push_back(g);
         pl.ldU = std::max(pl.ldU, g.rspan);
         pl.sbox = std::max(pl.sbox, (size_t)g.rspan * g.cspan);
@@ -426,7 +475,7 @@ fpm_status alloc_pipeline(fpm_context *ctx, const fpm_problem *p, const Shape &s
         FPM_CK(ctx->Rs.ensure(s.plane * 4 * pl.group));
     FPM_CK(ctx->dP.ensure(s.plane * 8));
     FPM_CK(ctx->parts.ensure(sizeof(double) * (size_t)std::max(pl.parts, 1)));
-    FPM_CK(ctx->flag.ensure(sizeof(int)));
+    FPM_CK(ctx->flag.ensure(sizeof(int) * 4));
     FPM_CK(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), ctx->stream));
     return FPM_OK;
 }
@@ -693,7 +742,10 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     std::vector<int32_t> led_host;
     rc = fetch_leds(ctx, p, s, led_host);
     if (rc != FPM_OK) return rc;
-    const Plan pl = make_plan(s, led_host, p->batch);
+    Support sup;
+    rc = pupil_support(ctx, p, s, sup);
+    if (rc != FPM_OK) return rc;
+    const Plan pl = make_plan(s, led_host, p->batch, sup);
     rc = alloc_pipeline(ctx, p, s, pl, res->spectrum != nullptr);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;
@@ -851,7 +903,9 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
     std::vector<int32_t> led_host;
     rc = fetch_leds(ctx, p, s, led_host);
     if (rc != FPM_OK) return rc;
-    const Plan pl = make_plan(s, led_host, s.L);
+    Support full;   // the pupil gradient is an output here: whole crops
+    full.r_hi = full.c_hi = s.h;
+    const Plan pl = make_plan(s, led_host, s.L, full);
     rc = alloc_pipeline(ctx, p, s, pl, true);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;

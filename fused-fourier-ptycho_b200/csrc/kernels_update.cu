@@ -278,4 +278,63 @@ cudaError_t launch_transpose(const float2 *in, size_t ldi, float2 *out, size_t l
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Bounding box of the non-zero pixels of a complex h x h pupil and of a real one
+// (either may be NULL; NaN counts as non-zero): box = {min row, max row, min col,
+// max col}, initialised by the launcher to {h, -1, h, -1} (no pixel).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_support_box(const float2 *__restrict__ P,
+                                                      const float *__restrict__ A, int h,
+                                                      int *__restrict__ box) {
+    int rmin = h, rmax = -1, cmin = h, cmax = -1;
+    const size_t n = (size_t)h * h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        bool nz = false;
+        if (P) {
+            const float2 v = P[i];
+            nz = !(v.x == 0.f && v.y == 0.f);
+        }
+        if (A) nz = nz || !(A[i] == 0.f);
+        if (nz) {
+            const int r = (int)(i % h), c = (int)(i / h);
+            rmin = min(rmin, r);
+            rmax = max(rmax, r);
+            cmin = min(cmin, c);
+            cmax = max(cmax, c);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        rmin = min(rmin, __shfl_down_sync(0xffffffffu, rmin, off));
+        rmax = max(rmax, __shfl_down_sync(0xffffffffu, rmax, off));
+        cmin = min(cmin, __shfl_down_sync(0xffffffffu, cmin, off));
+        cmax = max(cmax, __shfl_down_sync(0xffffffffu, cmax, off));
+    }
+    if ((threadIdx.x & 31) == 0 && rmax >= 0) {
+        atomicMin(&box[0], rmin);
+        atomicMax(&box[1], rmax);
+        atomicMin(&box[2], cmin);
+        atomicMax(&box[3], cmax);
+    }
+}
+
+__global__ void k_support_box_init(int *box, int h) {
+    if (threadIdx.x == 0) {
+        box[0] = h;
+        box[1] = -1;
+        box[2] = h;
+        box[3] = -1;
+    }
+}
+
+cudaError_t launch_support_box(const float2 *P, const float *A, int h, int *box, cudaStream_t st) {
+    k_support_box_init<<<1, 32, 0, st>>>(box, h);
+    const size_t n = (size_t)h * h;
+    size_t gx = (n + 255) / 256;
+    if (gx > (size_t)kB200SMs * 4) gx = (size_t)kB200SMs * 4;
+    k_support_box<<<(unsigned)gx, 256, 0, st>>>(P, A, h, box);
+    return cudaGetLastError();
+}
+
 }  // namespace fpm

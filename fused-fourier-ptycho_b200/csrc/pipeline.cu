@@ -96,24 +96,31 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     const bool live = gl < (long long)nl * N;
     constexpr int hh = N / 2;
     float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = make_float2(0.f, 0.f);
+    bool nz = false;   // the crop column meets the pupil support
     if (live) {
         const int lloc = (int)(gl / N);
         const int cq = (int)(gl % N);
-        const int2 ab = led_box_offset(led, l0 + lloc, g);
         const int c = cq + hh >= N ? cq + hh - N : cq + hh;
-        const float2 *scol = Sbox + (size_t)box_index(ab.y, c, g.H) * g.rspan;
-        const float2 *pcol = P + (size_t)c * N;
+        nz = c >= g.pc_lo && c < g.pc_hi;
+        if (nz) {
+            const int2 ab = led_box_offset(led, l0 + lloc, g);
+            const float2 *scol = Sbox + (size_t)box_index(ab.y, c, g.H) * g.rspan;
+            const float2 *pcol = P + (size_t)c * N;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const int e = t + m * G::T;
-            const int r = e + hh >= N ? e + hh - N : e + hh;
-            v[m] = cmul(scol[box_index(ab.x, r, g.H)], pcol[r]);
+            for (int m = 0; m < 16; ++m) {
+                const int e = t + m * G::T;
+                const int r = e + hh >= N ? e + hh - N : e + hh;
+                if (r >= g.pr_lo && r < g.pr_hi)   // the box holds only the support rows
+                    v[m] = cmul(scol[box_index(ab.x, r, g.H)], pcol[r]);
+            }
         }
-    } else {
-#pragma unroll
-        for (int m = 0; m < 16; ++m) v[m] = make_float2(0.f, 0.f);
     }
-    fft::line_fft_regs<N, +1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    // columns outside the support transform zeros: a CTA holding only such lines skips
+    // the transform and writes the zeros
+    if (__syncthreads_or(nz))
+        fft::line_fft_regs<N, +1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
     if (live) {
         float2 *dst = T1 + (size_t)gl * N;
 #pragma unroll
@@ -407,10 +414,14 @@ __global__ void __launch_bounds__(1024, 1)
         parts[blockIdx.x] = tot;
     }
     fft::line_fft_regs<N, -1>(v, line, s_hi, s_hi + 128, t);
-    if (central) {
+    if (central) {   // only the columns the next pass transforms (pupil support, fftshifted)
         float2 *dst = T2 + (size_t)lloc * N * N + r;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) dst[(size_t)(t + m * T) * N] = v[m];
+        for (int m = 0; m < 16; ++m) {
+            const int cf = t + m * T;
+            const int c = cf + N / 2 >= N ? cf - N / 2 : cf + N / 2;
+            if (c >= g.pc_lo && c < g.pc_hi) dst[(size_t)cf * N] = v[m];
+        }
     }
 }
 
@@ -420,7 +431,7 @@ __global__ void __launch_bounds__(1024, 1)
 // ---------------------------------------------------------------------------
 template <int N>
 __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
-    k_lr_cols_fwd(int l0, int nl, const float2 *__restrict__ T1, float2 *__restrict__ Xs,
+    k_lr_cols_fwd(BatchGeom g, int l0, int nl, const float2 *__restrict__ T1, float2 *__restrict__ Xs,
                   const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
     using G = fft::LG<N>;
     extern __shared__ float2 smem[];
@@ -429,15 +440,18 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     const long long gl = (long long)blockIdx.x * G::LPC + ln;
     const bool live = gl < (long long)nl * N;
     constexpr int hh = N / 2;
-    const float2 *src = T1 + (size_t)(live ? gl : 0) * N;
+    const int cf = live ? (int)(gl % N) : 0;
+    const int c = cf + hh >= N ? cf + hh - N : cf + hh;
+    // only gradient-spectrum columns inside the pupil support are ever read
+    const bool need = live && c >= g.pc_lo && c < g.pc_hi;
+    if (!__syncthreads_or(need)) return;
+    const float2 *src = T1 + (size_t)(need ? gl : 0) * N;
     float2 v[16];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) v[m] = live ? src[t + m * G::T] : make_float2(0.f, 0.f);
+    for (int m = 0; m < 16; ++m) v[m] = need ? src[t + m * G::T] : make_float2(0.f, 0.f);
     fft::line_fft_regs<N, -1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
-    if (!live) return;
+    if (!need) return;
     const int lloc = (int)(gl / N);
-    const int cf = (int)(gl % N);
-    const int c = cf + hh >= N ? cf + hh - N : cf + hh;
     float2 *xs = Xs + (size_t)(l0 + lloc) * N * N + c;
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
@@ -460,16 +474,21 @@ __global__ void __launch_bounds__(256) k_lr_pupil_grad(const float2 *__restrict_
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     KahanC acc[4];
-    for (int l = 0; l < g.nb; ++l) {
+    // outside the pupil support the gradient is never used (the amplitude clamp keeps
+    // the pupil at zero there): tiles beyond it only write zeros
+    const bool any = r0 < g.pr_hi && r0 + 32 > g.pr_lo && c0 < g.pc_hi && c0 + 32 > g.pc_lo;
+    for (int l = 0; any && l < g.nb; ++l) {
         const int2 ab = led_box_offset(led, l, g);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int cl = ty + 8 * k;
             const int r = r0 + tx, c = c0 + cl;       // sub: coalesced along r
-            if (r < h && c < h)
-                sA[cl][tx] = Sbox[(size_t)box_index(ab.y, c, g.H) * g.rspan + box_index(ab.x, r, g.H)];
+            const bool a_in = r >= g.pr_lo && r < g.pr_hi && c >= g.pc_lo && c < g.pc_hi;
+            sA[cl][tx] = a_in ? Sbox[(size_t)box_index(ab.y, c, g.H) * g.rspan + box_index(ab.x, r, g.H)]
+                              : make_float2(0.f, 0.f);
             const int rr = r0 + cl, cc = c0 + tx;     // Xs: coalesced along c
-            if (rr < h && cc < h) sB[cl][tx] = Xs[((size_t)l * h + rr) * h + cc];
+            const bool b_in = rr >= g.pr_lo && rr < g.pr_hi && cc >= g.pc_lo && cc < g.pc_hi;
+            sB[cl][tx] = b_in ? Xs[((size_t)l * h + rr) * h + cc] : make_float2(0.f, 0.f);
         }
         __syncthreads();
 #pragma unroll
@@ -522,7 +541,7 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
                 const int2 ab = s_ab[l];
                 int rr = i - ab.x;
                 if (rr < 0) rr += N;
-                if (rr >= h) continue;               // uniform per line
+                if (rr < g.pr_lo || rr >= g.pr_hi) continue;   // pupil zero on that crop row
                 const float2 *xrow = Xs + ((size_t)l * h + rr) * h;
                 const float2 *prow = Pt + (size_t)rr * h;
                 float2 x[4], pp[4];
@@ -531,7 +550,7 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
                 for (int k = 0; k < 4; ++k) {
                     int c = jj[k] - ab.y;
                     if (c < 0) c += N;
-                    in[k] = jj[k] >= 0 && c < h;
+                    in[k] = jj[k] >= 0 && c >= g.pc_lo && c < g.pc_hi;
                     x[k] = in[k] ? xrow[c] : make_float2(0.f, 0.f);
                     pp[k] = in[k] ? prow[c] : make_float2(0.f, 0.f);
                 }
@@ -849,7 +868,7 @@ cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs 
     e = set_smem(k_lr_cols_fwd<N>, smem_bytes<N>());                                      \
     if (e != cudaSuccess) return e;                                                       \
     k_lr_cols_fwd<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                   \
-        l0, nl, src, b.Xs, tw.lo_hi, tw.lo_lo);
+        g, l0, nl, src, b.Xs, tw.lo_hi, tw.lo_lo);
     FPM_DISPATCH_LR(g.h, F)
 #undef F
     return cudaGetLastError();

@@ -15,6 +15,10 @@ struct BatchGeom {
     int z_off = 0, nb = 0;
     int rlo = 0, rspan = 0, clo = 0, cspan = 0;
     int Ru0 = 0, Cu0 = 0;
+    // crop rows / columns [pr_lo, pr_hi) x [pc_lo, pc_hi) (centred h x h frame) outside
+    // which the pupil is zero: the crop there contributes nothing and the gradient
+    // spectrum there is never used, so the box above covers only this part of each crop
+    int pr_lo = 0, pr_hi = 0, pc_lo = 0, pc_hi = 0;
 };
 
 // Two-level twiddle tables (fft_core.cuh) for the low-res length h and the large length H.

@@ -393,3 +393,30 @@ def test_gradients_match_reference_build(engine, name):
     e_p = orc.rel_err(dP, g["ref_dP"])
     print(f"{name}: engine-vs-reference dO {e_o:.3e} dP {e_p:.3e} (tol {tol:.1e})")
     assert e_o < tol and e_p < tol
+
+
+def test_pupil_support_pruning_is_exact(engine, ds_small):
+    """The solve prunes every pass to the pupil's support box; with an off-centre,
+    asymmetric support the result must equal the unpruned solve (FPM_PUPIL_SUPPORT=0)
+    up to the rounding of the skipped zero terms, and the pupil must stay zero outside."""
+    import os
+    ds = ds_small
+    h = ds.h
+    P0 = np.zeros((h, h), np.float32)
+    P0[5:41, 20:61] = ds.pupil0[5:41, 20:61] + 0.25          # rows 5..40, cols 20..60
+    P0c = (P0 * np.exp(0.3j * np.arange(h)[None, :] / h)).astype(np.complex64)
+    args = (ds.O0, P0c, to_matlab_stack(ds.Y[:25]), led_matlab(ds.led_idx[:25]), P0, ds.pratio, 2, 6)
+    kw = dict(lr=2e-3, beta=0.999, eps=1e-4)
+    pruned = engine.solve(*args, **kw)
+    os.environ["FPM_PUPIL_SUPPORT"] = "0"
+    try:
+        whole = engine.solve(*args, **kw)
+    finally:
+        del os.environ["FPM_PUPIL_SUPPORT"]
+    for k in ("object", "pupil", "spectrum"):
+        assert orc.rel_err(pruned[k], whole[k]) < 1e-5, (k, orc.rel_err(pruned[k], whole[k]))
+    np.testing.assert_allclose(pruned["loss"], whole["loss"], rtol=1e-6)
+    assert np.all(pruned["pupil"][P0 == 0] == 0)
+    o64 = orc.cufpm_pure_v3(ds.O0, P0c, ds.Y[:25], ds.led_idx[:25], P0, ds.pratio, 2, 6,
+                            opt=(2e-3, 0.999, 1e-4))
+    assert orc.rel_err(pruned["object"], o64.object) < 2e-2
