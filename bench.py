@@ -488,6 +488,66 @@ def cpu_baseline_for(cfg: Cfg, wl, steps=2):
                       f"{math.ceil(cfg.L / cfg.batch)} batches"}
 
 
+def run_simulate(args, cfg: Cfg):
+    """Forward model (fpm_simulate): all LED images of a 16384^2 object, device-resident.
+    Not the headline metric: a separate line for the simulator row."""
+    import torch
+    import fpm_b200
+    from fpm_b200 import api, synth
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(cfg.seed)
+    H, h = cfg.H, cfg.h
+    O = torch.polar(0.5 + 0.5 * torch.rand((H, H), generator=g, device=dev),
+                    torch.randn((H, H), generator=g, device=dev))
+    optics = synth.Optics(led_grid=cfg.grid)
+    P = torch.from_numpy(np.ascontiguousarray(synth.pupil_circle(h, optics).T)).to(dev).to(torch.complex64)
+    led = torch.from_numpy(np.ascontiguousarray(synth.led_indices(h, cfg.pratio, optics))).to(dev)
+    out = torch.empty((cfg.L, h, h), dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    eng = fpm_b200.Engine(0, stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    call = lambda: eng._check(eng.lib.fpm_simulate(eng._ctx, O.data_ptr(), P.data_ptr(), led.data_ptr(),
+                                                   h, cfg.pratio, cfg.L, api.SIM_INTENSITY,
+                                                   out.data_ptr(), api.MEM_DEVICE))
+    for _ in range(args.warmup):
+        call()
+    eng.set_profiling(True)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stages = {}
+    e0.record(stream)
+    for _ in range(args.steps):
+        call()
+        for k, v in eng.stage_times().items():
+            n, t, _ = stages.get(k, (0, 0.0, v[2]))
+            stages[k] = (n + v[0], t + v[1], v[2])
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    peak, _ = measured_peaks()
+    px = h * h * cfg.L
+    sb = {"spectrum_fft2": 32 * H * H, "lr_cols_inverse": 16 * px, "sim_rows_inverse": 16 * px,
+          "sim_magnitude": 12 * px}
+    # bytes per call over the stage's summed time in the timed calls
+    st = {k: {"launches": n, "ms_total": round(t, 3),
+              "gbs": round(sb.get(k, 0) * args.steps / (t * 1e-3) / 1e9, 1)}
+          for k, (n, t, own) in stages.items()}
+    dom = max(st, key=lambda k: st[k]["ms_total"])
+    line = {"metric": "forward-model LED images per second", "value": round(cfg.L / (ms * 1e-3), 1),
+            "unit": "images/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "f32 (complex64)",
+            "data": "synthetic (seeded random object, circular pupil)",
+            "config": {"workload": f"forward model: {H}x{H} object -> {cfg.L} LED images of {h}x{h}",
+                       "h": h, "H": H, "leds": cfg.L},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": st[dom]["gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": round(st[dom]["gbs"] / peak, 3)},
+            "stages": st}
+    eng.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, cfg: Cfg):
     """Reference arm: the CPU restatement of the reference algorithm, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -532,6 +592,8 @@ def main():
     ap.add_argument("--grid", type=int, default=19)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="solve", choices=["solve", "simulate"],
+                    help="solve: the reconstruction (headline); simulate: the forward model")
     ap.add_argument("--quick-data", action="store_true",
                     help="random stack instead of the simulated one (profiler runs only)")
     args = ap.parse_args()
@@ -540,6 +602,9 @@ def main():
     cfg = Cfg(h=args.h, pratio=args.pratio, grid=args.grid, batch=args.batch)
     if args.impl == "reference":
         run_reference(args, cfg)
+        return
+    if args.workload == "simulate":
+        run_simulate(args, cfg)
         return
     out, wl, rank, world = run_ours(args, cfg)
     if rank == 0:

@@ -49,6 +49,10 @@ cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *minmax
 // (real), either may be NULL; {h, -1, h, -1} when none
 cudaError_t launch_support_box(const float2 *P, const float *A, int h, int *box, cudaStream_t st);
 
+// out[i] = |z[i] scale|^2, or its square root when amplitude != 0 (n even, 16-byte aligned)
+cudaError_t launch_sim_magnitude(const float2 *z, size_t n, float scale, int amplitude,
+                                 float *out, cudaStream_t st);
+
 // ---- LED geometry (FP64) -----------------------------------------------------
 struct LedGeom {
     int grid = 0, h = 0, NN = 0;     // LEDs per side, low-res side, high-res side

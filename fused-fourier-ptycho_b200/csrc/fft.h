@@ -26,6 +26,10 @@ public:
 
     // n x n transform of `count` pages of n*n elements; in may equal out.
     cudaError_t run(const float2 *in, float2 *out, int n, int count, FftDir dir, cudaStream_t st);
+    // One axis only: axis 0 transforms the contiguous lines (along rows r), axis 1 the
+    // strided ones (along columns c).
+    cudaError_t run_axis(const float2 *in, float2 *out, int n, int count, int axis, FftDir dir,
+                         cudaStream_t st);
     // Device two-level twiddle table of length n: hi (max(1, n/128) entries)
     // followed by lo (min(n, 128) entries), W_n^m = hi[m >> 7] * lo[m & 127].
     cudaError_t tables(int n, const float2 **hi, const float2 **lo);

@@ -72,9 +72,11 @@ __global__ void __launch_bounds__(LG<N>::THREADS, LG<N>::MINB)
     }
 }
 
+// axes: bit 0 = the contiguous pass, bit 1 = the strided pass (run in that order; the
+// strided pass reads the contiguous pass's output when both run)
 template <int N, int DIR>
-cudaError_t run_n(const float2 *in, float2 *out, int count, const float2 *hi, const float2 *lo,
-                  cudaStream_t st) {
+cudaError_t run_n(const float2 *in, float2 *out, int count, int axes, const float2 *hi,
+                  const float2 *lo, cudaStream_t st) {
     using G = LG<N>;
     cudaError_t e = set_smem(k_fft_contig<N, DIR>, G::SMEM);
     if (e != cudaSuccess) return e;
@@ -82,28 +84,34 @@ cudaError_t run_n(const float2 *in, float2 *out, int count, const float2 *hi, co
     if (e != cudaSuccess) return e;
     const long long lines = (long long)count * N;
     const long long blocks = (lines + G::LPC - 1) / G::LPC;
-    k_fft_contig<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(in, out, lines, hi, lo);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    k_fft_strided<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(out, out, lines, hi, lo);
-    return cudaGetLastError();
+    if (axes & 1) {
+        k_fft_contig<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(in, out, lines, hi, lo);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (axes & 2) {
+        k_fft_strided<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(
+            (axes & 1) ? out : in, out, lines, hi, lo);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 template <int DIR>
-cudaError_t dispatch(int n, const float2 *in, float2 *out, int count, const float2 *hi,
+cudaError_t dispatch(int n, const float2 *in, float2 *out, int count, int axes, const float2 *hi,
                      const float2 *lo, cudaStream_t st) {
     switch (n) {
-        case 16: return run_n<16, DIR>(in, out, count, hi, lo, st);
-        case 32: return run_n<32, DIR>(in, out, count, hi, lo, st);
-        case 64: return run_n<64, DIR>(in, out, count, hi, lo, st);
-        case 128: return run_n<128, DIR>(in, out, count, hi, lo, st);
-        case 256: return run_n<256, DIR>(in, out, count, hi, lo, st);
-        case 512: return run_n<512, DIR>(in, out, count, hi, lo, st);
-        case 1024: return run_n<1024, DIR>(in, out, count, hi, lo, st);
-        case 2048: return run_n<2048, DIR>(in, out, count, hi, lo, st);
-        case 4096: return run_n<4096, DIR>(in, out, count, hi, lo, st);
-        case 8192: return run_n<8192, DIR>(in, out, count, hi, lo, st);
-        case 16384: return run_n<16384, DIR>(in, out, count, hi, lo, st);
+        case 16: return run_n<16, DIR>(in, out, count, axes, hi, lo, st);
+        case 32: return run_n<32, DIR>(in, out, count, axes, hi, lo, st);
+        case 64: return run_n<64, DIR>(in, out, count, axes, hi, lo, st);
+        case 128: return run_n<128, DIR>(in, out, count, axes, hi, lo, st);
+        case 256: return run_n<256, DIR>(in, out, count, axes, hi, lo, st);
+        case 512: return run_n<512, DIR>(in, out, count, axes, hi, lo, st);
+        case 1024: return run_n<1024, DIR>(in, out, count, axes, hi, lo, st);
+        case 2048: return run_n<2048, DIR>(in, out, count, axes, hi, lo, st);
+        case 4096: return run_n<4096, DIR>(in, out, count, axes, hi, lo, st);
+        case 8192: return run_n<8192, DIR>(in, out, count, axes, hi, lo, st);
+        case 16384: return run_n<16384, DIR>(in, out, count, axes, hi, lo, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -155,8 +163,19 @@ cudaError_t FftEngine::run(const float2 *in, float2 *out, int n, int count, FftD
     const float2 *hi, *lo;
     cudaError_t e = tables(n, &hi, &lo);
     if (e != cudaSuccess) return e;
-    return dir == kForward ? dispatch<-1>(n, in, out, count, hi, lo, st)
-                           : dispatch<+1>(n, in, out, count, hi, lo, st);
+    return dir == kForward ? dispatch<-1>(n, in, out, count, 3, hi, lo, st)
+                           : dispatch<+1>(n, in, out, count, 3, hi, lo, st);
+}
+
+cudaError_t FftEngine::run_axis(const float2 *in, float2 *out, int n, int count, int axis,
+                                FftDir dir, cudaStream_t st) {
+    if (!fft_supported(n) || count < 1 || (axis != 0 && axis != 1)) return cudaErrorInvalidValue;
+    const float2 *hi, *lo;
+    cudaError_t e = tables(n, &hi, &lo);
+    if (e != cudaSuccess) return e;
+    const int axes = axis == 0 ? 1 : 2;
+    return dir == kForward ? dispatch<-1>(n, in, out, count, axes, hi, lo, st)
+                           : dispatch<+1>(n, in, out, count, axes, hi, lo, st);
 }
 
 }  // namespace fpm

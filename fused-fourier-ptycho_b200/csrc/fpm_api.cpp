@@ -76,13 +76,14 @@ namespace {
 enum Stage : int {
     ST_COLS_FORWARD, ST_ROWS_FORWARD, ST_LR_COLS_INV, ST_LR_ROWS_INV, ST_LR_ROWS_FWD,
     ST_LR_COLS_FWD, ST_LOSS, ST_PUPIL_GRAD, ST_ROWS_INV, ST_COLS_UPDATE, ST_RMS_PUPIL,
-    ST_SPECTRUM, ST_TRANSPOSE, ST_LR_ROWS_FUSED, ST_COUNT
+    ST_SPECTRUM, ST_TRANSPOSE, ST_LR_ROWS_FUSED, ST_SIM_ROWS_INV, ST_SIM_MAGNITUDE, ST_COUNT
 };
 const char *const kStageName[ST_COUNT] = {
     "cols_forward", "rows_forward", "lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
     "lr_cols_forward", "loss_reduce", "pupil_grad", "rows_inverse_stitch", "cols_update",
-    "rmsprop_pupil", "spectrum_fft2", "transpose", "lr_rows_fused"};
-const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    "rmsprop_pupil", "spectrum_fft2", "transpose", "lr_rows_fused", "sim_rows_inverse",
+    "sim_magnitude"};
+const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
 
 struct Profiler {
     bool on = false;
@@ -1039,6 +1040,111 @@ fpm_status fpm_led_indices(fpm_context *ctx, const fpm_led_geometry *geo, int32_
     FPM_CK(cudaMemcpyAsync(led_idx, d_idx, (size_t)L * 8, cudaMemcpyDeviceToHost, st));
     FPM_CK(cudaStreamSynchronize(st));
     if (grid_pos) std::memcpy(grid_pos, order.data(), (size_t)L * 8);
+    return FPM_OK;
+}
+
+fpm_status fpm_simulate(fpm_context *ctx, const float *object, const float *pupil,
+                        const int32_t *led_idx, int32_t h, int32_t pratio, int32_t n_leds,
+                        int32_t output, float *out, int32_t memory) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (!object || !pupil || !led_idx || !out)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "object, pupil, led_idx and out are required");
+    if (n_leds < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "n_leds = %d", n_leds);
+    if (output != FPM_SIM_INTENSITY && output != FPM_SIM_AMPLITUDE)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output = %d", output);
+    if (memory != FPM_MEM_DEVICE && memory != FPM_MEM_HOST)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", memory);
+    if (h < 2 || pratio < 1 || (long long)h * pratio > kMaxFftLen ||
+        !pipeline_supported(h, h * pratio))
+        return fail(ctx, FPM_ERR_UNSUPPORTED,
+                    "h = %d, pratio = %d: h and h*pratio powers of two, 16..8192 and ..16384", h,
+                    pratio);
+    FPM_CK(cudaSetDevice(ctx->device));
+    const bool dev = memory == FPM_MEM_DEVICE;
+    const void *ptrs[4] = {object, pupil, led_idx, out};
+    for (int i = 0; i < 4; ++i) {
+        if (dev && (!is_device_ptr(ptrs[i], ctx->device) ||
+                    (reinterpret_cast<uintptr_t>(ptrs[i]) & 15u)))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT,
+                        "pointer %d: 16-byte aligned device memory expected", i);
+        if (!dev && !is_host_ptr(ptrs[i]))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointer %d is not host memory", i);
+    }
+    const int H = h * pratio;
+    const size_t plane = (size_t)h * h, big = (size_t)H * H;
+    const int group = (int)std::max<size_t>(1, std::min<size_t>(n_leds, (2ull << 30) / (plane * 8)));
+    const size_t need = big * 8 * (dev ? 1 : 2) + plane * 8 * (group + (dev ? 0 : 1)) +
+                        (dev ? 0 : plane * 4 * group);
+    if (ctx->mem_limit && need > ctx->mem_limit)
+        return fail(ctx, FPM_ERR_OUT_OF_MEMORY, "simulation needs %zu bytes, limit is %zu", need,
+                    ctx->mem_limit);
+    cudaStream_t st = ctx->stream;
+    if (dev) {
+        const fpm_status rc = order_after_default_stream(ctx);
+        if (rc != FPM_OK) return rc;
+    }
+    std::vector<int32_t> led_host(2 * (size_t)n_leds);
+    FPM_CK(cudaMemcpyAsync(led_host.data(), led_idx, led_host.size() * 4,
+                           dev ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    fpm_status rc = check_leds(ctx, led_host, n_leds, H);
+    if (rc != FPM_OK) return rc;
+    ctx->prof.reset();
+    const float2 *O = reinterpret_cast<const float2 *>(object);
+    const float2 *P = reinterpret_cast<const float2 *>(pupil);
+    const int2 *led = reinterpret_cast<const int2 *>(led_idx);
+    if (!dev) {
+        FPM_CK(ctx->O.ensure(big * 8));
+        FPM_CK(ctx->P.ensure(plane * 8));
+        FPM_CK(ctx->led.ensure(led_host.size() * 4));
+        FPM_CK(cudaMemcpyAsync(ctx->O.p, object, big * 8, cudaMemcpyHostToDevice, st));
+        FPM_CK(cudaMemcpyAsync(ctx->P.p, pupil, plane * 8, cudaMemcpyHostToDevice, st));
+        FPM_CK(cudaMemcpyAsync(ctx->led.p, led_host.data(), led_host.size() * 4,
+                               cudaMemcpyHostToDevice, st));
+        O = ctx->O.as<float2>();
+        P = ctx->P.as<float2>();
+        led = ctx->led.as<int2>();
+    }
+    // centred spectrum of the object (gen_img_batch.m:184, fftshift(fft2(wavefront1)))
+    FPM_CK(ctx->S.ensure(big * 8));
+    float2 *Sc = ctx->S.as<float2>();
+    FPM_STAGE(ST_SPECTRUM, ctx->fft.run(O, Sc, H, 1, kForward, st));
+    FPM_CK(launch_centre_in_place(Sc, H, st));
+    // the whole centred spectrum as the box of every LED, whole crops
+    BatchGeom g;
+    g.H = H;
+    g.h = h;
+    g.pratio = pratio;
+    g.z_off = 0;
+    g.nb = n_leds;
+    g.rlo = g.clo = 0;
+    g.rspan = g.cspan = H;
+    g.Ru0 = g.Cu0 = H / 2;
+    g.pr_lo = g.pc_lo = 0;
+    g.pr_hi = g.pc_hi = h;
+    Twiddles tw;
+    FPM_CK(ctx->fft.tables(h, &tw.lo_hi, &tw.lo_lo));
+    FPM_CK(ctx->T1.ensure(plane * 8 * group));
+    if (!dev) FPM_CK(ctx->Rs.ensure(plane * 4 * group));
+    BatchBufs b;
+    b.Sbox = Sc;
+    b.T1 = ctx->T1.as<float2>();
+    const float scale = (float)(1.0 / ((double)plane * pratio * pratio));
+    for (int l0 = 0; l0 < n_leds; l0 += group) {
+        const int nl = std::min(group, n_leds - l0);
+        // crop x pupil, ifftshift, inverse FFT along r; then along c
+        FPM_STAGE(ST_LR_COLS_INV, launch_lr_cols_inv(g, led, P, b, l0, nl, tw, st));
+        FPM_STAGE(ST_SIM_ROWS_INV, ctx->fft.run_axis(b.T1, b.T1, h, nl, 1, kInverse, st));
+        float *dst = dev ? out + plane * l0 : ctx->Rs.as<float>();
+        FPM_STAGE(ST_SIM_MAGNITUDE, launch_sim_magnitude(b.T1, plane * nl, scale,
+                                                         output == FPM_SIM_AMPLITUDE, dst, st));
+        if (!dev)
+            FPM_CK(cudaMemcpyAsync(out + plane * l0, dst, plane * 4 * nl, cudaMemcpyDeviceToHost,
+                                   st));
+    }
+    FPM_CK(cudaStreamSynchronize(st));
+    ctx->prof.collect();
     return FPM_OK;
 }
 

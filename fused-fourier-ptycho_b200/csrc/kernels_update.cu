@@ -337,4 +337,33 @@ cudaError_t launch_support_box(const float2 *P, const float *A, int h, int *box,
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Forward model output (benchmark/gen_img_batch.m:197-199): x = z * scale with z the
+// unnormalised inverse FFT and scale = 1 / (h^2 pratio^2); out = |x|^2 (intensity)
+// or |x| (amplitude), float.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_sim_magnitude(const float4 *__restrict__ z, size_t n2,
+                                                        float scale, int amplitude,
+                                                        float2 *__restrict__ out) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float4 v = z[i];
+        const float ar = v.x * scale, ai = v.y * scale, br = v.z * scale, bi = v.w * scale;
+        float2 o = make_float2(ar * ar + ai * ai, br * br + bi * bi);
+        if (amplitude) o = make_float2(sqrtf(o.x), sqrtf(o.y));
+        out[i] = o;
+    }
+}
+
+cudaError_t launch_sim_magnitude(const float2 *z, size_t n, float scale, int amplitude,
+                                 float *out, cudaStream_t st) {
+    if (n % 2) return cudaErrorInvalidValue;
+    const size_t n2 = n / 2;
+    size_t gx = (n2 + 255) / 256;
+    if (gx > (size_t)kB200SMs * 16) gx = (size_t)kB200SMs * 16;
+    k_sim_magnitude<<<(unsigned)gx, 256, 0, st>>>(reinterpret_cast<const float4 *>(z), n2, scale,
+                                                  amplitude, reinterpret_cast<float2 *>(out));
+    return cudaGetLastError();
+}
+
 }  // namespace fpm

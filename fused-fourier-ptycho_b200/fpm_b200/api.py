@@ -37,7 +37,10 @@ LOSS_ANISOTROPIC = 0
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
             "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
-            "fpm_led_indices"]
+            "fpm_led_indices", "fpm_simulate"]
+
+
+SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
 
 
 class FpmError(RuntimeError):
@@ -118,6 +121,9 @@ def load_library(path: str | Path | None = None):
     lib.fpm_fft2.restype = C.c_int
     lib.fpm_led_indices.argtypes = [C.c_void_p, C.POINTER(LedGeometry), C.c_void_p, C.c_void_p]
     lib.fpm_led_indices.restype = C.c_int
+    lib.fpm_simulate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                 C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
+    lib.fpm_simulate.restype = C.c_int
     lib.fpm_abi_version.argtypes = []
     lib.fpm_abi_version.restype = C.c_int32
     if path is None:
@@ -323,6 +329,32 @@ class Engine:
         self._check(self.lib.fpm_led_indices(self._ctx, C.byref(g), led.ctypes.data,
                                              order.ctypes.data))
         return led, order
+
+    def simulate(self, obj, pupil, led_idx, pratio, amplitude=False):
+        """Forward model (gen_img_batch.m): MATLAB-order (h, h, L) float32 intensities
+        |ifft2(ifftshift(crop(fftshift(fft2(obj))) .* pupil)) / pratio^2|^2 (or amplitudes).
+        obj (H, H) and pupil (h, h) complex64, led_idx 2 x L int32 (MATLAB ledIdx); numpy
+        in host memory or torch tensors on the context's device."""
+        os_, ok, om = _colmajor(obj, np.complex64)
+        ps, pk, pm = _colmajor(pupil, np.complex64)
+        ls, lk, lm = _colmajor(led_idx, np.int32)
+        if len({om, pm, lm}) != 1:
+            raise ValueError("all inputs must live in the same memory")
+        h = int(pupil.shape[0])
+        L = int(led_idx.shape[1])
+        like = obj if om == MEM_DEVICE else None
+        if like is not None:
+            import torch
+            base = torch.empty((L, h, h), dtype=torch.float32, device=obj.device)
+            op, out = base.data_ptr(), base.permute(2, 1, 0)
+        else:
+            out = np.empty((h, h, L), np.float32, order="F")
+            op = out.ctypes.data
+        _inputs_ready(ok, pk, lk)
+        self._check(self.lib.fpm_simulate(self._ctx, os_, ps, ls, h, int(pratio), L,
+                                          SIM_AMPLITUDE if amplitude else SIM_INTENSITY, op, om))
+        del ok, pk, lk
+        return out
 
     def normalise_stack(self, counts):
         """Amplitude sqrt((I-min)/(max-min)) of a uint16 stack, same shape, float32."""

@@ -202,6 +202,21 @@ typedef struct fpm_led_geometry {
 fpm_status fpm_led_indices(fpm_context *ctx, const fpm_led_geometry *geo, int32_t *led_idx,
                            int32_t *grid_pos);
 
+/* Forward model of the reference's data generator (benchmark/gen_img_batch.m:178-201,
+   fpm_forward_gen): for every LED l,
+       x_l = ifft2(ifftshift(crop_l(fftshift(fft2(object))) .* pupil)) / pratio^2
+   with crop_l the h x h window at led_idx[l] = (kl, kt) of the centred spectrum
+   (1-based corner, wrapping modulo H as in fpm_problem), and out page l = |x_l|^2
+   (FPM_SIM_INTENSITY) or |x_l| (FPM_SIM_AMPLITUDE).  object: complex H*H (H = h *
+   pratio), pupil: complex h*h, led_idx: 2*n_leds int32, out: float h*h*n_leds; all
+   column-major, pointers follow `memory`.  h and H: powers of two (16..8192, ..16384).
+   The transforms are the engine's own; used to make training / test data and to
+   check a reconstruction against its measurements. */
+typedef enum fpm_sim_output { FPM_SIM_INTENSITY = 0, FPM_SIM_AMPLITUDE = 1 } fpm_sim_output;
+fpm_status fpm_simulate(fpm_context *ctx, const float *object, const float *pupil,
+                        const int32_t *led_idx, int32_t h, int32_t pratio, int32_t n_leds,
+                        int32_t output, float *out, int32_t memory);
+
 void fpm_destroy(fpm_context *ctx);
 
 /* Per-stage device timing (no counterpart in the reference, which only times

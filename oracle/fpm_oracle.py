@@ -427,3 +427,33 @@ def led_geometry(grid: int, h: int, pratio: int, wavelength_um: float, led_pitch
         vo = nearest(k_lamuda * v)
         out.append((uo - h // 2, vo - h // 2))
     return np.asarray(out, np.int32), np.asarray(order, np.int32)
+
+
+# ---------------------------------------------------------------------------
+# forward model (restated for checking the device simulator)
+# ---------------------------------------------------------------------------
+
+def forward_model(O, P, led_idx, pratio: int, amplitude: bool = False, dtype=np.float64):
+    """Images of every LED, (L, h, h) [l, r, c]: ``benchmark/gen_img_batch.m:178-201``.
+
+    ``ft = fftshift(fft2(O))`` (:184 with the shift made explicit, as its caller
+    passes the centred spectrum), the LED's h x h window with its 1-based
+    top-left corner at (kt, kl) taken modulo H like the solver's crop
+    (``cuFPM_v3/cuda/kernels.cuh:43-47``), times the pupil, ``x =
+    ifft2(ifftshift(.)) / pratio^2`` (:197), and ``|x|^2`` (the intensity the
+    data sets hold) or ``abs(x)`` (:199).
+    """
+    cdt = np.complex128 if dtype == np.float64 else np.complex64
+    O = np.asarray(O, cdt)
+    P = np.asarray(P, cdt)
+    H = O.shape[0]
+    h = P.shape[0]
+    F = np.fft.fftshift(np.fft.fft2(O))
+    out = np.empty((len(led_idx), h, h), dtype)
+    ar = np.arange(h)
+    for l, (kl, kt) in enumerate(np.asarray(led_idx)):
+        sub = F[np.ix_((kt - 1 + ar) % H, (kl - 1 + ar) % H)] * P
+        x = np.fft.ifft2(np.fft.ifftshift(sub)) / (pratio * pratio)
+        a = np.abs(x)
+        out[l] = a if amplitude else a * a
+    return out

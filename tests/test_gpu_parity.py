@@ -420,3 +420,38 @@ def test_pupil_support_pruning_is_exact(engine, ds_small):
     o64 = orc.cufpm_pure_v3(ds.O0, P0c, ds.Y[:25], ds.led_idx[:25], P0, ds.pratio, 2, 6,
                             opt=(2e-3, 0.999, 1e-4))
     assert orc.rel_err(pruned["object"], o64.object) < 2e-2
+
+
+@pytest.mark.parametrize("h,p,amplitude", [(64, 4, False), (32, 2, True), (256, 8, False)])
+def test_simulate_matches_oracle(engine, h, p, amplitude):
+    """Device forward model against the FP64 oracle, crops inside and past the edge."""
+    rng = np.random.default_rng(h + p)
+    H = h * p
+    O = (0.5 + 0.5 * rng.random((H, H))) * np.exp(1j * rng.standard_normal((H, H)))
+    from fpm_b200 import synth
+    P = synth.pupil_circle(h, synth.Optics(led_grid=5)) * np.exp(0.3j * rng.standard_normal((h, h)))
+    led = np.concatenate([rng.integers(1, H + 1, size=(9, 2)),
+                          np.array([[1, 1], [H, H], [H - h // 2, 3]])]).astype(np.int32)
+    got = engine.simulate(O.astype(np.complex64), P.astype(np.complex64), led_matlab(led), p,
+                          amplitude=amplitude)
+    ref = orc.forward_model(O, P, led, p, amplitude=amplitude)
+    assert got.shape == (h, h, len(led))
+    e = orc.rel_err(np.transpose(got, (2, 0, 1)), ref)
+    assert e < 2e-6 * max(1.0, np.log2(H) / 8), e
+
+
+def test_simulate_device_memory_and_bad_input(engine):
+    import torch
+    rng = np.random.default_rng(5)
+    h, p = 64, 2
+    H = h * p
+    O = (rng.standard_normal((H, H)) + 1j * rng.standard_normal((H, H))).astype(np.complex64)
+    P = np.ones((h, h), np.complex64)
+    led = led_matlab(np.array([[5, 9], [H, 1]], np.int32))
+    host = engine.simulate(O, P, led, p)
+    dev = engine.simulate(torch.from_numpy(O).cuda(), torch.from_numpy(P).cuda(),
+                          torch.from_numpy(led).cuda(), p).cpu().numpy()
+    np.testing.assert_array_equal(host, dev)
+    with pytest.raises(fpm_b200.FpmError) as e:
+        engine.simulate(O, P, led_matlab(np.array([[0, 1]], np.int32)), p)   # kl = 0
+    assert e.value.status == 1

@@ -210,6 +210,27 @@ def test_geometry_off_axis_sample_area():
     assert s[0, 0] > c[0, 0] and s[0, 1] > c[0, 1]   # u <- +dx, v <- -(-dy) after the swap
 
 
+def test_forward_model_matches_generator_statements():
+    """The oracle's forward model against the data generator's (gen_img_batch.m:194-200)
+    and a literal slice transcription for crops inside the spectrum."""
+    rng = np.random.default_rng(3)
+    h, p = 16, 4
+    H = h * p
+    O = rng.standard_normal((H, H)) + 1j * rng.standard_normal((H, H))
+    P = synth.pupil_circle(h, synth.Optics(led_grid=3)) * np.exp(0.2j * rng.standard_normal((h, h)))
+    led = np.array([[20, 17], [1, 1], [H - 5, 30], [H, H]], np.int32)
+    I = orc.forward_model(O, P, led, p)
+    spec = np.fft.fftshift(np.fft.fft2(O)).astype(np.complex64)
+    np.testing.assert_allclose(I, synth.forward_intensity(spec, P.astype(np.complex64), led, p),
+                               rtol=1e-4, atol=1e-6 * I.max())
+    F = np.fft.fftshift(np.fft.fft2(O))
+    kl, kt = led[0]
+    x = np.fft.ifft2(np.fft.ifftshift(F[kt - 1:kt - 1 + h, kl - 1:kl - 1 + h] * P)) / p ** 2
+    np.testing.assert_allclose(I[0], np.abs(x) ** 2, rtol=1e-12)
+    np.testing.assert_allclose(orc.forward_model(O, P, led, p, amplitude=True), np.sqrt(I),
+                               rtol=1e-12)
+
+
 def test_bicubic_restatements_agree_and_keep_constants():
     rng = np.random.default_rng(7)
     img = rng.random((12, 12))
