@@ -269,8 +269,8 @@ fpm_status validate(fpm_context *ctx, const fpm_problem *p, bool need_batch) {
     if (std::min(p->batch, p->n_leds) > 1024 && need_batch)
         return fail(ctx, FPM_ERR_UNSUPPORTED, "batch of %d LEDs exceeds 1024",
                     std::min(p->batch, p->n_leds));
-    if (p->loss_kind != FPM_LOSS_ANISOTROPIC)
-        return fail(ctx, FPM_ERR_UNSUPPORTED, "loss_kind %d not supported", p->loss_kind);
+    if (p->loss_kind != FPM_LOSS_ANISOTROPIC && p->loss_kind != FPM_LOSS_ISOTROPIC)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "loss_kind %d", p->loss_kind);
     if (p->memory != FPM_MEM_HOST && p->memory != FPM_MEM_DEVICE)
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", p->memory);
     if (p->stack_type != FPM_STACK_F32_AMPLITUDE && p->stack_type != FPM_STACK_U16_COUNTS)
@@ -396,7 +396,8 @@ struct Plan {
 };
 
 
-Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const Support &sup) {
+Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const Support &sup,
+               int loss) {
     Plan pl;
     for (int cur = 0; cur < s.L; cur += batch) {
         const int nb = std::min(batch, s.L - cur);
@@ -417,6 +418,7 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const
         g.pr_hi = sup.r_hi;
         g.pc_lo = sup.c_lo;
         g.pc_hi = sup.c_hi;
+        g.loss = loss == FPM_LOSS_ISOTROPIC ? kLossIsotropic : kLossAnisotropic;
         pl.geoms.push_back(g);
         pl.ldU = std::max(pl.ldU, g.rspan);
         pl.sbox = std::max(pl.sbox, (size_t)g.rspan * g.cspan);
@@ -746,7 +748,7 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     Support sup;
     rc = pupil_support(ctx, p, s, sup);
     if (rc != FPM_OK) return rc;
-    const Plan pl = make_plan(s, led_host, p->batch, sup);
+    const Plan pl = make_plan(s, led_host, p->batch, sup, p->loss_kind);
     rc = alloc_pipeline(ctx, p, s, pl, res->spectrum != nullptr);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;
@@ -906,7 +908,7 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
     if (rc != FPM_OK) return rc;
     Support full;   // the pupil gradient is an output here: whole crops
     full.r_hi = full.c_hi = s.h;
-    const Plan pl = make_plan(s, led_host, s.L, full);
+    const Plan pl = make_plan(s, led_host, s.L, full, p->loss_kind);
     rc = alloc_pipeline(ctx, p, s, pl, true);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;

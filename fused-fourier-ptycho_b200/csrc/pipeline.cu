@@ -63,6 +63,36 @@ cudaError_t set_smem(K kernel, int bytes) {
                                 cudaSharedmemCarveoutMaxShared);
 }
 
+// Loss-gradient stencil at one pixel from the residuals around it:
+// a = res(r, c), right = res(r, c+1), left = res(r, c-1), down = res(r+1, c),
+// up = res(r-1, c), dl = res(r+1, c-1), ur = res(r-1, c+1).  Returns d (before the
+// pratio^2 scale) and adds the pixel's loss term to lsum.
+//   anisotropic (v3, kernels.cuh:234-263): sign(Rx(c-1)) - sign(Rx) + sign(Ry(r-1)) - sign(Ry)
+//   isotropic (codes/func_ware/misc/ret_loss.m:7-11,18-19): ox = Rx / (|R| + 1e-5),
+//     oy = Ry / (|R| + 1e-5), d = (ox(c-1) - ox) + (oy(r-1) - oy), loss |R| = sqrt(Rx²+Ry²)
+template <int LOSS>
+__device__ __forceinline__ float stencil(float a, float right, float left, float down, float up,
+                                         float dl, float ur, double &lsum) {
+    const float rx = right - a;                  // Rx(r, c)
+    const float ry = down - a;                   // Ry(r, c)
+    if (LOSS == kLossAnisotropic) {
+        const float oxm = sign1(a - left);       // sign Rx(r, c-1)
+        const float oym = sign1(a - up);         // sign Ry(r-1, c)
+        lsum += (double)fabsf(rx) + (double)fabsf(ry);
+        return oxm - sign1(rx) + oym - sign1(ry);
+    } else {
+        const float n = sqrtf(__fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)));
+        const float den = n + 1e-5f;
+        const float ox = rx / den, oy = ry / den;
+        const float rxm = a - left, rym = dl - left;       // R(r, c-1) differences
+        const float oxm = rxm / (sqrtf(__fadd_rn(__fmul_rn(rxm, rxm), __fmul_rn(rym, rym))) + 1e-5f);
+        const float ryu = a - up, rxu = ur - up;           // R(r-1, c) differences
+        const float oyu = ryu / (sqrtf(__fadd_rn(__fmul_rn(rxu, rxu), __fmul_rn(ryu, ryu))) + 1e-5f);
+        lsum += (double)n;
+        return (oxm - ox) + (oyu - oy);
+    }
+}
+
 template <int TYPE>
 __device__ __forceinline__ float amplitude(const StackView &Y, size_t idx, float mn, float range) {
     if (TYPE == kStackF32) return static_cast<const float *>(Y.ptr)[idx];
@@ -174,7 +204,7 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 // ---------------------------------------------------------------------------
 // L3: sign stencil of the residual, phase, forward FFT along c (strided rows)
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, int LOSS>
 __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     k_lr_rows_fwd(BatchGeom g, int nl, float2 *__restrict__ T1, const float *__restrict__ Rs,
                   double *__restrict__ parts, const float2 *__restrict__ thi,
@@ -200,13 +230,12 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
         float2 o = make_float2(0.f, 0.f);
         if (live) {
             const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
-            const float a = rp[(size_t)c * N + r];
-            const float rx = rp[(size_t)cp * N + r] - a;     // res(r, c+1) - res(r, c)
-            const float ry = rp[(size_t)c * N + rpp] - a;    // res(r+1, c) - res(r, c)
-            const float oxm = sign1(a - rp[(size_t)cm * N + r]);
-            const float oym = sign1(a - rp[(size_t)c * N + rmm]);
-            const float d = (oxm - sign1(rx) + oym - sign1(ry)) * gscale;
-            lsum += (double)fabsf(rx) + (double)fabsf(ry);
+            const float d =
+                stencil<LOSS>(rp[(size_t)c * N + r], rp[(size_t)cp * N + r], rp[(size_t)cm * N + r],
+                              rp[(size_t)c * N + rpp], rp[(size_t)c * N + rmm],
+                              LOSS == kLossAnisotropic ? 0.f : rp[(size_t)cm * N + rpp],
+                              LOSS == kLossAnisotropic ? 0.f : rp[(size_t)cp * N + rmm], lsum) *
+                gscale;
             const float2 z = page[(size_t)c * N];
             const float mag = sqrtf(z.x * z.x + z.y * z.y);
             if (mag > 0.f) {
@@ -273,7 +302,7 @@ struct L23 {
     static_assert(LINE_BYTES % 128 == 0, "residual area 128-byte aligned for TMA");
 };
 
-template <int N, int TYPE>
+template <int N, int TYPE, int LOSS>
 __global__ void __launch_bounds__(1024, 1)
     k_lr_rows_fused(StackView Y, BatchGeom g, int l0, const float2 *__restrict__ T1,
                     float2 *__restrict__ T2, double *__restrict__ parts, int *__restrict__ flag,
@@ -387,13 +416,11 @@ __global__ void __launch_bounds__(1024, 1)
         float2 o = make_float2(0.f, 0.f);
         if (central) {
             const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
-            const float a = rk[c];
-            const float rx = rk[cp] - a;                    // res(r, c+1) - res(r, c)
-            const float ry = rk[F::RSTRIDE + c] - a;        // res(r+1, c) - res(r, c)
-            const float oxm = sign1(a - rk[cm]);
-            const float oym = sign1(a - rk[c - F::RSTRIDE]);
-            const float d = (oxm - sign1(rx) + oym - sign1(ry)) * gscale;
-            lsum += (double)fabsf(rx) + (double)fabsf(ry);
+            const float d =
+                stencil<LOSS>(rk[c], rk[cp], rk[cm], rk[F::RSTRIDE + c], rk[c - F::RSTRIDE],
+                              LOSS == kLossAnisotropic ? 0.f : rk[F::RSTRIDE + cm],
+                              LOSS == kLossAnisotropic ? 0.f : rk[cp - F::RSTRIDE], lsum) *
+                gscale;
             const float2 z = v[m];
             const float mag = sqrtf(z.x * z.x + z.y * z.y);
             if (mag > 0.f) {
@@ -767,10 +794,17 @@ cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, 
     const int blocks = lr_blocks(g.h, nl);
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                              \
-    e = set_smem(k_lr_rows_fwd<N>, smem_bytes<N>());                                      \
-    if (e != cudaSuccess) return e;                                                       \
-    k_lr_rows_fwd<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                   \
-        g, nl, b.T1, b.Rs, b.parts + part_off, tw.lo_hi, tw.lo_lo);
+    if (g.loss == kLossIsotropic) {                                                       \
+        e = set_smem(k_lr_rows_fwd<N, kLossIsotropic>, smem_bytes<N>());                  \
+        if (e != cudaSuccess) return e;                                                   \
+        k_lr_rows_fwd<N, kLossIsotropic><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>( \
+            g, nl, b.T1, b.Rs, b.parts + part_off, tw.lo_hi, tw.lo_lo);                   \
+    } else {                                                                              \
+        e = set_smem(k_lr_rows_fwd<N, kLossAnisotropic>, smem_bytes<N>());                \
+        if (e != cudaSuccess) return e;                                                   \
+        k_lr_rows_fwd<N, kLossAnisotropic><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>( \
+            g, nl, b.T1, b.Rs, b.parts + part_off, tw.lo_hi, tw.lo_lo);                   \
+    }
     FPM_DISPATCH_LR(g.h, F)
 #undef F
     return cudaGetLastError();
@@ -827,6 +861,17 @@ static cudaError_t page_tile_map(CUtensorMap *map, CUtensorMapDataType type, siz
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+template <int N, int TYPE, int LOSS>
+static cudaError_t launch_fused_k(int blocks, StackView Y, const BatchGeom &g, int l0,
+                                  const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
+                                  const CUtensorMap &tm_stack, const Twiddles &tw, cudaStream_t st) {
+    cudaError_t e = set_smem(k_lr_rows_fused<N, TYPE, LOSS>, L23<N>::SMEM);
+    if (e != cudaSuccess) return e;
+    k_lr_rows_fused<N, TYPE, LOSS><<<blocks, 1024, L23<N>::SMEM, st>>>(
+        Y, g, l0, b.T1, b.T2, b.parts + part_off, b.flag, tm_field, tm_stack, tw.lo_hi, tw.lo_lo);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_pages, BatchBufs b,
                                  int l0, int nl, int part_off, const Twiddles &tw,
                                  cudaStream_t st) {
@@ -843,18 +888,19 @@ cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_page
         e = page_tile_map(&tm_stack, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, Y.ptr, N,         \
                           stack_pages, L23<N>::YR, L23<N>::CB);                           \
         if (e != cudaSuccess) return e;                                                   \
-        e = set_smem(k_lr_rows_fused<N, kStackU16>, L23<N>::SMEM);                        \
-        if (e != cudaSuccess) return e;                                                   \
-        k_lr_rows_fused<N, kStackU16><<<blocks, 1024, L23<N>::SMEM, st>>>(                \
-            Y, g, l0, b.T1, b.T2, b.parts + part_off, b.flag, tm_field, tm_stack,         \
-            tw.lo_hi, tw.lo_lo);                                                          \
+        e = g.loss == kLossIsotropic                                                      \
+                ? launch_fused_k<N, kStackU16, kLossIsotropic>(blocks, Y, g, l0, b, part_off, \
+                                                               tm_field, tm_stack, tw, st)    \
+                : launch_fused_k<N, kStackU16, kLossAnisotropic>(blocks, Y, g, l0, b, part_off, \
+                                                                 tm_field, tm_stack, tw, st); \
     } else {                                                                              \
-        e = set_smem(k_lr_rows_fused<N, kStackF32>, L23<N>::SMEM);                        \
-        if (e != cudaSuccess) return e;                                                   \
-        k_lr_rows_fused<N, kStackF32><<<blocks, 1024, L23<N>::SMEM, st>>>(                \
-            Y, g, l0, b.T1, b.T2, b.parts + part_off, b.flag, tm_field, tm_stack,         \
-            tw.lo_hi, tw.lo_lo);                                                          \
-    }
+        e = g.loss == kLossIsotropic                                                      \
+                ? launch_fused_k<N, kStackF32, kLossIsotropic>(blocks, Y, g, l0, b, part_off, \
+                                                               tm_field, tm_stack, tw, st)    \
+                : launch_fused_k<N, kStackF32, kLossAnisotropic>(blocks, Y, g, l0, b, part_off, \
+                                                                 tm_field, tm_stack, tw, st); \
+    }                                                                                     \
+    if (e != cudaSuccess) return e;
     FPM_DISPATCH_FUSED(g.h, F)
 #undef F
     return cudaGetLastError();

@@ -8,6 +8,8 @@
 
 namespace fpm {
 
+enum LossKind : int { kLossAnisotropic = 0, kLossIsotropic = 1 };
+
 // One mini-batch's crop box.  Centred rows [rlo, rlo + rspan) and columns
 // [clo, clo + cspan), modulo H; Ru0 / Cu0 are the matching un-shifted starts.
 struct BatchGeom {
@@ -19,6 +21,7 @@ struct BatchGeom {
     // which the pupil is zero: the crop there contributes nothing and the gradient
     // spectrum there is never used, so the box above covers only this part of each crop
     int pr_lo = 0, pr_hi = 0, pc_lo = 0, pc_hi = 0;
+    int loss = 0;   // LossKind
 };
 
 // Two-level twiddle tables (fft_core.cuh) for the low-res length h and the large length H.

@@ -31,7 +31,8 @@ STATUS_NAMES = {0: "FPM_OK", 1: "FPM_ERR_INVALID_ARGUMENT", 2: "FPM_ERR_UNSUPPOR
                 6: "FPM_ERR_NO_DEVICE", 7: "FPM_ERR_INTERNAL"}
 MEM_HOST, MEM_DEVICE = 0, 1
 STACK_F32, STACK_U16 = 0, 1
-LOSS_ANISOTROPIC = 0
+LOSS_ANISOTROPIC, LOSS_ISOTROPIC = 0, 1
+_LOSS = {"anisotropic": LOSS_ANISOTROPIC, "isotropic": LOSS_ISOTROPIC}
 
 # Every symbol include/fpm.h declares.
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
@@ -229,7 +230,7 @@ class Engine:
 
     # -- MATLAB-shaped entry points --------------------------------------------
     def _problem(self, O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr, beta, eps, am,
-                 lr_halve_after, lr_decay):
+                 lr_halve_after, lr_decay, loss="anisotropic"):
         keep = []
         y_is_u16 = (str(getattr(Y, "dtype", "")).endswith("uint16"))
         ydt = np.uint16 if y_is_u16 else np.float32
@@ -253,16 +254,18 @@ class Engine:
         L = int(shp[2]) if len(shp) == 3 else 1
         prob = Problem(h=h, n_leds=L, pratio=int(pratio), batch=int(batch), epochs=int(epochs),
                        lr=lr, beta=beta, eps=eps, pupil_margin=am, lr_halve_after=lr_halve_after,
-                       lr_decay=lr_decay, loss_kind=LOSS_ANISOTROPIC, memory=ymem,
+                       lr_decay=lr_decay, loss_kind=_LOSS[loss], memory=ymem,
                        stack_type=STACK_U16 if y_is_u16 else STACK_F32, stack=ys, led_idx=ls,
                        pupil_init=ps, pupil_amp=as_, object_init=os_)
         return prob, keep, ymem
 
     def solve(self, O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr=5e-4, beta=0.999,
-              eps=1e-4, am=0.2, lr_halve_after=12, lr_decay=0.5, spectrum=True):
-        """Full reconstruction; returns dict(object, pupil, spectrum, loss) in MATLAB order."""
+              eps=1e-4, am=0.2, lr_halve_after=12, lr_decay=0.5, spectrum=True,
+              loss="anisotropic"):
+        """Full reconstruction; returns dict(object, pupil, spectrum, loss) in MATLAB order.
+        loss: "anisotropic" (the v3 mex) or "isotropic" (ret_loss.m)."""
         prob, keep, mem = self._problem(O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr,
-                                        beta, eps, am, lr_halve_after, lr_decay)
+                                        beta, eps, am, lr_halve_after, lr_decay, loss)
         h = prob.h
         H = h * prob.pratio
         like = Y if mem == MEM_DEVICE else None
@@ -278,10 +281,10 @@ class Engine:
         del keep
         return {"object": o, "pupil": p, "spectrum": s, "loss": loss[: int(epochs)]}
 
-    def batch_gradients(self, O, P, Y, led_idx, P0, pratio):
+    def batch_gradients(self, O, P, Y, led_idx, P0, pratio, loss="anisotropic"):
         """v3 gradients of one LED batch (the fullyfusedFPM contract): (dO, dP, loss)."""
         prob, keep, mem = self._problem(O, P, Y, led_idx, P0, pratio, 0, 1, 0.0, 0.0, 0.0, 0.0,
-                                        12, 0.5)
+                                        12, 0.5, loss)
         h = prob.h
         H = h * prob.pratio
         like = Y if mem == MEM_DEVICE else None

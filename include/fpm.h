@@ -73,7 +73,11 @@ typedef enum fpm_stack_type {
 typedef enum fpm_loss_kind {
     /* sum |d/dx (|x| - Y)| + |d/dy (|x| - Y)| with periodic forward differences,
        sign(0) = +1 (cuFPM_v3/cuda/kernels.cuh:197-275, benchmark/func_ware/ret_loss.m) */
-    FPM_LOSS_ANISOTROPIC = 0
+    FPM_LOSS_ANISOTROPIC = 0,
+    /* sum sqrt(Rx^2 + Ry^2) of the same differences, gradient through
+       R/(|R| + 1e-5) (codes/func_ware/misc/ret_loss.m 'isotropic', the loss of
+       benchmark/func_ware/fpm_forward_GPU.m:38); no counterpart in the v3 mex */
+    FPM_LOSS_ISOTROPIC = 1
 } fpm_loss_kind;
 
 typedef struct fpm_device_opts {

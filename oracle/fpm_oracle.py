@@ -113,8 +113,11 @@ def residual(z, Y_l, h: int, pratio: int, dtype):
     return abs_c(z, dtype) / ratio - Y_l.astype(dtype, copy=False)
 
 
-def feature_grad(res, pratio: int, dtype):
-    """Anisotropic feature-domain gradient of ``Σ|∂c res| + |∂r res|``.
+def feature_grad(res, pratio: int, dtype, loss: str = "anisotropic"):
+    """Feature-domain gradient of the residual; ``loss="isotropic"`` selects
+    :func:`feature_grad_isotropic`.
+
+    Anisotropic: gradient of ``Σ|∂c res| + |∂r res|``.
 
     ``differenceKernel_acc``, ``kernels.cuh:234-263``; MATLAB statement in
     ``benchmark/func_ware/ret_loss.m:3-4,11-12,18-19`` with periodic forward
@@ -122,6 +125,8 @@ def feature_grad(res, pratio: int, dtype):
     Returns ``(d, loss)`` with ``d = (ox(c-1)-ox(c) + oy(r-1)-oy(r))·pratio²``
     and ``loss = Σ |Rx| + |Ry|`` (accumulated in float64).
     """
+    if loss == "isotropic":
+        return feature_grad_isotropic(res, pratio, dtype)
     rx = np.roll(res, -1, axis=1) - res          # res(:, c+1) - res(:, c)
     ry = np.roll(res, -1, axis=0) - res          # res(r+1, :) - res(r, :)
     ox = sign_copysign(rx)
@@ -129,6 +134,25 @@ def feature_grad(res, pratio: int, dtype):
     d = ((np.roll(ox, 1, axis=1) - ox) + (np.roll(oy, 1, axis=0) - oy)) * dtype(pratio * pratio)
     loss = float(np.abs(rx.astype(np.float64)).sum() + np.abs(ry.astype(np.float64)).sum())
     return d.astype(dtype, copy=False), loss
+
+
+def feature_grad_isotropic(res, pratio: int, dtype):
+    """Isotropic feature-domain gradient of ``Σ sqrt(Rx² + Ry²)``.
+
+    ``codes/func_ware/misc/ret_loss.m:7-11,18-19`` ('isotropic', the loss the
+    benchmark's ``fpm_forward_GPU.m:38`` selects): ``den = sqrt(Rx² + Ry²) + 1e-5``,
+    ``ox = Rx/den``, ``oy = Ry/den``, ``out = ox(c-1) - ox(c) + oy(r-1) - oy(r)``;
+    the caller scales by ``pratio²`` as for the anisotropic loss (``:41``).  In the
+    working precision, one rounding per operation in this order.
+    """
+    rx = np.roll(res, -1, axis=1) - res
+    ry = np.roll(res, -1, axis=0) - res
+    n = np.sqrt(rx * rx + ry * ry)
+    den = n + dtype(1e-5)
+    ox = rx / den
+    oy = ry / den
+    d = ((np.roll(ox, 1, axis=1) - ox) + (np.roll(oy, 1, axis=0) - oy)) * dtype(pratio * pratio)
+    return d.astype(dtype, copy=False), float(n.astype(np.float64).sum())
 
 
 def phase_times(z, d, dtype):
@@ -182,7 +206,8 @@ def pupil_clamp(w, P0, am, dtype):
 # one LED batch (cuFPM_pure_v3.cu:135-199)
 # ---------------------------------------------------------------------------
 
-def batch_gradients(S, P, Y_b, leds_b, pratio: int, dtype, workers: int = 1):
+def batch_gradients(S, P, Y_b, leds_b, pratio: int, dtype, workers: int = 1,
+                    loss_kind: str = "anisotropic"):
     """Gradients of one LED batch at the current object spectrum ``S``.
 
     ``S`` is the *un-shifted* FFT2 of the object (``cuFPM_pure_v3.cu:135-140``).
@@ -208,7 +233,7 @@ def batch_gradients(S, P, Y_b, leds_b, pratio: int, dtype, workers: int = 1):
         z = (_ifft2(lat, workers) * ctype(h * h)).astype(ctype, copy=False)
         # K4: feature-domain loss gradient (kernels.cuh:197-275)
         res = residual(z, Y_b[l], h, pratio, dtype)
-        d, lval = feature_grad(res, pratio, dtype)
+        d, lval = feature_grad(res, pratio, dtype, loss_kind)
         loss += lval
         rec = phase_times(z, d, dtype)
         # K5: unnormalised forward FFT (cuFPM_pure_v3.cu:164-169), read shifted
@@ -235,14 +260,16 @@ class OracleResult:
 
 def cufpm_pure_v3(O0, P0c, Y, led_idx, P0, pratio: int, epochs: int, batch: int,
                   opt=(5e-4, 0.999, 1e-4), am: float = 0.2, lr_halve_after: int = 12,
-                  dtype=np.float64, workers: int | None = None) -> OracleResult:
+                  dtype=np.float64, workers: int | None = None,
+                  loss_kind: str = "anisotropic") -> OracleResult:
     """Oracle of ``[O, P] = cuFPM_pure_v3(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, [lr beta eps])``.
 
     ``Y`` is ``(L, h, h)`` amplitude (page ``l`` = LED ``l``, the reference's
     ``h x h x L`` MATLAB array with the page axis moved first).  The
     hyper-parameters are rounded to float32 first, as the mex does
     (``cuFPM_pure_v3.cu:63-65``).  Returns the object, pupil, the centred
-    spectrum ``fftshift(fft2(O))`` and the per-epoch loss.
+    spectrum ``fftshift(fft2(O))`` and the per-epoch loss.  ``loss_kind``
+    "isotropic" swaps the v3 loss for :func:`feature_grad_isotropic`.
     """
     if workers is None:
         workers = default_workers()
@@ -267,7 +294,7 @@ def cufpm_pure_v3(O0, P0c, Y, led_idx, P0, pratio: int, epochs: int, batch: int,
             nb = min(batch, L - cur)
             S = _fft2(O, workers).astype(ctype, copy=False)
             G, dP, lv = batch_gradients(S, P, Y[cur:cur + nb], led_idx[cur:cur + nb],
-                                        pratio, dtype, workers)
+                                        pratio, dtype, workers, loss_kind)
             losses[ep] += lv
             # K8: unnormalised inverse FFT of G (the 1/H² is already inside G)
             g = (_ifft2(G, workers) * ctype(H * H)).astype(ctype, copy=False)

@@ -455,3 +455,34 @@ def test_simulate_device_memory_and_bad_input(engine):
     with pytest.raises(fpm_b200.FpmError) as e:
         engine.simulate(O, P, led_matlab(np.array([[0, 1]], np.int32)), p)   # kl = 0
     assert e.value.status == 1
+
+
+def test_isotropic_loss_gradients_and_solve(engine, ds_small, ds_a):
+    """The isotropic loss (ret_loss.m 'isotropic'): no sign decisions, so the FP32 engine
+    tracks the FP64 oracle closely; both the separate (h = 64) and fused (h = 128) row
+    passes run it."""
+    for ds in (ds_small, ds_a):
+        H = ds.h * ds.pratio
+        rng = np.random.default_rng(21)
+        O = (ds.O0 * np.exp(1j * 0.2 * rng.standard_normal((H, H)))).astype(np.complex64)
+        P = ds.pupil_true
+        sel = slice(0, 9)
+        dO, dP, loss = engine.batch_gradients(O, P, to_matlab_stack(ds.Y[sel]),
+                                              led_matlab(ds.led_idx[sel]), ds.pupil0, ds.pratio,
+                                              loss="isotropic")
+        G, dP64, l64 = orc.batch_gradients(np.fft.fft2(O.astype(np.complex128)),
+                                           P.astype(np.complex128), ds.Y[sel].astype(np.float64),
+                                           ds.led_idx[sel], ds.pratio, np.float64,
+                                           loss_kind="isotropic")
+        assert abs(loss - l64) < 1e-6 * abs(l64)
+        assert orc.rel_err(dO, np.fft.ifft2(G) * H * H) < TIGHT
+        assert orc.rel_err(dP, dP64) < TIGHT
+        opt = (1e-3, 0.999, 1e-4)
+        r = engine.solve(ds.O0, ds.P0c, to_matlab_stack(ds.Y[:16]), led_matlab(ds.led_idx[:16]),
+                         ds.pupil0, ds.pratio, 2, 8, lr=opt[0], beta=opt[1], eps=opt[2],
+                         loss="isotropic")
+        o = orc.cufpm_pure_v3(ds.O0, ds.P0c, ds.Y[:16], ds.led_idx[:16], ds.pupil0, ds.pratio, 2, 8,
+                              opt=opt, loss_kind="isotropic")
+        assert orc.rel_err(r["object"], o.object) < TIGHT      # the FP32 twin: 2.6e-7
+        assert orc.rel_err(r["pupil"], o.pupil) < TIGHT
+        np.testing.assert_allclose(r["loss"], o.loss, rtol=1e-6)

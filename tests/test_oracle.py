@@ -99,6 +99,30 @@ def test_feature_grad_matches_ret_loss():
     np.testing.assert_array_equal(d, outm * 16)
 
 
+def m_ret_loss_isotropic(dW):  # codes/func_ware/misc/ret_loss.m:3-11,18-21, 'isotropic'
+    RxdW = np.concatenate([dW[:, 1:] - dW[:, :-1], dW[:, :1] - dW[:, -1:]], axis=1)
+    RydW = np.concatenate([dW[1:, :] - dW[:-1, :], dW[:1, :] - dW[-1:, :]], axis=0)
+    den = np.sqrt(RxdW ** 2 + RydW ** 2) + 1e-5
+    loss = np.sqrt(RxdW ** 2 + RydW ** 2)
+    ox = RxdW / den
+    oy = RydW / den
+    out = np.concatenate([ox[:, -1:] - ox[:, :1], ox[:, :-1] - ox[:, 1:]], axis=1)
+    out = out + np.concatenate([oy[-1:, :] - oy[:1, :], oy[:-1, :] - oy[1:, :]], axis=0)
+    return loss.sum(), out
+
+
+def test_feature_grad_isotropic_matches_ret_loss():
+    rng = np.random.default_rng(12)
+    res = rng.standard_normal((16, 24))
+    d, loss = orc.feature_grad(res, 4, np.float64, "isotropic")
+    lm, outm = m_ret_loss_isotropic(res)
+    np.testing.assert_allclose(loss, lm, rtol=1e-13)
+    np.testing.assert_allclose(d, outm * 16, rtol=1e-12, atol=1e-12)
+    # the FP32 twin tracks it to single-precision rounding
+    d32, l32 = orc.feature_grad(res.astype(np.float32), 4, np.float32, "isotropic")
+    np.testing.assert_allclose(d32, outm * 16, rtol=1e-4, atol=1e-5)
+
+
 def test_feature_grad_sign_of_zero_is_plus_one():
     # v3 uses copysignf(1, x) (kernels.cuh:11-15): equal neighbours give +1, MATLAB gives 0
     res = np.zeros((4, 4))
