@@ -37,7 +37,10 @@ cudaError_t launch_centre_in_place(float2 *S, int H, cudaStream_t st);
 // out[c*ldo + r] = in[r*ldi + c] (r < rows, c < cols); conj_scale != 0 conjugates and scales.
 cudaError_t launch_transpose(const float2 *in, size_t ldi, float2 *out, size_t ldo, int rows,
                              int cols, float conj_scale, cudaStream_t st);
-cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, cudaStream_t st);
+// work: bicubic_work_bytes(h, pratio) bytes of device scratch (tap table + amplitude image)
+size_t bicubic_work_bytes(int h, int pratio);
+cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, void *work,
+                                cudaStream_t st);
 
 // ---- reductions and ingest ------------------------------------------------
 cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cudaStream_t st);

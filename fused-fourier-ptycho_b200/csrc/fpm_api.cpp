@@ -779,7 +779,8 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
         if ((const void *)p->object_init != (const void *)O)
             FPM_CK(cudaMemcpyAsync(O, p->object_init, s.big * 8, kin, st));
     } else {
-        FPM_CK(launch_bicubic_init(in.Y, s.h, s.pratio, O, st));
+        FPM_CK(ctx->T2.ensure(bicubic_work_bytes(s.h, s.pratio)));   // scratch before the loop
+        FPM_CK(launch_bicubic_init(in.Y, s.h, s.pratio, O, ctx->T2.p, st));
     }
     if ((const void *)p->pupil_init != (const void *)P)
         FPM_CK(cudaMemcpyAsync(P, p->pupil_init, s.plane * 8, kin, st));

@@ -109,53 +109,90 @@ __device__ __forceinline__ void cubic_taps(int u0, int p, int n, int idx[4], dou
     for (int k = 0; k < 4; ++k) w[k] /= s;
 }
 
+// The taps and weights depend only on the output index (the same table serves rows
+// and columns of the square image), and the amplitude only on the input pixel, so
+// both are computed once and the per-pixel work is 16 FP64 multiply-adds.
+struct Taps {
+    int4 idx;
+    double w[4];
+};
+
+__global__ void __launch_bounds__(256) k_bicubic_taps(int h, int p, Taps *__restrict__ taps) {
+    const int n_out = h * p;
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n_out; u += gridDim.x * blockDim.x) {
+        int idx[4];
+        double w[4];
+        cubic_taps(u, p, h, idx, w);
+        Taps t;
+        t.idx = make_int4(idx[0], idx[1], idx[2], idx[3]);
+        for (int k = 0; k < 4; ++k) t.w[k] = w[k];
+        taps[u] = t;
+    }
+}
+
 template <int TYPE>
-__global__ void __launch_bounds__(256) k_bicubic_init(StackView Y, int h, int p,
-                                                       float2 *__restrict__ O) {
-    const int H = h * p;
-    const size_t total = (size_t)H * H;
+__global__ void __launch_bounds__(256) k_amplitude_page0(StackView Y, int h, float *__restrict__ amp) {
     float mn = 0.f, range = 0.f;
     if (TYPE == kStackU16) {
         mn = (float)Y.minmax[0];
         range = (float)(Y.minmax[1] - Y.minmax[0]);
     }
+    const int n = h * h;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float a;
+        if (TYPE == kStackF32) {
+            a = static_cast<const float *>(Y.ptr)[i];
+        } else {
+            const float x = (float)static_cast<const uint16_t *>(Y.ptr)[i] - mn;
+            a = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+        }
+        amp[i] = a;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bicubic_init(const float *__restrict__ amp,
+                                                       const Taps *__restrict__ taps, int h, int H,
+                                                       float2 *__restrict__ O) {
+    const size_t total = (size_t)H * H;
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
          q += (size_t)gridDim.x * blockDim.x) {
         const int R = (int)(q % H);
         const int C = (int)(q / H);
-        int ir[4], ic[4];
-        double wr[4], wc[4];
-        cubic_taps(R, p, h, ir, wr);
-        cubic_taps(C, p, h, ic, wc);
+        const Taps tr = taps[R], tc = taps[C];
+        const int ir[4] = {tr.idx.x, tr.idx.y, tr.idx.z, tr.idx.w};
+        const int ic[4] = {tc.idx.x, tc.idx.y, tc.idx.z, tc.idx.w};
         double acc = 0.0;
         for (int kc = 0; kc < 4; ++kc) {
             double t = 0.0;
-            for (int kr = 0; kr < 4; ++kr) {
-                const size_t idx = (size_t)ic[kc] * h + ir[kr];
-                float a;
-                if (TYPE == kStackF32) {
-                    a = static_cast<const float *>(Y.ptr)[idx];
-                } else {
-                    const float x = (float)static_cast<const uint16_t *>(Y.ptr)[idx] - mn;
-                    a = range > 0.f ? sqrtf(x / range) : sqrtf(x);
-                }
-                t += wr[kr] * (double)a;
-            }
-            acc += wc[kc] * t;
+            for (int kr = 0; kr < 4; ++kr)
+                t += tr.w[kr] * (double)amp[(size_t)ic[kc] * h + ir[kr]];
+            acc += tc.w[kc] * t;
         }
         O[q] = make_float2((float)acc, 0.f);
     }
 }
 
-cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, cudaStream_t st) {
-    const size_t total = (size_t)h * pratio * h * pratio;
+size_t bicubic_work_bytes(int h, int pratio) {
+    return (size_t)h * pratio * sizeof(Taps) + (size_t)h * h * sizeof(float) + 256;
+}
+
+cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, void *work,
+                                cudaStream_t st) {
+    const int H = h * pratio;
+    Taps *taps = static_cast<Taps *>(work);
+    float *amp = reinterpret_cast<float *>(
+        (reinterpret_cast<uintptr_t>(taps + H) + 255) & ~static_cast<uintptr_t>(255));
+    k_bicubic_taps<<<(H + 255) / 256, 256, 0, st>>>(h, pratio, taps);
+    const int ga = (h * h + 255) / 256 < kB200SMs * 8 ? (h * h + 255) / 256 : kB200SMs * 8;
+    if (Y.type == kStackU16)
+        k_amplitude_page0<kStackU16><<<ga, 256, 0, st>>>(Y, h, amp);
+    else
+        k_amplitude_page0<kStackF32><<<ga, 256, 0, st>>>(Y, h, amp);
+    const size_t total = (size_t)H * H;
     size_t gx = (total + 255) / 256;
     const size_t cap = (size_t)kB200SMs * 8 * 8;
     if (gx > cap) gx = cap;
-    if (Y.type == kStackU16)
-        k_bicubic_init<kStackU16><<<(unsigned)gx, 256, 0, st>>>(Y, h, pratio, O);
-    else
-        k_bicubic_init<kStackF32><<<(unsigned)gx, 256, 0, st>>>(Y, h, pratio, O);
+    k_bicubic_init<<<(unsigned)gx, 256, 0, st>>>(amp, taps, h, H, O);
     return cudaGetLastError();
 }
 
@@ -186,7 +223,21 @@ cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cud
 __global__ void __launch_bounds__(256) k_stack_minmax(const uint16_t *__restrict__ p, size_t n,
                                                        unsigned *__restrict__ mm) {
     unsigned lo = 0xffffu, hi = 0u;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+    // eight values per 16-byte load over the aligned bulk, then the tail
+    const size_t n8 = (reinterpret_cast<uintptr_t>(p) & 15u) ? 0 : n / 8;
+    const uint4 *p8 = reinterpret_cast<const uint4 *>(p);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n8;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const uint4 v = p8[i];
+        const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const unsigned a = w[k] & 0xffffu, b = w[k] >> 16;
+            lo = min(lo, min(a, b));
+            hi = max(hi, max(a, b));
+        }
+    }
+    for (size_t i = n8 * 8 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
         const unsigned v = p[i];
         lo = v < lo ? v : lo;
@@ -209,7 +260,7 @@ cudaError_t launch_stack_minmax(const uint16_t *p, size_t n, unsigned *mm, cudaS
     const unsigned init[2] = {0xffffu, 0u};
     cudaError_t e = cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
-    size_t gx = (n + 255) / 256;
+    size_t gx = (n / 8 + 255) / 256;
     if (gx > (size_t)kB200SMs * 16) gx = (size_t)kB200SMs * 16;
     if (gx == 0) gx = 1;
     k_stack_minmax<<<(unsigned)gx, 256, 0, st>>>(p, n, mm);
