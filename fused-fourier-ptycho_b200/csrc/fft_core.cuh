@@ -26,6 +26,19 @@ namespace fft {
 
 __device__ __forceinline__ int swz(int l) { return l ^ ((l >> 4) & 15); }
 
+// Exchange addresses for E values per thread: E = 16 uses swz above; E = 32 (radix-32
+// stages, whose first-stage stores stride 32 values) uses l ^ ((l >> 5) & 15), which
+// keeps every store and load of the 16384-point plan 32 x 16 x ... on distinct bank
+// pairs.
+template <int E>
+__device__ __forceinline__ int swz_e(int l) {
+    if constexpr (E == 32) {
+        return l ^ ((l >> 5) & 15);
+    } else {
+        return swz(l);
+    }
+}
+
 // Complex arithmetic on packed float pairs: one sm_100 two-lane instruction
 // (FADD2 / FMUL2 / FFMA2) per complex add and two per complex product, half the
 // scalar count.  Each lane is an ordinary IEEE round-to-nearest operation.
@@ -58,6 +71,27 @@ __device__ __forceinline__ float2 w16(int k) {
     return make_float2(c, DIR < 0 ? -s : s);
 }
 
+// cos / sin of 2 pi k / 32, k = 0..8
+__host__ __device__ constexpr float c32(int k) {
+    return k == 0 ? 1.0f
+         : k == 1 ? 0.98078528040323043f
+         : k == 2 ? 0.92387953251128674f
+         : k == 3 ? 0.83146961230254524f
+         : k == 4 ? 0.70710678118654757f
+         : k == 5 ? 0.55557023301960218f
+         : k == 6 ? 0.38268343236508978f
+         : k == 7 ? 0.19509032201612825f
+                  : 0.0f;
+}
+
+// W_32^k = exp(DIR 2 pi i k / 32) for k in [0, 16)
+template <int DIR>
+__device__ __forceinline__ float2 w32(int k) {
+    const float c = k <= 8 ? c32(k) : -c32(16 - k);
+    const float s = k <= 8 ? c32(8 - k) : c32(k - 8);
+    return make_float2(c, DIR < 0 ? -s : s);
+}
+
 // multiply by W_16^k (k compile-time), special-casing the trivial factors
 template <int DIR, int K>
 __device__ __forceinline__ float2 mul_w16(float2 v) {
@@ -85,6 +119,27 @@ template <int R, int DIR>
 __device__ __forceinline__ void dft(float2 (&v)[R]) {
     if constexpr (R == 1) {
         return;
+    } else if constexpr (R == 32) {
+        // the 16-point networks of the even and odd halves, then the last level with W_32^j
+        float2 e[16], o[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            e[i] = v[2 * i];
+            o[i] = v[2 * i + 1];
+        }
+        dft<16, DIR>(e);
+        dft<16, DIR>(o);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            float2 t = o[j];
+            if (j == 8) {
+                t = mul_w16<DIR, 4>(t);
+            } else if (j != 0) {
+                t = cmulf(w32<DIR>(j), t);
+            }
+            v[j] = cadd(e[j], t);
+            v[j + 16] = csub(e[j], t);
+        }
     } else {
         constexpr int B = ilog2(R);
         float2 a[R];
@@ -131,30 +186,40 @@ __device__ __forceinline__ float2 twiddle(const float2 *hi, const float2 *lo, in
 template <int R, int DIR>
 __device__ __forceinline__ void apply_twiddles(float2 (&u)[R], const float2 *hi, const float2 *lo,
                                                int m1) {
+    // radix 32: u[16 + q] takes W^((16 + q) m1) = W^(q m1) W^(16 m1), next to u[q]
+    float2 w16 = make_float2(1.f, 0.f);
+    if constexpr (R >= 32) {
+        w16 = twiddle<DIR>(hi, lo, 16 * m1);
+        u[16] = cmulf(w16, u[16]);
+    }
+    auto put = [&](int q, float2 wq) {
+        u[q] = cmulf(wq, u[q]);
+        if constexpr (R >= 32) u[16 + q] = cmulf(cmulf(wq, w16), u[16 + q]);
+    };
     const float2 w1 = twiddle<DIR>(hi, lo, m1);
-    u[1] = cmulf(w1, u[1]);
+    put(1, w1);
     if constexpr (R >= 4) {
         const float2 w2 = twiddle<DIR>(hi, lo, 2 * m1);
-        u[2] = cmulf(w2, u[2]);
+        put(2, w2);
         const float2 w3 = cmulf(w1, w2);
-        u[3] = cmulf(w3, u[3]);
+        put(3, w3);
         if constexpr (R >= 8) {
             const float2 w4 = twiddle<DIR>(hi, lo, 4 * m1);
-            u[4] = cmulf(w4, u[4]);
-            u[5] = cmulf(cmulf(w1, w4), u[5]);
-            u[6] = cmulf(cmulf(w2, w4), u[6]);
-            u[7] = cmulf(cmulf(w3, w4), u[7]);
+            put(4, w4);
+            put(5, cmulf(w1, w4));
+            put(6, cmulf(w2, w4));
+            put(7, cmulf(w3, w4));
             if constexpr (R >= 16) {
                 const float2 w8 = twiddle<DIR>(hi, lo, 8 * m1);
-                u[8] = cmulf(w8, u[8]);
-                u[9] = cmulf(cmulf(w1, w8), u[9]);
-                u[10] = cmulf(cmulf(w2, w8), u[10]);
-                u[11] = cmulf(cmulf(w3, w8), u[11]);
+                put(8, w8);
+                put(9, cmulf(w1, w8));
+                put(10, cmulf(w2, w8));
+                put(11, cmulf(w3, w8));
                 const float2 w12 = cmulf(w4, w8);
-                u[12] = cmulf(w12, u[12]);
-                u[13] = cmulf(cmulf(w1, w12), u[13]);
-                u[14] = cmulf(cmulf(w2, w12), u[14]);
-                u[15] = cmulf(cmulf(w3, w12), u[15]);
+                put(12, w12);
+                put(13, cmulf(w1, w12));
+                put(14, cmulf(w2, w12));
+                put(15, cmulf(w3, w12));
             }
         }
     }
@@ -171,20 +236,20 @@ __device__ __forceinline__ void apply_twiddles(float2 (&u)[R], const float2 *hi,
 // from global memory (16 independent loads per thread) and store it back, or
 // hand it to the next computation without a shared-memory round trip.
 // ---------------------------------------------------------------------------
-template <int N, int DIR, int P>
-__device__ __forceinline__ void stages_regs(float2 (&v)[16], float2 *s, const float2 *hi,
+template <int N, int DIR, int P, int E>
+__device__ __forceinline__ void stages_regs(float2 (&v)[E], float2 *s, const float2 *hi,
                                             const float2 *lo, int t) {
     constexpr int REM = N / P;
-    constexpr int R = REM >= 16 ? 16 : REM;
-    constexpr int T = N / 16;
-    constexpr int NB = 16 / R;
+    constexpr int R = REM >= E ? E : REM;
+    constexpr int T = N / E;
+    constexpr int NB = E / R;
     constexpr bool FIRST = P == 1;
     constexpr bool LAST = P * R == N;
     if constexpr (!FIRST) {
 #pragma unroll
         for (int j = 0; j < NB; ++j)
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[j + r * NB] = s[swz(t + j * T + r * (N / R))];
+            for (int r = 0; r < R; ++r) v[j + r * NB] = s[swz_e<E>(t + j * T + r * (N / R))];
     }
     if constexpr (!LAST) __syncthreads();   // every read of s done before it is rewritten
 #pragma unroll
@@ -202,12 +267,12 @@ __device__ __forceinline__ void stages_regs(float2 (&v)[16], float2 *s, const fl
         } else {
             const int base = (i - k) * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) s[swz(base + r * P)] = u[r];
+            for (int r = 0; r < R; ++r) s[swz_e<E>(base + r * P)] = u[r];
         }
     }
     if constexpr (!LAST) {
         __syncthreads();
-        stages_regs<N, DIR, P * R>(v, s, hi, lo, t);
+        stages_regs<N, DIR, P * R, E>(v, s, hi, lo, t);
     }
 }
 
@@ -218,7 +283,16 @@ template <int N, int DIR>
 __device__ __forceinline__ void line_fft_regs(float2 (&v)[16], float2 *s, const float2 *hi,
                                               const float2 *lo, int t) {
     static_assert(N >= 16 && (N & (N - 1)) == 0, "power-of-two length >= 16");
-    stages_regs<N, DIR, 1>(v, s, hi, lo, t);
+    stages_regs<N, DIR, 1, 16>(v, s, hi, lo, t);
+}
+
+// The same with 32 values per thread (t + m N/32, m < 32): radix-32 stages, one
+// exchange fewer for N = 16384 (32 x 32 x 16) at N/32 threads per line.
+template <int N, int DIR>
+__device__ __forceinline__ void line_fft_regs32(float2 (&v)[32], float2 *s, const float2 *hi,
+                                                const float2 *lo, int t) {
+    static_assert(N >= 1024 && (N & (N - 1)) == 0, "power-of-two length >= 1024");
+    stages_regs<N, DIR, 1, 32>(v, s, hi, lo, t);
 }
 
 // Copies the two-level twiddle table of length N into shared memory.
@@ -232,12 +306,14 @@ __device__ __forceinline__ void load_twiddles(float2 *s_hi, float2 *s_lo, const 
 // CTA shape for the register-resident kernels: LPC lines of length N per CTA,
 // T = N/16 threads per line, lines padded in shared memory by PAD values so that
 // the LPC lines of an interleaved warp fall on different banks.
-template <int N>
+template <int N, int E = 16>
 struct LG {
-    static constexpr int T = N / 16;
+    static constexpr int T = N / E;
     static constexpr int LPC = (N * 8 >= 64 * 1024) ? 1 : (64 * 1024) / (N * 8);
     static constexpr int THREADS = T * LPC;
-    static constexpr int MINB = THREADS <= 512 ? 2 : 1;      // 64 registers per thread
+    // 16 values per thread: 64 registers, two CTAs per SM when they fit; 32 values:
+    // up to 128 registers, one CTA
+    static constexpr int MINB = (E == 16 && THREADS <= 512) ? 2 : 1;
     static constexpr int PAD = LPC == 1 ? 0 : (16 / LPC > 0 ? 16 / LPC : 1);
     static constexpr int STRIDE = N + PAD;
     static constexpr int SMEM = LPC * STRIDE * 8 + 2 * 128 * 8;

@@ -1,5 +1,6 @@
 // 2-D FFT passes built on the shared-memory line FFT of fft_core.cuh.
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "fft.h"
@@ -9,8 +10,18 @@ namespace fpm {
 
 namespace {
 
-template <int N>
-using LG = fft::LG<N>;
+template <int N, int E = 16>
+using LG = fft::LG<N, E>;
+
+template <int N, int DIR, int E>
+__device__ __forceinline__ void line_fft_e(float2 (&v)[E], float2 *s, const float2 *hi,
+                                           const float2 *lo, int t) {
+    if constexpr (E == 32) {
+        fft::line_fft_regs32<N, DIR>(v, s, hi, lo, t);
+    } else {
+        fft::line_fft_regs<N, DIR>(v, s, hi, lo, t);
+    }
+}
 
 template <class K>
 cudaError_t set_smem(K kernel, int bytes) {
@@ -21,11 +32,11 @@ cudaError_t set_smem(K kernel, int bytes) {
 }
 
 // Lines along the contiguous axis: line L (over all pages) = elements [L*N, (L+1)*N).
-template <int N, int DIR>
-__global__ void __launch_bounds__(LG<N>::THREADS, LG<N>::MINB)
+template <int N, int DIR, int E>
+__global__ void __launch_bounds__(LG<N, E>::THREADS, LG<N, E>::MINB)
     k_fft_contig(const float2 *__restrict__ in, float2 *__restrict__ out, long long n_lines,
                  const float2 *__restrict__ g_hi, const float2 *__restrict__ g_lo) {
-    using G = LG<N>;
+    using G = LG<N, E>;
     extern __shared__ float2 smem[];
     float2 *s_hi = G::tw_hi(smem);
     fft::load_twiddles(s_hi, s_hi + 128, g_hi, g_lo, G::NHI, G::NLO);
@@ -34,25 +45,25 @@ __global__ void __launch_bounds__(LG<N>::THREADS, LG<N>::MINB)
     const long long L = (long long)blockIdx.x * G::LPC + ln;
     const bool live = L < n_lines;
     const float2 *src = in + (size_t)(live ? L : 0) * N;
-    float2 v[16];
+    float2 v[E];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) v[m] = live ? src[t + m * G::T] : make_float2(0.f, 0.f);
-    fft::line_fft_regs<N, DIR>(v, smem + ln * G::STRIDE, s_hi, s_hi + 128, t);
+    for (int m = 0; m < E; ++m) v[m] = live ? src[t + m * G::T] : make_float2(0.f, 0.f);
+    line_fft_e<N, DIR, E>(v, smem + ln * G::STRIDE, s_hi, s_hi + 128, t);
     if (live) {
         float2 *dst = out + (size_t)L * N;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) dst[t + m * G::T] = v[m];
+        for (int m = 0; m < E; ++m) dst[t + m * G::T] = v[m];
     }
 }
 
 // Lines along the strided axis: line (p, r) = elements p*N*N + c*N + r, c = 0..N-1,
 // numbered g = p*N + r; a CTA takes LPC consecutive g with its warps interleaved
 // over them, so each c contributes LPC*8 contiguous bytes.
-template <int N, int DIR>
-__global__ void __launch_bounds__(LG<N>::THREADS, LG<N>::MINB)
+template <int N, int DIR, int E>
+__global__ void __launch_bounds__(LG<N, E>::THREADS, LG<N, E>::MINB)
     k_fft_strided(const float2 *__restrict__ in, float2 *__restrict__ out, long long n_lines,
                   const float2 *__restrict__ g_hi, const float2 *__restrict__ g_lo) {
-    using G = LG<N>;
+    using G = LG<N, E>;
     extern __shared__ float2 smem[];
     float2 *s_hi = G::tw_hi(smem);
     fft::load_twiddles(s_hi, s_hi + 128, g_hi, g_lo, G::NHI, G::NLO);
@@ -61,40 +72,52 @@ __global__ void __launch_bounds__(LG<N>::THREADS, LG<N>::MINB)
     const long long g = (long long)blockIdx.x * G::LPC + ln;
     const bool live = g < n_lines;
     const size_t base = live ? (size_t)(g / N) * N * N + (size_t)(g % N) : 0;
-    float2 v[16];
+    float2 v[E];
 #pragma unroll
-    for (int m = 0; m < 16; ++m)
+    for (int m = 0; m < E; ++m)
         v[m] = live ? in[base + (size_t)(t + m * G::T) * N] : make_float2(0.f, 0.f);
-    fft::line_fft_regs<N, DIR>(v, smem + ln * G::STRIDE, s_hi, s_hi + 128, t);
+    line_fft_e<N, DIR, E>(v, smem + ln * G::STRIDE, s_hi, s_hi + 128, t);
     if (live) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) out[base + (size_t)(t + m * G::T) * N] = v[m];
+        for (int m = 0; m < E; ++m) out[base + (size_t)(t + m * G::T) * N] = v[m];
     }
 }
 
 // axes: bit 0 = the contiguous pass, bit 1 = the strided pass (run in that order; the
 // strided pass reads the contiguous pass's output when both run)
-template <int N, int DIR>
-cudaError_t run_n(const float2 *in, float2 *out, int count, int axes, const float2 *hi,
-                  const float2 *lo, cudaStream_t st) {
-    using G = LG<N>;
-    cudaError_t e = set_smem(k_fft_contig<N, DIR>, G::SMEM);
+template <int N, int DIR, int E>
+cudaError_t run_ne(const float2 *in, float2 *out, int count, int axes, const float2 *hi,
+                   const float2 *lo, cudaStream_t st) {
+    using G = LG<N, E>;
+    cudaError_t e = set_smem(k_fft_contig<N, DIR, E>, G::SMEM);
     if (e != cudaSuccess) return e;
-    e = set_smem(k_fft_strided<N, DIR>, G::SMEM);
+    e = set_smem(k_fft_strided<N, DIR, E>, G::SMEM);
     if (e != cudaSuccess) return e;
     const long long lines = (long long)count * N;
     const long long blocks = (lines + G::LPC - 1) / G::LPC;
     if (axes & 1) {
-        k_fft_contig<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(in, out, lines, hi, lo);
+        k_fft_contig<N, DIR, E><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(in, out, lines, hi, lo);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     if (axes & 2) {
-        k_fft_strided<N, DIR><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(
+        k_fft_strided<N, DIR, E><<<(unsigned)blocks, G::THREADS, G::SMEM, st>>>(
             (axes & 1) ? out : in, out, lines, hi, lo);
         e = cudaGetLastError();
     }
     return e;
+}
+
+// 16384-point lines run with 32 values per thread (FPM_COLS_E16=1 keeps 16, for
+// measurements); shorter lines with 16
+template <int N, int DIR>
+cudaError_t run_n(const float2 *in, float2 *out, int count, int axes, const float2 *hi,
+                  const float2 *lo, cudaStream_t st) {
+    if constexpr (N == 16384) {
+        const char *env = std::getenv("FPM_COLS_E16");
+        if (!(env && std::atoi(env) != 0)) return run_ne<N, DIR, 32>(in, out, count, axes, hi, lo, st);
+    }
+    return run_ne<N, DIR, 16>(in, out, count, axes, hi, lo, st);
 }
 
 template <int DIR>

@@ -31,6 +31,7 @@
 #include "tma.cuh"
 
 #include <cudaTypedefs.h>
+#include <cstdlib>
 
 namespace fpm {
 
@@ -101,9 +102,9 @@ __device__ __forceinline__ float amplitude(const StackView &Y, size_t idx, float
 }
 
 // Shared set-up of every pass kernel: twiddles into shared memory.
-template <int N>
+template <int N, int E = 16>
 __device__ __forceinline__ void setup(float2 *smem, const float2 *thi, const float2 *tlo) {
-    using G = fft::LG<N>;
+    using G = fft::LG<N, E>;
     float2 *s_hi = G::tw_hi(smem);
     fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, G::NHI, G::NLO);
     __syncthreads();
@@ -603,35 +604,46 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 // FFT of the updated column; the IFFT's last stage hands its registers to the
 // RMSprop and the FFT's first stage without a shared-memory round trip.
 // ---------------------------------------------------------------------------
-template <int N, int MODE>
-__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
+// E values per thread: 16, or 32 for N = 16384 (radix-32 stages, one exchange fewer)
+template <int N, int DIR, int E>
+__device__ __forceinline__ void line_fft_e(float2 (&v)[E], float2 *s, const float2 *hi,
+                                           const float2 *lo, int t) {
+    if constexpr (E == 32) {
+        fft::line_fft_regs32<N, DIR>(v, s, hi, lo, t);
+    } else {
+        fft::line_fft_regs<N, DIR>(v, s, hi, lo, t);
+    }
+}
+
+template <int N, int MODE, int E>
+__global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     k_big_cols(ColsArgs a, const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
-    using G = fft::LG<N>;
+    using G = fft::LG<N, E>;
     extern __shared__ float2 smem[];
-    setup<N>(smem, thi, tlo);
+    setup<N, E>(smem, thi, tlo);
     const int ln = G::cline(), t = G::ct();
     const int c = blockIdx.x * G::LPC + ln;    // column; c >= N only when N < LPC
     const bool live = c < N;
     float2 *line = smem + ln * G::STRIDE;
     const float2 *s_hi = G::tw_hi(smem);
     const size_t col = (size_t)(live ? c : 0) * N;
-    float2 v[16];
+    float2 v[E];
     if (MODE == kColsForward) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) v[m] = live ? a.O[col + t + m * G::T] : make_float2(0.f, 0.f);
+        for (int m = 0; m < E; ++m) v[m] = live ? a.O[col + t + m * G::T] : make_float2(0.f, 0.f);
     } else {
         const float2 *u = a.U + (size_t)(live ? c : 0) * a.ldU;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
+        for (int m = 0; m < E; ++m) {
             int i = t + m * G::T - a.Ru0;          // box row of element e
             if (i < 0) i += N;
             v[m] = (live && i < a.rspan) ? u[i] : make_float2(0.f, 0.f);
         }
-        fft::line_fft_regs<N, +1>(v, line, s_hi, s_hi + 128, t);
+        line_fft_e<N, +1, E>(v, line, s_hi, s_hi + 128, t);
         if (MODE == kColsGradient) {
             if (live) {
 #pragma unroll
-                for (int m = 0; m < 16; ++m) a.gout[col + t + m * G::T] = v[m];
+                for (int m = 0; m < E; ++m) a.gout[col + t + m * G::T] = v[m];
             }
             return;
         }
@@ -639,7 +651,7 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
         const float omb = 1.0f - a.beta;
         if (live) {
 #pragma unroll
-            for (int m0 = 0; m0 < 16; m0 += 4) {
+            for (int m0 = 0; m0 < E; m0 += 4) {
                 float2 w[4];
                 float mv[4];
 #pragma unroll
@@ -663,11 +675,11 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
         }
         if (a.rspan_n == 0) return;   // uniform over the grid: no next batch
     }
-    fft::line_fft_regs<N, -1>(v, line, s_hi, s_hi + 128, t);
+    line_fft_e<N, -1, E>(v, line, s_hi, s_hi + 128, t);
     if (live) {
         float2 *vv = a.V + (size_t)c * a.ldV;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
+        for (int m = 0; m < E; ++m) {
             int i = t + m * G::T - a.Ru0n;
             if (i < 0) i += N;
             if (i < a.rspan_n) vv[i] = v[m];
@@ -945,31 +957,40 @@ cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float
     return cudaGetLastError();
 }
 
+template <int N, int MODE, int E>
+static cudaError_t launch_cols_k(const ColsArgs &a, const Twiddles &tw, cudaStream_t st) {
+    using G = fft::LG<N, E>;
+    const int blocks = (N + G::LPC - 1) / G::LPC;
+    cudaError_t e = set_smem(k_big_cols<N, MODE, E>, G::SMEM);
+    if (e != cudaSuccess) return e;
+    k_big_cols<N, MODE, E><<<blocks, G::THREADS, G::SMEM, st>>>(a, tw.hi_hi, tw.hi_lo);
+    return cudaGetLastError();
+}
+
+template <int N, int E>
+static cudaError_t launch_cols_e(const ColsArgs &a, const Twiddles &tw, cudaStream_t st) {
+    if (a.mode == kColsForward) return launch_cols_k<N, kColsForward, E>(a, tw, st);
+    if (a.mode == kColsUpdate) return launch_cols_k<N, kColsUpdate, E>(a, tw, st);
+    return launch_cols_k<N, kColsGradient, E>(a, tw, st);
+}
+
+// 16384-point columns run with 32 values per thread; FPM_COLS_E16=1 keeps 16
+// (measurements).
+static bool cols_e16() {
+    const char *e = std::getenv("FPM_COLS_E16");
+    return e && std::atoi(e) != 0;
+}
+
 cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                                  \
-    {                                                                                         \
-        const int blocks = (N + fft::LG<N>::LPC - 1) / fft::LG<N>::LPC;                               \
-        if (a.mode == kColsForward) {                                                         \
-            e = set_smem(k_big_cols<N, kColsForward>, smem_bytes<N>());                       \
-            if (e != cudaSuccess) return e;                                                   \
-            k_big_cols<N, kColsForward><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(    \
-                a, tw.hi_hi, tw.hi_lo);                                                       \
-        } else if (a.mode == kColsUpdate) {                                                   \
-            e = set_smem(k_big_cols<N, kColsUpdate>, smem_bytes<N>());                        \
-            if (e != cudaSuccess) return e;                                                   \
-            k_big_cols<N, kColsUpdate><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(     \
-                a, tw.hi_hi, tw.hi_lo);                                                       \
-        } else {                                                                              \
-            e = set_smem(k_big_cols<N, kColsGradient>, smem_bytes<N>());                      \
-            if (e != cudaSuccess) return e;                                                   \
-            k_big_cols<N, kColsGradient><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(   \
-                a, tw.hi_hi, tw.hi_lo);                                                       \
-        }                                                                                     \
-    }
+    if (N == 16384 && !cols_e16())                                                            \
+        e = launch_cols_e<N, (N == 16384 ? 32 : 16)>(a, tw, st);                             \
+    else                                                                                      \
+        e = launch_cols_e<N, 16>(a, tw, st);
     FPM_DISPATCH_BIG(a.H, F)
 #undef F
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, int cspan_n,

@@ -486,3 +486,37 @@ def test_isotropic_loss_gradients_and_solve(engine, ds_small, ds_a):
         assert orc.rel_err(r["object"], o.object) < TIGHT      # the FP32 twin: 2.6e-7
         assert orc.rel_err(r["pupil"], o.pupil) < TIGHT
         np.testing.assert_allclose(r["loss"], o.loss, rtol=1e-6)
+
+
+def test_16384_columns_32_values_per_thread_match_16(engine):
+    """The 16384-point column pass runs radix-32 stages with 32 values per thread; the
+    16-value variant (FPM_COLS_E16=1) is the same transform with other roundings.  A short
+    solve at 2048^2 -> 16384^2 and a gradient call must agree to FP32 rounding."""
+    import os
+    import torch
+    from fpm_b200 import synth
+    h, p = 2048, 8
+    H = h * p
+    optics = synth.Optics(led_grid=3)
+    circ = synth.pupil_circle(h, optics)
+    led = led_matlab(synth.led_indices(h, p, optics)[:3])
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    Y = (torch.rand((3, h, h), generator=g, device="cuda") * 0.5 + 0.25).permute(1, 2, 0)
+    O0 = torch.polar(torch.ones((H, H), device="cuda"),
+                     0.1 * torch.randn((H, H), generator=g, device="cuda")).contiguous()
+    P0c = torch.from_numpy(circ.astype(np.complex64)).cuda()
+    P0 = torch.from_numpy(circ).cuda()
+    ledt = torch.from_numpy(led).cuda()
+    runs = {}
+    for flag in ("0", "1"):
+        os.environ["FPM_COLS_E16"] = flag
+        try:
+            r = engine.solve(O0, P0c, Y, ledt, P0, p, 1, 3, lr=1e-3, spectrum=False)
+            d = engine.batch_gradients(O0, P0c, Y, ledt, P0, p)
+            runs[flag] = (r["object"].cpu().numpy(), r["pupil"].cpu().numpy(),
+                          d[0].cpu().numpy(), d[1].cpu().numpy())
+        finally:
+            del os.environ["FPM_COLS_E16"]
+    for a, b in zip(runs["0"], runs["1"]):
+        assert orc.rel_err(a, b) < 1e-5, orc.rel_err(a, b)
