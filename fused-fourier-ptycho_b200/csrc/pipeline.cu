@@ -110,6 +110,17 @@ __device__ __forceinline__ void setup(float2 *smem, const float2 *thi, const flo
     __syncthreads();
 }
 
+// E values per thread: 16, or 32 for N = 16384 (radix-32 stages, one exchange fewer)
+template <int N, int DIR, int E>
+__device__ __forceinline__ void line_fft_e(float2 (&v)[E], float2 *s, const float2 *hi,
+                                           const float2 *lo, int t) {
+    if constexpr (E == 32) {
+        fft::line_fft_regs32<N, DIR>(v, s, hi, lo, t);
+    } else {
+        fft::line_fft_regs<N, DIR>(v, s, hi, lo, t);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // L1: crop x pupil, ifftshift, inverse FFT along r (contiguous column lines)
 // ---------------------------------------------------------------------------
@@ -536,24 +547,24 @@ __global__ void __launch_bounds__(256) k_lr_pupil_grad(const float2 *__restrict_
 // ---------------------------------------------------------------------------
 // Pass A: stitch the box rows of the gradient spectrum, inverse FFT along the row
 // ---------------------------------------------------------------------------
-template <int N>
-__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
+template <int N, int E>
+__global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     k_big_rows_inv(BatchGeom g, const int2 *__restrict__ led, const float2 *__restrict__ Pt,
                    const float2 *__restrict__ Xs, float2 *__restrict__ Ur,
                    const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
-    using G = fft::LG<N>;
+    using G = fft::LG<N, E>;
     extern __shared__ float2 smem[];
     int2 *s_ab = reinterpret_cast<int2 *>(G::tw_hi(smem) + 256);
     for (int l = threadIdx.x; l < g.nb; l += G::THREADS) s_ab[l] = led_box_offset(led, l, g);
-    setup<N>(smem, thi, tlo);
+    setup<N, E>(smem, thi, tlo);
     const int ln = G::cline(), t = G::ct();
     const int i = blockIdx.x * G::LPC + ln;     // box row of this line
     const bool live = i < g.rspan;
     const int h = g.h;
-    float2 v[16];
+    float2 v[E];
     // four elements per LED sweep: four independent gathers in flight per thread
 #pragma unroll
-    for (int m0 = 0; m0 < 16; m0 += 4) {
+    for (int m0 = 0; m0 < E; m0 += 4) {
         int jj[4];
         bool any = false;
 #pragma unroll
@@ -591,11 +602,11 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 #pragma unroll
         for (int k = 0; k < 4; ++k) v[m0 + k] = acc[k].s;
     }
-    fft::line_fft_regs<N, +1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    line_fft_e<N, +1, E>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
     if (live) {
         float2 *row = Ur + (size_t)i * N;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) row[t + m * G::T] = v[m];
+        for (int m = 0; m < E; ++m) row[t + m * G::T] = v[m];
     }
 }
 
@@ -604,17 +615,6 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 // FFT of the updated column; the IFFT's last stage hands its registers to the
 // RMSprop and the FFT's first stage without a shared-memory round trip.
 // ---------------------------------------------------------------------------
-// E values per thread: 16, or 32 for N = 16384 (radix-32 stages, one exchange fewer)
-template <int N, int DIR, int E>
-__device__ __forceinline__ void line_fft_e(float2 (&v)[E], float2 *s, const float2 *hi,
-                                           const float2 *lo, int t) {
-    if constexpr (E == 32) {
-        fft::line_fft_regs32<N, DIR>(v, s, hi, lo, t);
-    } else {
-        fft::line_fft_regs<N, DIR>(v, s, hi, lo, t);
-    }
-}
-
 template <int N, int MODE, int E>
 __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     k_big_cols(ColsArgs a, const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
@@ -690,25 +690,25 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
 // ---------------------------------------------------------------------------
 // Pass C: rows of V (strided) -> FFT along the row -> the next batch's Sbox
 // ---------------------------------------------------------------------------
-template <int N>
-__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
+template <int N, int E>
+__global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     k_big_rows_fwd(const float2 *__restrict__ Vr, int rspan_n, int Cu0n, int cspan_n,
                    float2 *__restrict__ Sboxr, const float2 *__restrict__ thi,
                    const float2 *__restrict__ tlo) {
-    using G = fft::LG<N>;
+    using G = fft::LG<N, E>;
     extern __shared__ float2 smem[];
-    setup<N>(smem, thi, tlo);
+    setup<N, E>(smem, thi, tlo);
     const int ln = G::cline(), t = G::ct();
     const int i = blockIdx.x * G::LPC + ln;
     const bool live = i < rspan_n;
     const float2 *row = Vr + (size_t)(live ? i : 0) * N;
-    float2 v[16];
+    float2 v[E];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) v[m] = live ? row[t + m * G::T] : make_float2(0.f, 0.f);
-    fft::line_fft_regs<N, -1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+    for (int m = 0; m < E; ++m) v[m] = live ? row[t + m * G::T] : make_float2(0.f, 0.f);
+    line_fft_e<N, -1, E>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
     if (live) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
+        for (int m = 0; m < E; ++m) {
             int j = t + m * G::T - Cu0n;
             if (j < 0) j += N;
             if (j < cspan_n) Sboxr[(size_t)i * cspan_n + j] = v[m];
@@ -939,22 +939,33 @@ cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs 
     return cudaGetLastError();
 }
 
+template <int N, int E>
+static cudaError_t launch_rows_inv_e(const BatchGeom &g, const int2 *led, const float2 *Pt,
+                                     const float2 *Xs, float2 *Ur, const Twiddles &tw,
+                                     cudaStream_t st) {
+    using G = fft::LG<N, E>;
+    const int smem = G::SMEM + g.nb * (int)sizeof(int2);
+    const int blocks = (g.rspan + G::LPC - 1) / G::LPC;
+    cudaError_t e = set_smem(k_big_rows_inv<N, E>, smem);
+    if (e != cudaSuccess) return e;
+    k_big_rows_inv<N, E><<<blocks, G::THREADS, smem, st>>>(g, led, Pt, Xs, Ur, tw.hi_hi, tw.hi_lo);
+    return cudaGetLastError();
+}
+
+static bool cols_e16();
+
 cudaError_t launch_big_rows_inv(const BatchGeom &g, const int2 *led, const float2 *Pt,
                                 const float2 *Xs, float2 *Ur, const Twiddles &tw,
                                 cudaStream_t st) {
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                                  \
-    {                                                                                         \
-        const int smem = smem_bytes<N>() + g.nb * (int)sizeof(int2);                          \
-        const int blocks = (g.rspan + fft::LG<N>::LPC - 1) / fft::LG<N>::LPC;                          \
-        e = set_smem(k_big_rows_inv<N>, smem);                                                \
-        if (e != cudaSuccess) return e;                                                       \
-        k_big_rows_inv<N><<<blocks, fft::LG<N>::THREADS, smem, st>>>(                           \
-            g, led, Pt, Xs, Ur, tw.hi_hi, tw.hi_lo);                                                                        \
-    }
+    if (N == 16384 && !cols_e16())                                                            \
+        e = launch_rows_inv_e<N, (N == 16384 ? 32 : 16)>(g, led, Pt, Xs, Ur, tw, st);       \
+    else                                                                                      \
+        e = launch_rows_inv_e<N, 16>(g, led, Pt, Xs, Ur, tw, st);
     FPM_DISPATCH_BIG(g.H, F)
 #undef F
-    return cudaGetLastError();
+    return e;
 }
 
 template <int N, int MODE, int E>
@@ -974,8 +985,8 @@ static cudaError_t launch_cols_e(const ColsArgs &a, const Twiddles &tw, cudaStre
     return launch_cols_k<N, kColsGradient, E>(a, tw, st);
 }
 
-// 16384-point columns run with 32 values per thread; FPM_COLS_E16=1 keeps 16
-// (measurements).
+// 16384-point lines (passes A, B, C) run with 32 values per thread; FPM_COLS_E16=1
+// keeps 16 (measurements).
 static bool cols_e16() {
     const char *e = std::getenv("FPM_COLS_E16");
     return e && std::atoi(e) != 0;
@@ -993,20 +1004,29 @@ cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t 
     return e;
 }
 
+template <int N, int E>
+static cudaError_t launch_rows_fwd_e(int rspan_n, int Cu0n, int cspan_n, const float2 *Vr,
+                                     float2 *Sboxr, const Twiddles &tw, cudaStream_t st) {
+    using G = fft::LG<N, E>;
+    const int blocks = (rspan_n + G::LPC - 1) / G::LPC;
+    cudaError_t e = set_smem(k_big_rows_fwd<N, E>, G::SMEM);
+    if (e != cudaSuccess) return e;
+    k_big_rows_fwd<N, E><<<blocks, G::THREADS, G::SMEM, st>>>(Vr, rspan_n, Cu0n, cspan_n, Sboxr,
+                                                             tw.hi_hi, tw.hi_lo);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, int cspan_n,
                                 float2 *Sboxr, const Twiddles &tw, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                                  \
-    {                                                                                         \
-        const int blocks = (rspan_n + fft::LG<N>::LPC - 1) / fft::LG<N>::LPC;                          \
-        e = set_smem(k_big_rows_fwd<N>, smem_bytes<N>());                                     \
-        if (e != cudaSuccess) return e;                                                       \
-        k_big_rows_fwd<N><<<blocks, fft::LG<N>::THREADS, smem_bytes<N>(), st>>>(                  \
-            Vr, rspan_n, Cu0n, cspan_n, Sboxr, tw.hi_hi, tw.hi_lo);                           \
-    }
+    if (N == 16384 && !cols_e16())                                                            \
+        e = launch_rows_fwd_e<N, (N == 16384 ? 32 : 16)>(rspan_n, Cu0n, cspan_n, Vr, Sboxr, tw, st); \
+    else                                                                                      \
+        e = launch_rows_fwd_e<N, 16>(rspan_n, Cu0n, cspan_n, Vr, Sboxr, tw, st);
     FPM_DISPATCH_BIG(H, F)
 #undef F
-    return cudaGetLastError();
+    return e;
 }
 
 }  // namespace fpm

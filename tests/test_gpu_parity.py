@@ -489,9 +489,10 @@ def test_isotropic_loss_gradients_and_solve(engine, ds_small, ds_a):
 
 
 def test_16384_columns_32_values_per_thread_match_16(engine):
-    """The 16384-point column pass runs radix-32 stages with 32 values per thread; the
-    16-value variant (FPM_COLS_E16=1) is the same transform with other roundings.  A short
-    solve at 2048^2 -> 16384^2 and a gradient call must agree to FP32 rounding."""
+    """The 16384-point passes run radix-32 stages with 32 values per thread; the 16-value
+    variant (FPM_COLS_E16=1) is the same transform with other roundings.  A short solve at
+    2048^2 -> 16384^2 and a gradient call must agree to FP32 rounding (isotropic loss: no
+    sign decisions that a rounding difference could flip)."""
     import os
     import torch
     from fpm_b200 import synth
@@ -512,11 +513,14 @@ def test_16384_columns_32_values_per_thread_match_16(engine):
     for flag in ("0", "1"):
         os.environ["FPM_COLS_E16"] = flag
         try:
-            r = engine.solve(O0, P0c, Y, ledt, P0, p, 1, 3, lr=1e-3, spectrum=False)
-            d = engine.batch_gradients(O0, P0c, Y, ledt, P0, p)
+            r = engine.solve(O0, P0c, Y, ledt, P0, p, 1, 3, lr=1e-3, spectrum=False,
+                             loss="isotropic")
+            d = engine.batch_gradients(O0, P0c, Y, ledt, P0, p, loss="isotropic")
             runs[flag] = (r["object"].cpu().numpy(), r["pupil"].cpu().numpy(),
                           d[0].cpu().numpy(), d[1].cpu().numpy())
         finally:
             del os.environ["FPM_COLS_E16"]
+    # two FP32 roundings of 16384^2 transforms (each ~5e-6 relative) apart; a wrong
+    # transform would be O(1) off
     for a, b in zip(runs["0"], runs["1"]):
-        assert orc.rel_err(a, b) < 1e-5, orc.rel_err(a, b)
+        assert orc.rel_err(a, b) < 3e-5, orc.rel_err(a, b)
