@@ -276,43 +276,65 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 }
 
 // ---------------------------------------------------------------------------
-// L2 + L3 fused: a CTA of 1024 threads takes LIN consecutive row lines r0-1 ..
-// r0+LOUT (modulo h) of one LED, runs their inverse FFTs, keeps the residuals of
-// all LIN lines in shared memory and finishes the LOUT central lines (stencil,
-// phase, forward FFT).  The two halo lines supply res(r -/+ 1, c); their inverse
-// FFTs are recomputed by the neighbouring CTAs.  The output goes to a second
-// buffer because neighbours still read the halo rows of the input.
+// L2 + L3 fused.  A 2-CTA cluster takes 2 LIN consecutive row lines r0-1 .. of one
+// LED (LIN per CTA, 1024 threads each): every line gets its inverse FFT and its
+// residual |z|/(h^2 p^2) - Y in shared memory; the CTAs then swap their boundary
+// residual rows through distributed shared memory, and the 2 LIN - 2 central lines
+// get the loss stencil, the phase and the forward FFT.  The pair's two outer lines
+// are halo: their inverse FFTs are recomputed by the neighbouring pairs.  The output
+// goes to a second buffer because neighbours still read the halo rows of the input.
 //
 // The row lines are strided in memory (element c of row r at c*h + r): instead of
 // 16 scattered 8-byte loads per thread, the TMA unit copies the CTA's tile of
 // rows [r0-2, r0-2+XR) x all columns into shared memory (boxes of XR x 256) and
 // the threads pick their values there; the stack tile of the same rows (uint16)
 // follows by TMA while the inverse FFTs run.  Lines whose row wraps past the
-// image edge (first and last CTA of an LED) read global memory directly.
+// image edge (first and last pair of an LED) read global memory directly.
 // ---------------------------------------------------------------------------
 template <int N>
 struct L23 {
     static constexpr int T = N / 16;
-    static constexpr int LIN = 1024 / T;              // lines per CTA, halo included
-    static constexpr int LOUT = LIN - 2;              // central lines per CTA
+    static constexpr int LIN = 1024 / T;              // lines per CTA
+    static constexpr int POUT = 2 * LIN - 2;          // central lines per 2-CTA cluster
     static constexpr int PAD = 16 / LIN > 0 ? 16 / LIN : 1;
     static constexpr int STRIDE = N + PAD;            // FFT exchange line stride (float2)
     // residual line stride (float): the 32 (line, t) pairs of a warp on 32 banks
     static constexpr int RSTRIDE = N + (LIN >= 32 ? 1 : 32 / LIN);
     static constexpr int LINE_BYTES = LIN * STRIDE * 8;
-    static constexpr int RES_BYTES = LIN * RSTRIDE * 4;
+    // residual rows: the LIN lines plus a ghost row above and below (the partner's)
+    static constexpr int RES_BYTES = (LIN + 2) * RSTRIDE * 4;
     static constexpr int CB = N < 256 ? N : 256;      // TMA box width along c
     static constexpr int XR = LIN == 8 ? 12 : LIN + 2;   // field tile rows (even; 12: no bank conflicts)
     static constexpr int YR = LIN + 8;                // stack tile rows (uint16, 16-byte aligned start)
     static constexpr int SMEM = LINE_BYTES + RES_BYTES + 2 * 128 * 8 + 16;
-    static constexpr int CTAS_PER_LED = (N + LOUT - 1) / LOUT;
+    static constexpr int PAIRS_PER_LED = (N + POUT - 1) / POUT;
+    static constexpr int CTAS_PER_LED = 2 * PAIRS_PER_LED;
     static constexpr int NHI = N >= 128 ? N / 128 : 1;
     static constexpr int NLO = N >= 128 ? 128 : N;
     static_assert(LIN >= 8 && LIN % 8 == 0, "fused row pass needs T <= 128");
+    static_assert(POUT % 2 == 0, "even pair stride keeps the TMA row start even");
     static_assert(XR * N * 8 <= LINE_BYTES + RES_BYTES, "field tile fits the line + residual areas");
     static_assert(YR * N * 2 <= RES_BYTES, "stack tile fits the residual area");
     static_assert(LINE_BYTES % 128 == 0, "residual area 128-byte aligned for TMA");
+    static_assert(SMEM + 256 <= 227 * 1024, "shared memory per CTA");
 };
+
+__device__ __forceinline__ void cluster_arrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// value at the same shared-memory location of CTA `rank` of this cluster
+__device__ __forceinline__ float cluster_load(const float *p, unsigned rank) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(remote)
+                 : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))), "r"(rank));
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(remote) : "memory");
+    return v;
+}
 
 template <int N, int TYPE, int LOSS>
 __global__ void __launch_bounds__(1024, 1)
@@ -325,14 +347,16 @@ __global__ void __launch_bounds__(1024, 1)
     constexpr int T = F::T;
     extern __shared__ __align__(128) float2 smem[];
     __shared__ double s_red[32];
-    float *res = reinterpret_cast<float *>(smem + F::LIN * F::STRIDE);
-    float2 *s_hi = reinterpret_cast<float2 *>(res + F::LIN * F::RSTRIDE);
+    float *res = reinterpret_cast<float *>(smem + F::LIN * F::STRIDE);   // row 0: ghost above
+    float2 *s_hi = reinterpret_cast<float2 *>(res + (F::LIN + 2) * F::RSTRIDE);
     uint64_t *bar = reinterpret_cast<uint64_t *>(s_hi + 256);          // [0] field, [1] stack
     const float2 *tile = smem;                                          // [c][XR] field tile
     const uint16_t *ytile = reinterpret_cast<const uint16_t *>(res);    // [c][YR] stack tile
     const int k = threadIdx.x % F::LIN, t = threadIdx.x / F::LIN;
-    const int lloc = blockIdx.x / F::CTAS_PER_LED;
-    const int r0 = (blockIdx.x % F::CTAS_PER_LED) * F::LOUT;
+    const unsigned j = blockIdx.x & 1;                  // rank in the 2-CTA cluster
+    const int pair = blockIdx.x >> 1;
+    const int lloc = pair / F::PAIRS_PER_LED;
+    const int r0 = (pair % F::PAIRS_PER_LED) * F::POUT + (int)j * F::LIN;   // rows r0-1+k
     const int x0 = r0 - 2;                      // first tile row (even: 16-byte TMA rule)
     const int y0 = (r0 - 1) & ~7;               // first stack tile row (8 x 2 bytes)
     const int zpage = g.z_off + l0 + lloc;
@@ -350,62 +374,61 @@ __global__ void __launch_bounds__(1024, 1)
     const int rraw = r0 - 1 + k;                        // row before the wrap
     const bool wrapped = rraw < 0 || rraw >= N;
     const int r = rraw < 0 ? rraw + N : (rraw >= N ? rraw - N : rraw);
-    const bool central = k >= 1 && k <= F::LOUT && rraw < N;
+    const int q = (int)j * F::LIN + k;                  // line within the pair
+    const bool central = q >= 1 && q <= F::POUT && rraw < N;
+    float *rk = res + (k + 1) * F::RSTRIDE;
     float2 v[16];
-    if (wrapped) {   // first / last CTA of an LED: the wrapped halo row from global memory
+    if (wrapped) {   // first / last pair of an LED: the wrapped halo row from global memory
         const float2 *page = T1 + (size_t)lloc * N * N + r;
 #pragma unroll
         for (int m = 0; m < 16; ++m) v[m] = page[(size_t)(t + m * T) * N];
     }
-    bool bad = !tma::mbar_wait(&bar[0], 0);
-    if (__syncthreads_or(bad)) {   // a tile load never completed: flag it, drain, leave
-        if (threadIdx.x == 0) {
-            atomicExch(flag, 1);
-            tma::mbar_wait(&bar[0], 0);
-        }
-        return;
+    // A tile load that never completes is flagged for the host; the CTA then skips its
+    // work but still passes both cluster barriers, so its partner never waits for ever.
+    bool failed = __syncthreads_or(!tma::mbar_wait(&bar[0], 0));
+    if (failed && threadIdx.x == 0) {
+        atomicExch(flag, 1);
+        tma::mbar_wait(&bar[0], 0);
     }
-    if (!wrapped) {
+    double lsum = 0.0;
+    if (!failed) {
+        if (!wrapped) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) v[m] = tile[(t + m * T) * F::XR + (rraw - x0)];
-    }
-    __syncthreads();                                    // the tile area becomes FFT scratch
-    if (TYPE == kStackU16 && threadIdx.x == 0) {
-        tma::fence_proxy_async();
-        tma::arrive_expect_tx(&bar[1], F::YR * N * 2);
+            for (int m = 0; m < 16; ++m) v[m] = tile[(t + m * T) * F::XR + (rraw - x0)];
+        }
+        __syncthreads();                                // the tile area becomes FFT scratch
+        if (TYPE == kStackU16 && threadIdx.x == 0) {
+            tma::fence_proxy_async();
+            tma::arrive_expect_tx(&bar[1], F::YR * N * 2);
 #pragma unroll 1
-        for (int q = 0; q < N / F::CB; ++q)
-            tma::load_3d(const_cast<uint16_t *>(ytile) + q * F::CB * F::YR, &tm_stack, y0,
-                         q * F::CB, zpage, &bar[1]);
-    }
-    float2 *line = smem + k * F::STRIDE;
-    fft::line_fft_regs<N, +1>(v, line, s_hi, s_hi + 128, t);
-    float mn = 0.f, range = 0.f;
-    if (TYPE == kStackU16) {
-        mn = (float)Y.minmax[0];
-        range = (float)(Y.minmax[1] - Y.minmax[0]);
-    }
-    const float ratio = (float)((double)N * N * g.pratio * g.pratio);
-    const size_t ypage = (size_t)zpage * N * N + r;
-    float *rk = res + k * F::RSTRIDE;
-    {
+            for (int qb = 0; qb < N / F::CB; ++qb)
+                tma::load_3d(const_cast<uint16_t *>(ytile) + qb * F::CB * F::YR, &tm_stack, y0,
+                             qb * F::CB, zpage, &bar[1]);
+        }
+        fft::line_fft_regs<N, +1>(v, smem + k * F::STRIDE, s_hi, s_hi + 128, t);
+        float mn = 0.f, range = 0.f;
+        if (TYPE == kStackU16) {
+            mn = (float)Y.minmax[0];
+            range = (float)(Y.minmax[1] - Y.minmax[0]);
+        }
+        const float ratio = (float)((double)N * N * g.pratio * g.pratio);
+        const size_t ypage = (size_t)zpage * N * N + r;
         float y[16];
         if (TYPE == kStackU16) {
-            bad = !tma::mbar_wait(&bar[1], 0);
-            if (__syncthreads_or(bad)) {
-                if (threadIdx.x == 0) {
-                    atomicExch(flag, 1);
-                    tma::mbar_wait(&bar[1], 0);
-                }
-                return;
+            failed = __syncthreads_or(!tma::mbar_wait(&bar[1], 0));
+            if (failed && threadIdx.x == 0) {
+                atomicExch(flag, 1);
+                tma::mbar_wait(&bar[1], 0);
             }
+            if (!failed) {
 #pragma unroll
-            for (int m = 0; m < 16; ++m) {
-                const int c = t + m * T;
-                const uint16_t raw = wrapped ? static_cast<const uint16_t *>(Y.ptr)[ypage + (size_t)c * N]
-                                             : ytile[c * F::YR + (rraw - y0)];
-                const float x = (float)raw - mn;
-                y[m] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+                for (int m = 0; m < 16; ++m) {
+                    const int c = t + m * T;
+                    const uint16_t raw = wrapped ? static_cast<const uint16_t *>(Y.ptr)[ypage + (size_t)c * N]
+                                                 : ytile[c * F::YR + (rraw - y0)];
+                    const float x = (float)raw - mn;
+                    y[m] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+                }
             }
             __syncthreads();                            // the stack tile area becomes residuals
         } else {
@@ -413,55 +436,71 @@ __global__ void __launch_bounds__(1024, 1)
             for (int m = 0; m < 16; ++m)
                 y[m] = amplitude<TYPE>(Y, ypage + (size_t)(t + m * T) * N, mn, range);
         }
+        if (!failed) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const float2 z = v[m];
-            rk[t + m * T] = sqrtf(z.x * z.x + z.y * z.y) / ratio - y[m];
-        }
-    }
-    __syncthreads();
-    const float gscale = (float)(g.pratio * g.pratio);
-    double lsum = 0.0;
-#pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const int c = t + m * T;
-        float2 o = make_float2(0.f, 0.f);
-        if (central) {
-            const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
-            const float d =
-                stencil<LOSS>(rk[c], rk[cp], rk[cm], rk[F::RSTRIDE + c], rk[c - F::RSTRIDE],
-                              LOSS == kLossAnisotropic ? 0.f : rk[F::RSTRIDE + cm],
-                              LOSS == kLossAnisotropic ? 0.f : rk[cp - F::RSTRIDE], lsum) *
-                gscale;
-            const float2 z = v[m];
-            const float mag = sqrtf(z.x * z.x + z.y * z.y);
-            if (mag > 0.f) {
-                const float inv = 1.0f / mag;
-                o.x = z.x * inv * d;
-                o.y = z.y * inv * d;
+            for (int m = 0; m < 16; ++m) {
+                const float2 z = v[m];
+                rk[t + m * T] = sqrtf(z.x * z.x + z.y * z.y) / ratio - y[m];
             }
         }
-        v[m] = o;
+        __syncthreads();
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = lsum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int w = 0; w < 32; ++w) tot += s_red[w];
-        parts[blockIdx.x] = tot;
+    // residual rows of both CTAs written: take the partner's boundary row as a ghost row
+    cluster_arrive();
+    cluster_wait();
+    if (!failed) {
+        float *ghost = j == 0 ? res + (F::LIN + 1) * F::RSTRIDE : res;
+        const float *theirs = j == 0 ? res + F::RSTRIDE : res + F::LIN * F::RSTRIDE;
+        for (int c = threadIdx.x; c < N; c += 1024) ghost[c] = cluster_load(theirs + c, j ^ 1u);
+        __syncthreads();
     }
-    fft::line_fft_regs<N, -1>(v, line, s_hi, s_hi + 128, t);
-    if (central) {   // only the columns the next pass transforms (pupil support, fftshifted)
-        float2 *dst = T2 + (size_t)lloc * N * N + r;
+    cluster_arrive();   // done with the partner's memory; waited for before leaving
+    if (!failed) {
+        const float gscale = (float)(g.pratio * g.pratio);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
-            const int cf = t + m * T;
-            const int c = cf + N / 2 >= N ? cf - N / 2 : cf + N / 2;
-            if (c >= g.pc_lo && c < g.pc_hi) dst[(size_t)cf * N] = v[m];
+            const int c = t + m * T;
+            float2 o = make_float2(0.f, 0.f);
+            if (central) {
+                const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
+                const float d =
+                    stencil<LOSS>(rk[c], rk[cp], rk[cm], rk[F::RSTRIDE + c], rk[c - F::RSTRIDE],
+                                  LOSS == kLossAnisotropic ? 0.f : rk[F::RSTRIDE + cm],
+                                  LOSS == kLossAnisotropic ? 0.f : rk[cp - F::RSTRIDE], lsum) *
+                    gscale;
+                const float2 z = v[m];
+                const float mag = sqrtf(z.x * z.x + z.y * z.y);
+                if (mag > 0.f) {
+                    const float inv = 1.0f / mag;
+                    o.x = z.x * inv * d;
+                    o.y = z.y * inv * d;
+                }
+            }
+            v[m] = o;
         }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
+        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = lsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < 32; ++w) tot += s_red[w];
+            parts[blockIdx.x] = tot;
+        }
+        fft::line_fft_regs<N, -1>(v, smem + k * F::STRIDE, s_hi, s_hi + 128, t);
+        if (central) {   // only the columns the next pass transforms (pupil support, fftshifted)
+            float2 *dst = T2 + (size_t)lloc * N * N + r;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int cf = t + m * T;
+                const int c = cf + N / 2 >= N ? cf - N / 2 : cf + N / 2;
+                if (c >= g.pc_lo && c < g.pc_hi) dst[(size_t)cf * N] = v[m];
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        parts[blockIdx.x] = 0.0;
     }
+    cluster_wait();
 }
 
 // ---------------------------------------------------------------------------
@@ -824,9 +863,9 @@ cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, 
 
 bool lr_rows_fused_supported(int h) { return h >= 128 && h <= 2048 && (h & (h - 1)) == 0; }
 
-static int ctas_per_led_fused(int h) {   // L23<h>::CTAS_PER_LED
-    const int lout = 1024 / (h / 16) - 2;
-    return (h + lout - 1) / lout;
+static int ctas_per_led_fused(int h) {   // L23<h>::CTAS_PER_LED: 2 CTAs per pair of LIN lines
+    const int pout = 2 * (1024 / (h / 16)) - 2;
+    return 2 * ((h + pout - 1) / pout);
 }
 
 int lr_rows_fused_blocks(int h, int nl) { return nl * ctas_per_led_fused(h); }
@@ -877,11 +916,23 @@ template <int N, int TYPE, int LOSS>
 static cudaError_t launch_fused_k(int blocks, StackView Y, const BatchGeom &g, int l0,
                                   const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
                                   const CUtensorMap &tm_stack, const Twiddles &tw, cudaStream_t st) {
-    cudaError_t e = set_smem(k_lr_rows_fused<N, TYPE, LOSS>, L23<N>::SMEM);
+    auto kern = k_lr_rows_fused<N, TYPE, LOSS>;
+    cudaError_t e = set_smem(kern, L23<N>::SMEM);
     if (e != cudaSuccess) return e;
-    k_lr_rows_fused<N, TYPE, LOSS><<<blocks, 1024, L23<N>::SMEM, st>>>(
-        Y, g, l0, b.T1, b.T2, b.parts + part_off, b.flag, tm_field, tm_stack, tw.lo_hi, tw.lo_lo);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = L23<N>::SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, Y, g, l0, (const float2 *)b.T1, b.T2, b.parts + part_off,
+                              b.flag, tm_field, tm_stack, tw.lo_hi, tw.lo_lo);
 }
 
 cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_pages, BatchBufs b,
@@ -891,7 +942,8 @@ cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_page
     cudaError_t e = cudaSuccess;
     CUtensorMap tm_field{}, tm_stack{};
 #define F(N)                                                                              \
-    static_assert(L23<N>::CTAS_PER_LED == (N + 1024 / (N / 16) - 3) / (1024 / (N / 16) - 2), \
+    static_assert(L23<N>::CTAS_PER_LED ==                                                 \
+                      2 * ((N + 2 * (1024 / (N / 16)) - 3) / (2 * (1024 / (N / 16)) - 2)),     \
                   "host CTA count");                                                      \
     e = page_tile_map(&tm_field, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, b.T1, N, nl,          \
                       L23<N>::XR, L23<N>::CB);                                            \
