@@ -291,11 +291,11 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 // follows by TMA while the inverse FFTs run.  Lines whose row wraps past the
 // image edge (first and last pair of an LED) read global memory directly.
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, int CL = 2>
 struct L23 {
     static constexpr int T = N / 16;
     static constexpr int LIN = 1024 / T;              // lines per CTA
-    static constexpr int POUT = 2 * LIN - 2;          // central lines per 2-CTA cluster
+    static constexpr int POUT = CL * LIN - 2;         // central lines per CL-CTA cluster
     static constexpr int PAD = 16 / LIN > 0 ? 16 / LIN : 1;
     static constexpr int STRIDE = N + PAD;            // FFT exchange line stride (float2)
     // residual line stride (float): the 32 (line, t) pairs of a warp on 32 banks
@@ -307,8 +307,8 @@ struct L23 {
     static constexpr int XR = LIN == 8 ? 12 : LIN + 2;   // field tile rows (even; 12: no bank conflicts)
     static constexpr int YR = LIN + 8;                // stack tile rows (uint16, 16-byte aligned start)
     static constexpr int SMEM = LINE_BYTES + RES_BYTES + 2 * 128 * 8 + 16;
-    static constexpr int PAIRS_PER_LED = (N + POUT - 1) / POUT;
-    static constexpr int CTAS_PER_LED = 2 * PAIRS_PER_LED;
+    static constexpr int PAIRS_PER_LED = (N + POUT - 1) / POUT;   // clusters per LED
+    static constexpr int CTAS_PER_LED = CL * PAIRS_PER_LED;
     static constexpr int NHI = N >= 128 ? N / 128 : 1;
     static constexpr int NLO = N >= 128 ? 128 : N;
     static_assert(LIN >= 8 && LIN % 8 == 0, "fused row pass needs T <= 128");
@@ -336,14 +336,14 @@ __device__ __forceinline__ float cluster_load(const float *p, unsigned rank) {
     return v;
 }
 
-template <int N, int TYPE, int LOSS>
+template <int N, int TYPE, int LOSS, int CL>
 __global__ void __launch_bounds__(1024, 1)
     k_lr_rows_fused(StackView Y, BatchGeom g, int l0, const float2 *__restrict__ T1,
                     float2 *__restrict__ T2, double *__restrict__ parts, int *__restrict__ flag,
                     const __grid_constant__ CUtensorMap tm_field,
                     const __grid_constant__ CUtensorMap tm_stack, const float2 *__restrict__ thi,
                     const float2 *__restrict__ tlo) {
-    using F = L23<N>;
+    using F = L23<N, CL>;
     constexpr int T = F::T;
     extern __shared__ __align__(128) float2 smem[];
     __shared__ double s_red[32];
@@ -353,8 +353,8 @@ __global__ void __launch_bounds__(1024, 1)
     const float2 *tile = smem;                                          // [c][XR] field tile
     const uint16_t *ytile = reinterpret_cast<const uint16_t *>(res);    // [c][YR] stack tile
     const int k = threadIdx.x % F::LIN, t = threadIdx.x / F::LIN;
-    const unsigned j = blockIdx.x & 1;                  // rank in the 2-CTA cluster
-    const int pair = blockIdx.x >> 1;
+    const unsigned j = blockIdx.x % CL;                 // rank in the cluster
+    const int pair = blockIdx.x / CL;
     const int lloc = pair / F::PAIRS_PER_LED;
     const int r0 = (pair % F::PAIRS_PER_LED) * F::POUT + (int)j * F::LIN;   // rows r0-1+k
     const int x0 = r0 - 2;                      // first tile row (even: 16-byte TMA rule)
@@ -449,9 +449,11 @@ __global__ void __launch_bounds__(1024, 1)
     cluster_arrive();
     cluster_wait();
     if (!failed) {
-        float *ghost = j == 0 ? res + (F::LIN + 1) * F::RSTRIDE : res;
-        const float *theirs = j == 0 ? res + F::RSTRIDE : res + F::LIN * F::RSTRIDE;
-        for (int c = threadIdx.x; c < N; c += 1024) ghost[c] = cluster_load(theirs + c, j ^ 1u);
+        // ghost above: the last line of rank j-1; ghost below: the first line of rank j+1
+        for (int c = threadIdx.x; c < N; c += 1024) {
+            if (j > 0) res[c] = cluster_load(res + F::LIN * F::RSTRIDE + c, j - 1);
+            if (j + 1 < CL) res[(F::LIN + 1) * F::RSTRIDE + c] = cluster_load(res + F::RSTRIDE + c, j + 1);
+        }
         __syncthreads();
     }
     cluster_arrive();   // done with the partner's memory; waited for before leaving
@@ -863,9 +865,12 @@ cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, 
 
 bool lr_rows_fused_supported(int h) { return h >= 128 && h <= 2048 && (h & (h - 1)) == 0; }
 
-static int ctas_per_led_fused(int h) {   // L23<h>::CTAS_PER_LED: 2 CTAs per pair of LIN lines
-    const int pout = 2 * (1024 / (h / 16)) - 2;
-    return 2 * ((h + pout - 1) / pout);
+static int fused_cluster();
+
+static int ctas_per_led_fused(int h) {   // L23<h, CL>::CTAS_PER_LED
+    const int cl = fused_cluster();
+    const int pout = cl * (1024 / (h / 16)) - 2;
+    return cl * ((h + pout - 1) / pout);
 }
 
 int lr_rows_fused_blocks(int h, int nl) { return nl * ctas_per_led_fused(h); }
@@ -912,21 +917,21 @@ static cudaError_t page_tile_map(CUtensorMap *map, CUtensorMapDataType type, siz
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-template <int N, int TYPE, int LOSS>
-static cudaError_t launch_fused_k(int blocks, StackView Y, const BatchGeom &g, int l0,
-                                  const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
-                                  const CUtensorMap &tm_stack, const Twiddles &tw, cudaStream_t st) {
-    auto kern = k_lr_rows_fused<N, TYPE, LOSS>;
-    cudaError_t e = set_smem(kern, L23<N>::SMEM);
+template <int N, int TYPE, int LOSS, int CL>
+static cudaError_t launch_fused_cl(int nl, StackView Y, const BatchGeom &g, int l0,
+                                   const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
+                                   const CUtensorMap &tm_stack, const Twiddles &tw, cudaStream_t st) {
+    auto kern = k_lr_rows_fused<N, TYPE, LOSS, CL>;
+    cudaError_t e = set_smem(kern, L23<N, CL>::SMEM);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.gridDim = dim3((unsigned)(nl * L23<N, CL>::CTAS_PER_LED));
     cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = L23<N>::SMEM;
+    cfg.dynamicSmemBytes = L23<N, CL>::SMEM;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.x = CL;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
@@ -935,33 +940,47 @@ static cudaError_t launch_fused_k(int blocks, StackView Y, const BatchGeom &g, i
                               b.flag, tm_field, tm_stack, tw.lo_hi, tw.lo_lo);
 }
 
+// cluster size of the fused row pass: 2 (FPM_L23_CLUSTER=4 for measurements)
+static int fused_cluster() {
+    const char *e = std::getenv("FPM_L23_CLUSTER");
+    return e && std::atoi(e) == 4 ? 4 : 2;
+}
+
+template <int N, int TYPE, int LOSS>
+static cudaError_t launch_fused_k(int nl, StackView Y, const BatchGeom &g, int l0,
+                                  const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
+                                  const CUtensorMap &tm_stack, const Twiddles &tw, cudaStream_t st) {
+    return fused_cluster() == 4
+               ? launch_fused_cl<N, TYPE, LOSS, 4>(nl, Y, g, l0, b, part_off, tm_field, tm_stack, tw, st)
+               : launch_fused_cl<N, TYPE, LOSS, 2>(nl, Y, g, l0, b, part_off, tm_field, tm_stack, tw, st);
+}
+
 cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_pages, BatchBufs b,
                                  int l0, int nl, int part_off, const Twiddles &tw,
                                  cudaStream_t st) {
-    const int blocks = lr_rows_fused_blocks(g.h, nl);
     cudaError_t e = cudaSuccess;
     CUtensorMap tm_field{}, tm_stack{};
 #define F(N)                                                                              \
-    static_assert(L23<N>::CTAS_PER_LED ==                                                 \
+    static_assert(L23<N, 2>::CTAS_PER_LED ==                                              \
                       2 * ((N + 2 * (1024 / (N / 16)) - 3) / (2 * (1024 / (N / 16)) - 2)),     \
                   "host CTA count");                                                      \
     e = page_tile_map(&tm_field, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, b.T1, N, nl,          \
-                      L23<N>::XR, L23<N>::CB);                                            \
+                      L23<N, 2>::XR, L23<N, 2>::CB);                                            \
     if (e != cudaSuccess) return e;                                                       \
     if (Y.type == kStackU16) {                                                            \
         e = page_tile_map(&tm_stack, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, Y.ptr, N,         \
-                          stack_pages, L23<N>::YR, L23<N>::CB);                           \
+                          stack_pages, L23<N, 2>::YR, L23<N, 2>::CB);                           \
         if (e != cudaSuccess) return e;                                                   \
         e = g.loss == kLossIsotropic                                                      \
-                ? launch_fused_k<N, kStackU16, kLossIsotropic>(blocks, Y, g, l0, b, part_off, \
+                ? launch_fused_k<N, kStackU16, kLossIsotropic>(nl, Y, g, l0, b, part_off, \
                                                                tm_field, tm_stack, tw, st)    \
-                : launch_fused_k<N, kStackU16, kLossAnisotropic>(blocks, Y, g, l0, b, part_off, \
+                : launch_fused_k<N, kStackU16, kLossAnisotropic>(nl, Y, g, l0, b, part_off, \
                                                                  tm_field, tm_stack, tw, st); \
     } else {                                                                              \
         e = g.loss == kLossIsotropic                                                      \
-                ? launch_fused_k<N, kStackF32, kLossIsotropic>(blocks, Y, g, l0, b, part_off, \
+                ? launch_fused_k<N, kStackF32, kLossIsotropic>(nl, Y, g, l0, b, part_off, \
                                                                tm_field, tm_stack, tw, st)    \
-                : launch_fused_k<N, kStackF32, kLossAnisotropic>(blocks, Y, g, l0, b, part_off, \
+                : launch_fused_k<N, kStackF32, kLossAnisotropic>(nl, Y, g, l0, b, part_off, \
                                                                  tm_field, tm_stack, tw, st); \
     }                                                                                     \
     if (e != cudaSuccess) return e;
