@@ -420,7 +420,7 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const
         g.pc_hi = sup.c_hi;
         g.loss = loss == FPM_LOSS_ISOTROPIC ? kLossIsotropic : kLossAnisotropic;
         pl.geoms.push_back(g);
-        pl.ldU = std::max(pl.ldU, g.rspan);
+        pl.ldU = std::max(pl.ldU, (g.rspan + 3) & ~3);   // columns 32-byte aligned (bulk copies)
         pl.sbox = std::max(pl.sbox, (size_t)g.rspan * g.cspan);
     }
     // LEDs per low-resolution launch: the whole batch (measured fastest: large
@@ -829,6 +829,7 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
             a.ldV = pl.ldU;
             a.Ru0n = last ? 0 : gn.Ru0;
             a.rspan_n = last ? 0 : gn.rspan;
+            a.err = ctx->flag.as<int>();
             FPM_STAGE(ST_COLS_UPDATE, launch_big_cols(a, tw, st));
             if (!last) {
                 rc = rows_forward(ctx, pl, tw, gn);

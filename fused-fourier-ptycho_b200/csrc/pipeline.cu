@@ -729,6 +729,145 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
 }
 
 // ---------------------------------------------------------------------------
+// Pass B, update mode, persistent with prefetch (N = 16384, 32 values per thread).
+// A CTA per SM walks the columns c = blockIdx.x + k gridDim.x; while it transforms
+// one column, bulk copies bring the next column's RMSprop moment (64 KiB) and, when
+// they fit, its gradient rows into shared memory, so those loads leave the critical
+// path.  Waits are bounded; a copy that never completes sets the device flag and the
+// CTA drains its copies in flight and stops.
+// ---------------------------------------------------------------------------
+constexpr int kColsUCap = 4096;   // gradient rows staged in shared memory (32 KiB)
+
+template <int N, int E>
+struct ColsAsync {
+    static constexpr int SMEM = N * 8 + 2 * 128 * 8 + N * 4 + kColsUCap * 8 + 16;
+    static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+    static_assert(fft::LG<N, E>::LPC == 1, "one line per CTA");
+};
+
+template <int N, int E>
+__global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
+    k_big_cols_async(ColsArgs a, const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
+    using G = fft::LG<N, E>;
+    extern __shared__ __align__(128) float2 smem[];
+    float2 *line = smem;
+    float2 *s_hi = smem + N;
+    float *mbuf = reinterpret_cast<float *>(smem + N + 256);
+    float2 *ubuf = reinterpret_cast<float2 *>(mbuf + N);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ubuf + kColsUCap);   // [0] moment, [1] rows
+    const int t = threadIdx.x;
+    const bool u_async = a.rspan > 0 && a.rspan <= kColsUCap;
+    const uint32_t ubytes = (uint32_t)((a.rspan + 1) & ~1) * 8u;
+    int c = blockIdx.x;
+    if (t == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_barrier_init();
+        if (c < N) {
+            tma::arrive_expect_tx(&bar[0], N * 4);
+            tma::load_1d(mbuf, a.m + (size_t)c * N, N * 4, &bar[0]);
+            if (u_async) {
+                tma::arrive_expect_tx(&bar[1], ubytes);
+                tma::load_1d(ubuf, a.U + (size_t)c * a.ldU, ubytes, &bar[1]);
+            }
+        }
+    }
+    fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, G::NHI, G::NLO);
+    __syncthreads();
+    // each barrier completes once per column: the parity of the copy in flight, and
+    // whether one is in flight (block-uniform)
+    uint32_t pm = 0, pu = 0;
+    bool mp = c < N, up = c < N && u_async;
+    bool failed = false;
+    const float omb = 1.0f - a.beta;
+    for (; c < N; c += gridDim.x) {
+        const int cn = c + gridDim.x;
+        const size_t col = (size_t)c * N;
+        float2 v[E];
+        if (u_async) {
+            failed = __syncthreads_or(!tma::mbar_wait(&bar[1], pu));
+            if (failed) break;
+            up = false;
+            pu ^= 1u;
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                int i = t + m * G::T - a.Ru0;          // box row of element e
+                if (i < 0) i += N;
+                v[m] = i < a.rspan ? ubuf[i] : make_float2(0.f, 0.f);
+            }
+            __syncthreads();                           // the rows buffer is free
+            if (cn < N) {
+                if (t == 0) {
+                    tma::fence_proxy_async();
+                    tma::arrive_expect_tx(&bar[1], ubytes);
+                    tma::load_1d(ubuf, a.U + (size_t)cn * a.ldU, ubytes, &bar[1]);
+                }
+                up = true;
+            }
+        } else {
+            const float2 *u = a.U + (size_t)c * a.ldU;
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                int i = t + m * G::T - a.Ru0;
+                if (i < 0) i += N;
+                v[m] = i < a.rspan ? u[i] : make_float2(0.f, 0.f);
+            }
+        }
+        line_fft_e<N, +1, E>(v, line, s_hi, s_hi + 128, t);
+        failed = __syncthreads_or(!tma::mbar_wait(&bar[0], pm));
+        if (failed) break;
+        mp = false;
+        pm ^= 1u;
+        // RMSprop on the column (constrained_RMSprop_both, kernels.cuh:364-382)
+#pragma unroll
+        for (int m0 = 0; m0 < E; m0 += 4) {
+            float2 w[4];
+            float mv[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                w[k] = a.O[col + t + (m0 + k) * G::T];
+                mv[k] = mbuf[t + (m0 + k) * G::T];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float2 gv = v[m0 + k];
+                float mu = gv.x * gv.x + gv.y * gv.y;
+                mu = a.beta * mv[k] + omb * mu;
+                const float sq = a.lr / (sqrtf(mu) + a.eps);
+                w[k].x -= gv.x * sq;
+                w[k].y -= gv.y * sq;
+                a.O[col + t + (m0 + k) * G::T] = w[k];
+                a.m[col + t + (m0 + k) * G::T] = mu;
+                v[m0 + k] = w[k];
+            }
+        }
+        __syncthreads();                               // the moment buffer is free
+        if (cn < N) {
+            if (t == 0) {
+                tma::fence_proxy_async();
+                tma::arrive_expect_tx(&bar[0], N * 4);
+                tma::load_1d(mbuf, a.m + (size_t)cn * N, N * 4, &bar[0]);
+            }
+            mp = true;
+        }
+        if (a.rspan_n == 0) continue;                  // uniform: no next batch
+        line_fft_e<N, -1, E>(v, line, s_hi, s_hi + 128, t);
+        float2 *vv = a.V + (size_t)c * a.ldV;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            int i = t + m * G::T - a.Ru0n;
+            if (i < 0) i += N;
+            if (i < a.rspan_n) vv[i] = v[m];
+        }
+    }
+    if (failed && t == 0) {
+        atomicExch(a.err, 1);
+        if (mp) tma::mbar_wait(&bar[0], pm);           // bounded drains of copies in flight
+        if (up) tma::mbar_wait(&bar[1], pu);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Pass C: rows of V (strided) -> FFT along the row -> the next batch's Sbox
 // ---------------------------------------------------------------------------
 template <int N, int E>
@@ -1063,7 +1202,29 @@ static bool cols_e16() {
     return e && std::atoi(e) != 0;
 }
 
+// FPM_COLS_ASYNC=0 runs the update with plain loads (measurements)
+static bool cols_async() {
+    const char *e = std::getenv("FPM_COLS_ASYNC");
+    return !(e && std::atoi(e) == 0);
+}
+
+static cudaError_t launch_cols_async(const ColsArgs &a, const Twiddles &tw, cudaStream_t st) {
+    constexpr int N = 16384, E = 32;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = set_smem(k_big_cols_async<N, E>, ColsAsync<N, E>::SMEM);
+    if (e != cudaSuccess) return e;
+    const int grid = sms < N ? sms : N;
+    k_big_cols_async<N, E><<<grid, fft::LG<N, E>::THREADS, ColsAsync<N, E>::SMEM, st>>>(
+        a, tw.hi_hi, tw.hi_lo);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t st) {
+    if (a.H == 16384 && a.mode == kColsUpdate && a.err && !cols_e16() && cols_async())
+        return launch_cols_async(a, tw, st);
     cudaError_t e = cudaSuccess;
 #define F(N)                                                                                  \
     if (N == 16384 && !cols_e16())                                                            \

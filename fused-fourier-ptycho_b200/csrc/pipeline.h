@@ -88,6 +88,7 @@ struct ColsArgs {
     float2 *V = nullptr;
     int ldV = 0, Ru0n = 0, rspan_n = 0;
     float2 *gout = nullptr;
+    int *err = nullptr;   // device flag set when a bounded wait gives up (update mode)
 };
 cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t st);
 
