@@ -47,6 +47,9 @@ cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cud
 cudaError_t launch_stack_minmax(const uint16_t *p, size_t n, unsigned *minmax, cudaStream_t st);
 cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *minmax, float *out,
                              cudaStream_t st);
+// float stack: min / max and normalise in two launches; mm: 2 unsigned of scratch
+cudaError_t launch_normalise_f32(const float *p, size_t n, unsigned *mm, float *out,
+                                 cudaStream_t st);
 
 // box = {min row, max row, min col, max col} of the non-zero pixels of P (complex) or A
 // (real), either may be NULL; {h, -1, h, -1} when none

@@ -26,6 +26,7 @@
 #include "engine.h"
 #include "fft.h"
 #include "pipeline.h"
+#include "tiff.h"
 
 using namespace fpm;
 
@@ -160,13 +161,16 @@ struct fpm_context {
 
 namespace {
 
+// detail of the last failure of a call made without a context, per host thread
+thread_local std::string t_err;
+
 fpm_status fail(fpm_context *ctx, fpm_status s, const char *fmt, ...) {
-    char buf[512];
+    char buf[1024];
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(buf, sizeof buf, fmt, ap);
     va_end(ap);
-    if (ctx) ctx->err = buf;
+    (ctx ? ctx->err : t_err) = buf;
     return s;
 }
 
@@ -602,7 +606,7 @@ const char *fpm_status_string(fpm_status s) {
     return "unknown status";
 }
 
-const char *fpm_last_error(const fpm_context *ctx) { return ctx ? ctx->err.c_str() : ""; }
+const char *fpm_last_error(const fpm_context *ctx) { return ctx ? ctx->err.c_str() : t_err.c_str(); }
 
 fpm_status fpm_set_profiling(fpm_context *ctx, int32_t enable) {
     if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
@@ -1185,6 +1189,57 @@ fpm_status fpm_normalise_stack(fpm_context *ctx, const uint16_t *counts, size_t 
     FPM_CK(launch_normalise(src, n, ctx->minmax.as<unsigned>(), dst, st));
     if (!dev) FPM_CK(cudaMemcpyAsync(amplitude, dst, n * 4, cudaMemcpyDeviceToHost, st));
     FPM_CK(cudaStreamSynchronize(st));
+    return FPM_OK;
+}
+
+fpm_status fpm_normalise_stack_f32(fpm_context *ctx, const float *values, size_t n,
+                                   float *amplitude, int32_t memory) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (!values || !amplitude || n == 0)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "values/amplitude NULL or n == 0");
+    FPM_CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const bool dev = memory == FPM_MEM_DEVICE;
+    if (memory != FPM_MEM_DEVICE && memory != FPM_MEM_HOST)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", memory);
+    if (dev && (!is_device_ptr(values, ctx->device) || !is_device_ptr(amplitude, ctx->device)))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not device memory");
+    if (!dev && (!is_host_ptr(values) || !is_host_ptr(amplitude)))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not host memory");
+    if (dev) {
+        const fpm_status rc = order_after_default_stream(ctx);
+        if (rc != FPM_OK) return rc;
+    }
+    const float *src = values;
+    float *dst = amplitude;
+    if (!dev) {
+        // normalised in place in one device buffer
+        FPM_CK(ctx->spec.ensure(n * 4));
+        FPM_CK(cudaMemcpyAsync(ctx->spec.p, values, n * 4, cudaMemcpyHostToDevice, st));
+        src = dst = ctx->spec.as<float>();
+    }
+    FPM_CK(ctx->minmax.ensure(2 * sizeof(unsigned)));
+    FPM_CK(launch_normalise_f32(src, n, ctx->minmax.as<unsigned>(), dst, st));
+    if (!dev) FPM_CK(cudaMemcpyAsync(amplitude, dst, n * 4, cudaMemcpyDeviceToHost, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    return FPM_OK;
+}
+
+fpm_status fpm_read_tiff_stack(fpm_context *ctx, const char *const *paths, int32_t n_images,
+                               int32_t row0, int32_t col0, int32_t h, int32_t type, void *stack,
+                               int32_t threads) {
+    (ctx ? ctx->err : t_err).clear();
+    if (!paths || !stack || n_images <= 0 || h <= 0)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "paths/stack NULL, n_images <= 0 or h <= 0");
+    if (type != FPM_INGEST_U16 && type != FPM_INGEST_F32_MEAN)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "type = %d", type);
+    if (row0 < 0 || col0 < 0)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "row0 = %d, col0 = %d", row0, col0);
+    const std::string err =
+        read_tiff_stack(paths, n_images, row0, col0, h,
+                        type == FPM_INGEST_U16 ? TiffOut::kU16 : TiffOut::kF32Mean, stack, threads);
+    if (!err.empty()) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "%s", err.c_str());
     return FPM_OK;
 }
 

@@ -288,6 +288,67 @@ cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *mm, fl
     return cudaGetLastError();
 }
 
+
+// Float stacks (multi-sample frames averaged on ingest): the same min / max and
+// sqrt((x - min) / (max - min)), min / max over order-preserving integer keys
+// of the float bits (NaN skipped, as MATLAB's min / max omit NaN).
+__device__ __forceinline__ unsigned float_key(float x) {
+    const unsigned b = __float_as_uint(x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void __launch_bounds__(256) k_stack_minmax_f32(const float *__restrict__ p, size_t n,
+                                                           unsigned *__restrict__ mm) {
+    unsigned lo = 0xffffffffu, hi = 0u;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float x = p[i];
+        if (x != x) continue;
+        const unsigned k = float_key(x);
+        lo = k < lo ? k : lo;
+        hi = k > hi ? k : hi;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned a = __shfl_down_sync(0xffffffffu, lo, off);
+        const unsigned b = __shfl_down_sync(0xffffffffu, hi, off);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&mm[0], lo);
+        atomicMax(&mm[1], hi);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_normalise_f32(const float *p, size_t n,
+                                                        const unsigned *__restrict__ mm,
+                                                        float *out) {  // out may equal p
+    const float mn = key_float(mm[0]);
+    const float range = key_float(mm[1]) - mn;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float x = p[i] - mn;
+        out[i] = range > 0.f ? sqrtf(x / range) : sqrtf(x);  // constant stack: zeros, as for uint16
+    }
+}
+
+cudaError_t launch_normalise_f32(const float *p, size_t n, unsigned *mm, float *out,
+                                 cudaStream_t st) {
+    const unsigned init[2] = {0xffffffffu, 0u};
+    cudaError_t e = cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    size_t gx = (n + 255) / 256;
+    if (gx > (size_t)kB200SMs * 16) gx = (size_t)kB200SMs * 16;
+    if (gx == 0) gx = 1;
+    k_stack_minmax_f32<<<(unsigned)gx, 256, 0, st>>>(p, n, mm);
+    k_normalise_f32<<<(unsigned)gx, 256, 0, st>>>(p, n, mm, out);
+    return cudaGetLastError();
+}
+
 }  // namespace fpm
 
 namespace fpm {

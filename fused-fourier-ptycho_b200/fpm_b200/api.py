@@ -13,12 +13,13 @@ their index order is MATLAB's, and they are handed to the C ABI in
 column-major memory order (numpy Fortran order; for torch, dimensions
 reversed and made contiguous, which is free for tensors already laid out so).
 
-There is no CPU path: without the built library or a CUDA device every call
-raises.
+There is no CPU path: without the built library or a CUDA device every compute
+call raises.  Only the frame reader (``read_tiff_stack``) is host code by nature.
 """
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -38,10 +39,11 @@ _LOSS = {"anisotropic": LOSS_ANISOTROPIC, "isotropic": LOSS_ISOTROPIC}
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
             "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
-            "fpm_led_indices", "fpm_simulate"]
+            "fpm_led_indices", "fpm_simulate", "fpm_normalise_stack_f32", "fpm_read_tiff_stack"]
 
 
 SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
+INGEST_U16, INGEST_F32_MEAN = 0, 1
 
 
 class FpmError(RuntimeError):
@@ -125,6 +127,12 @@ def load_library(path: str | Path | None = None):
     lib.fpm_simulate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                  C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
     lib.fpm_simulate.restype = C.c_int
+    lib.fpm_normalise_stack_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                            C.c_int32]
+    lib.fpm_normalise_stack_f32.restype = C.c_int
+    lib.fpm_read_tiff_stack.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int32, C.c_int32,
+                                        C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
+    lib.fpm_read_tiff_stack.restype = C.c_int
     lib.fpm_abi_version.argtypes = []
     lib.fpm_abi_version.restype = C.c_int32
     if path is None:
@@ -360,21 +368,53 @@ class Engine:
         return out
 
     def normalise_stack(self, counts):
-        """Amplitude sqrt((I-min)/(max-min)) of a uint16 stack, same shape, float32."""
+        """Amplitude sqrt((I-min)/(max-min)) over a whole uint16 or float32 stack
+        (codes_v2/main_run_FPM.m:43-45), same shape, float32."""
         if _is_torch(counts):
             import torch
             x = counts.contiguous()
+            if x.dtype not in (torch.uint16, torch.float32):
+                raise TypeError(f"expected uint16 or float32, got {x.dtype}")
+            fn = (self.lib.fpm_normalise_stack if x.dtype == torch.uint16
+                  else self.lib.fpm_normalise_stack_f32)
             out = torch.empty(x.shape, dtype=torch.float32, device=x.device)
             mem = MEM_DEVICE if x.is_cuda else MEM_HOST
             _inputs_ready(x)
-            self._check(self.lib.fpm_normalise_stack(self._ctx, x.data_ptr(), x.numel(),
-                                                     out.data_ptr(), mem))
+            self._check(fn(self._ctx, x.data_ptr(), x.numel(), out.data_ptr(), mem))
             return out
-        x = np.ascontiguousarray(counts, dtype=np.uint16)
+        x = np.asarray(counts)
+        if x.dtype == np.float32:
+            fn = self.lib.fpm_normalise_stack_f32
+        else:
+            x, fn = x.astype(np.uint16, copy=False), self.lib.fpm_normalise_stack
+        x = np.ascontiguousarray(x)
         out = np.empty(x.shape, np.float32)
-        self._check(self.lib.fpm_normalise_stack(self._ctx, x.ctypes.data, x.size,
-                                                 out.ctypes.data, MEM_HOST))
+        self._check(fn(self._ctx, x.ctypes.data, x.size, out.ctypes.data, MEM_HOST))
         return out
+
+    def read_stack(self, paths, h, row0=0, col0=0, dtype="u16", threads=0):
+        """read_tiff_stack, failures reported on this context."""
+        return read_tiff_stack(paths, h, row0, col0, dtype, threads, _ctx=self)
+
+
+def read_tiff_stack(paths, h, row0=0, col0=0, dtype="u16", threads=0, _ctx=None):
+    """Measured frames, one TIFF per LED in LED order (codes_v2/main_run_FPM.m:26-41):
+    the h x h region at 0-based (row0, col0) of each file, as a MATLAB-order (h, h, L)
+    array in column-major memory: uint16 counts (dtype "u16", single-sample frames)
+    or the float32 mean over each pixel's samples (dtype "f32", mean(single(x), 3)).
+    Host-side; needs no GPU.  Raises FpmError naming the file on an unreadable,
+    unsupported or too small file."""
+    lib = load_library()
+    kind = {"u16": INGEST_U16, "f32": INGEST_F32_MEAN}[dtype]
+    names = [os.fsencode(p) for p in paths]
+    arr = (C.c_char_p * max(1, len(names)))(*names)
+    out = np.empty((h, h, len(names)), np.uint16 if kind == INGEST_U16 else np.float32, order="F")
+    ctx = _ctx._ctx if _ctx is not None else None
+    st = lib.fpm_read_tiff_stack(ctx, arr, len(names), int(row0), int(col0), int(h), kind,
+                                 out.ctypes.data, int(threads))
+    if st != FPM_OK:
+        raise FpmError(st, lib.fpm_last_error(ctx).decode())
+    return out
 
 
 _default_engine = None

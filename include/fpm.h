@@ -150,6 +150,34 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *prob,
 fpm_status fpm_normalise_stack(fpm_context *ctx, const uint16_t *counts, size_t n,
                                float *amplitude, int32_t memory);
 
+/* fpm_normalise_stack for a float stack (fpm_read_tiff_stack with
+   FPM_INGEST_F32_MEAN): amplitude = sqrt((x-min)/(max-min)) over all n values,
+   NaN left out of the min / max as MATLAB's min / max do. */
+fpm_status fpm_normalise_stack_f32(fpm_context *ctx, const float *values, size_t n,
+                                   float *amplitude, int32_t memory);
+
+/* Element type fpm_read_tiff_stack writes. */
+typedef enum fpm_ingest_type {
+    FPM_INGEST_U16 = 0,      /* uint16 counts (single-sample frames): the stack of
+                                FPM_STACK_U16_COUNTS, normalised inside fpm_solve */
+    FPM_INGEST_F32_MEAN = 1  /* float mean over each pixel's samples, mean(single(x), 3) */
+} fpm_ingest_type;
+
+/* Ingest of the measured frames (codes_v2/main_run_FPM.m:26-41): for each of the
+   n_images files, in LED order, the h x h pixel region whose top-left pixel is
+   (row0, col0), 0-based (the reference's imread 'PixelRegion' {[rect(2),
+   rect(2)+pix-1], [rect(1), rect(1)+pix-1]} is row0 = rect(2)-1, col0 = rect(1)-1),
+   into page i of the host array `stack` (column-major h*h per page).  Reads the
+   first image of baseline TIFF files: uncompressed strips, 8- or 16-bit unsigned
+   samples, 1 to 4 samples per pixel (chunky), either byte order; anything else,
+   a region outside the image or a short file fails with FPM_ERR_INVALID_ARGUMENT
+   naming the file.  Host-side only: the files are read on `threads` host threads
+   (<= 0: one per hardware thread, at most 32).  ctx may be NULL (no device is
+   needed); the failure detail then goes to fpm_last_error(NULL). */
+fpm_status fpm_read_tiff_stack(fpm_context *ctx, const char *const *paths, int32_t n_images,
+                               int32_t row0, int32_t col0, int32_t h, int32_t type, void *stack,
+                               int32_t threads);
+
 /* The engine's own unnormalised 2-D FFT of `count` column-major n x n complex
    pages (direction -1 forward, +1 inverse), the transform behind the cuFFT calls
    of cuFPM_pure_v3.cu:135-187.  n: power of two, 16 <= n <= 16384.  in may equal
@@ -243,7 +271,9 @@ int32_t fpm_stage_times(const fpm_context *ctx, fpm_stage_time *out, int32_t cap
 
 const char *fpm_status_string(fpm_status s);
 
-/* Human-readable detail of the last failure on this context ("" if none). */
+/* Human-readable detail of the last failure on this context ("" if none); with
+   ctx NULL, of the calling host thread's last failed fpm_read_tiff_stack made
+   without a context. */
 const char *fpm_last_error(const fpm_context *ctx);
 
 int32_t fpm_abi_version(void);

@@ -337,6 +337,40 @@ def normalise_stack_u16(I_u16):
     return np.sqrt(x).astype(np.float32)
 
 
+def normalise_stack_f32(x):
+    """The same ``sqrt((x - min) / max(x - min))`` over a float stack, in single, with
+    NaN left out of the min / max (MATLAB ``min`` / ``max`` omit NaN).  A constant
+    stack gives zeros (no division), as ``normalise_stack_u16``."""
+    x = np.asarray(x, np.float32)
+    mn = np.float32(np.nanmin(x))
+    d = x - mn
+    mx = np.float32(np.nanmax(x)) - mn
+    d = d / mx if mx > 0 else d
+    return np.sqrt(d).astype(np.float32)
+
+
+def read_frame(path, row0: int, col0: int, h: int):
+    """One measured frame as ``codes_v2/main_run_FPM.m:37-40`` loads it:
+    ``mean(single(imread(name, 'PixelRegion', {rows, cols})), 3)``, the h x h region
+    whose top-left pixel is (row0, col0), 0-based.  Decoded by Pillow (an
+    independent TIFF decoder standing in for MATLAB's imread); returns float32
+    (h, h) in [row, col] order."""
+    from PIL import Image
+    with Image.open(path) as im:
+        a = np.asarray(im)
+    a = a[row0:row0 + h, col0:col0 + h]
+    if a.shape[:2] != (h, h):
+        raise ValueError("pixel region outside the image")
+    a = a.astype(np.float32)
+    if a.ndim == 3:
+        # single-precision sum then one division, as MATLAB's mean of single
+        s = np.zeros(a.shape[:2], np.float32)
+        for k in range(a.shape[2]):
+            s = s + a[:, :, k]
+        a = s / np.float32(a.shape[2])
+    return a
+
+
 def _cubic(x, a=-0.5):
     ax = np.abs(x)
     ax2 = ax * ax
