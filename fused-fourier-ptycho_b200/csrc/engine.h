@@ -47,6 +47,23 @@ cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cud
 cudaError_t launch_stack_minmax(const uint16_t *p, size_t n, unsigned *minmax, cudaStream_t st);
 cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *minmax, float *out,
                              cudaStream_t st);
+// One step of a MATLAB optimiser class over n complex parameters (optimizers.cu).
+enum OptKind { kOptRmsprop = 0, kOptAdam = 1, kOptYogi = 2, kOptSgd = 3 };
+struct OptStep {
+    int kind = kOptRmsprop;
+    size_t n = 0;
+    float2 *p = nullptr;
+    const float2 *g = nullptr;
+    float2 *mom1 = nullptr;    // Adam / Yogi first moment; RMSprop g0 (centered), else null
+    float *mom2 = nullptr;     // Adam / Yogi second moment
+    float2 *buffer = nullptr;  // RMSprop momentum buffer (momentum > 0), else null
+    const float *amp = nullptr;  // pupil clamp amplitude, null = no clamp
+    // scalars rounded to single from the double values: r1, 1 - r1, r2, 1 - r2, lr,
+    // momentum, Adam's bias sqrt(1 - r2^t) / (1 - r1^t), clamp margin
+    float r1 = 0, c1 = 0, r2 = 0, c2 = 0, lr = 0, mum = 0, bias = 1, margin = 0;
+};
+cudaError_t launch_optimizer_step(const OptStep &o, cudaStream_t st);
+
 // float stack: min / max and normalise in two launches; mm: 2 unsigned of scratch
 cudaError_t launch_normalise_f32(const float *p, size_t n, unsigned *mm, float *out,
                                  cudaStream_t st);

@@ -157,6 +157,7 @@ struct fpm_context {
     // work buffers, kept between calls
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
         minmax, spec, flag;
+    DevBuf opt[6];   // device copies of an optimiser step's host arrays
 };
 
 namespace {
@@ -1240,6 +1241,99 @@ fpm_status fpm_read_tiff_stack(fpm_context *ctx, const char *const *paths, int32
         read_tiff_stack(paths, n_images, row0, col0, h,
                         type == FPM_INGEST_U16 ? TiffOut::kU16 : TiffOut::kF32Mean, stack, threads);
     if (!err.empty()) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+    return FPM_OK;
+}
+
+fpm_status fpm_optimizer_step(fpm_context *ctx, const fpm_optimizer *opt, float *param,
+                              const float *grad, size_t n, int32_t memory) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (!opt || !param || !grad || n == 0)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "opt/param/grad NULL or n == 0");
+    if (memory != FPM_MEM_DEVICE && memory != FPM_MEM_HOST)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", memory);
+    const int kind = opt->kind;
+    if (kind < FPM_OPT_RMSPROP || kind > FPM_OPT_SGD)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "optimizer kind = %d", kind);
+    if (!std::isfinite(opt->lr) || !std::isfinite(opt->beta1) || !std::isfinite(opt->beta2) ||
+        !std::isfinite(opt->momentum) || !std::isfinite(opt->clamp_margin))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "non-finite hyper-parameter");
+    const bool rms = kind == FPM_OPT_RMSPROP, moments = kind == FPM_OPT_ADAM || kind == FPM_OPT_YOGI;
+    const bool use_g0 = rms && opt->centered, use_buf = rms && opt->momentum > 0;
+    if (moments && (!opt->mom1 || !opt->mom2))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "Adam / Yogi need mom1 and mom2");
+    if (use_g0 && !opt->mom1)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "centered RMSprop needs mom1 (g0)");
+    if (use_buf && !opt->buffer)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "RMSprop with momentum needs buffer");
+    if (kind == FPM_OPT_ADAM && opt->iter < 1)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "Adam needs iter >= 1");
+    FPM_CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const bool dev = memory == FPM_MEM_DEVICE;
+    // (pointer, bytes, written back) of every array the step touches
+    struct Arr {
+        const void *p;
+        size_t bytes;
+        bool out;
+    } arrs[6] = {{param, n * 8, true},
+                 {grad, n * 8, false},
+                 {(moments || use_g0) ? opt->mom1 : nullptr, n * 8, true},
+                 {moments ? opt->mom2 : nullptr, n * 4, true},
+                 {use_buf ? opt->buffer : nullptr, n * 8, true},
+                 {opt->clamp_amp, n * 4, false}};
+    for (const Arr &a : arrs) {
+        if (!a.p) continue;
+        if (dev && !is_device_ptr(a.p, ctx->device))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not device memory");
+        if (dev && (reinterpret_cast<uintptr_t>(a.p) & 7))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "device pointers must be 8-byte aligned");
+        if (!dev && !is_host_ptr(a.p))
+            return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pointers are not host memory");
+    }
+    if (dev) {
+        const fpm_status rc = order_after_default_stream(ctx);
+        if (rc != FPM_OK) return rc;
+    }
+    void *d[6] = {};
+    for (int k = 0; k < 6; ++k) {
+        if (!arrs[k].p) continue;
+        if (dev) {
+            d[k] = const_cast<void *>(arrs[k].p);
+        } else {
+            FPM_CK(ctx->opt[k].ensure(arrs[k].bytes));
+            FPM_CK(cudaMemcpyAsync(ctx->opt[k].p, arrs[k].p, arrs[k].bytes, cudaMemcpyHostToDevice,
+                                   st));
+            d[k] = ctx->opt[k].p;
+        }
+    }
+    OptStep o;
+    o.kind = kind;
+    o.n = n;
+    o.p = static_cast<float2 *>(d[0]);
+    o.g = static_cast<const float2 *>(d[1]);
+    o.mom1 = static_cast<float2 *>(d[2]);
+    o.mom2 = static_cast<float *>(d[3]);
+    o.buffer = static_cast<float2 *>(d[4]);
+    o.amp = static_cast<const float *>(d[5]);
+    o.r1 = (float)opt->beta1;
+    o.c1 = (float)(1.0 - opt->beta1);
+    o.r2 = (float)opt->beta2;
+    o.c2 = (float)(1.0 - opt->beta2);
+    o.lr = (float)opt->lr;
+    o.mum = (float)opt->momentum;
+    o.margin = (float)opt->clamp_margin;
+    if (kind == FPM_OPT_ADAM) {
+        const double t = (double)opt->iter;
+        o.bias = (float)(std::sqrt(1.0 - std::pow(opt->beta2, t)) / (1.0 - std::pow(opt->beta1, t)));
+    }
+    FPM_CK(launch_optimizer_step(o, st));
+    if (!dev)
+        for (int k = 0; k < 6; ++k)
+            if (arrs[k].p && arrs[k].out)
+                FPM_CK(cudaMemcpyAsync(const_cast<void *>(arrs[k].p), d[k], arrs[k].bytes,
+                                       cudaMemcpyDeviceToHost, st));
+    FPM_CK(cudaStreamSynchronize(st));
     return FPM_OK;
 }
 

@@ -24,7 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(INCLUDE),
                   "--expt-relaxed-constexpr"]
 LIBS_SOURCES = ["kernels_lowres.cu", "kernels_update.cu", "fft_own.cu", "fpm_api.cpp",
-                "noalloc.cu", "pipeline.cu", "geometry.cu", "tiff.cpp"]
+                "noalloc.cu", "pipeline.cu", "geometry.cu", "tiff.cpp",
+                "optimizers.cu"]
 LINK_LIBS = ["-lcudart", "-lpthread"]
 
 

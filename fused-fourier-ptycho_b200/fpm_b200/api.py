@@ -39,11 +39,13 @@ _LOSS = {"anisotropic": LOSS_ANISOTROPIC, "isotropic": LOSS_ISOTROPIC}
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
             "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
-            "fpm_led_indices", "fpm_simulate", "fpm_normalise_stack_f32", "fpm_read_tiff_stack"]
+            "fpm_led_indices", "fpm_simulate", "fpm_normalise_stack_f32", "fpm_read_tiff_stack",
+            "fpm_optimizer_step"]
 
 
 SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
 INGEST_U16, INGEST_F32_MEAN = 0, 1
+OPT_RMSPROP, OPT_ADAM, OPT_YOGI, OPT_SGD = 0, 1, 2, 3
 
 
 class FpmError(RuntimeError):
@@ -65,6 +67,14 @@ class LedGeometry(C.Structure):
                 ("led_pitch_um", C.c_double), ("led_height_um", C.c_double),
                 ("camera_pixel_um", C.c_double), ("magnification", C.c_double),
                 ("sample_dx_um", C.c_double), ("sample_dy_um", C.c_double)]
+
+
+class Optimizer(C.Structure):
+    """fpm_optimizer (include/fpm.h)."""
+    _fields_ = [("kind", C.c_int32), ("centered", C.c_int32), ("lr", C.c_double),
+                ("beta1", C.c_double), ("beta2", C.c_double), ("momentum", C.c_double),
+                ("iter", C.c_int64), ("mom1", C.c_void_p), ("mom2", C.c_void_p),
+                ("buffer", C.c_void_p), ("clamp_amp", C.c_void_p), ("clamp_margin", C.c_double)]
 
 
 class Problem(C.Structure):
@@ -133,6 +143,9 @@ def load_library(path: str | Path | None = None):
     lib.fpm_read_tiff_stack.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int32, C.c_int32,
                                         C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
     lib.fpm_read_tiff_stack.restype = C.c_int
+    lib.fpm_optimizer_step.argtypes = [C.c_void_p, C.POINTER(Optimizer), C.c_void_p, C.c_void_p,
+                                       C.c_size_t, C.c_int32]
+    lib.fpm_optimizer_step.restype = C.c_int
     lib.fpm_abi_version.argtypes = []
     lib.fpm_abi_version.restype = C.c_int32
     if path is None:
@@ -391,6 +404,18 @@ class Engine:
         out = np.empty(x.shape, np.float32)
         self._check(fn(self._ctx, x.ctypes.data, x.size, out.ctypes.data, MEM_HOST))
         return out
+
+    def optimizer_step(self, opt: Optimizer, param, grad):
+        """One fpm_optimizer_step: param (complex64) updated in place; grad, the states
+        named in opt and its clamp amplitude in the same memory (numpy arrays in host
+        memory or torch tensors on the context's device, any contiguous layout with the
+        same element order)."""
+        if _is_torch(param):
+            _inputs_ready(param, grad)
+            ptr_p, ptr_g, n, mem = param.data_ptr(), grad.data_ptr(), param.numel(), MEM_DEVICE
+        else:
+            ptr_p, ptr_g, n, mem = param.ctypes.data, grad.ctypes.data, param.size, MEM_HOST
+        self._check(self.lib.fpm_optimizer_step(self._ctx, C.byref(opt), ptr_p, ptr_g, n, mem))
 
     def read_stack(self, paths, h, row0=0, col0=0, dtype="u16", threads=0):
         """read_tiff_stack, failures reported on this context."""

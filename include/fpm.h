@@ -249,6 +249,55 @@ fpm_status fpm_simulate(fpm_context *ctx, const float *object, const float *pupi
                         const int32_t *led_idx, int32_t h, int32_t pratio, int32_t n_leds,
                         int32_t output, float *out, int32_t memory);
 
+/* The optimiser classes of the reference's script-level loop, which pairs
+   fullyfusedFPM (fpm_batch_gradients here) with a MATLAB optimiser step and a pupil
+   amplitude clamp per mini-batch (benchmark/cuFPM_recon_2025_circular.m:108-113,
+   180-186; codes/main_run_FPM.m:85-86).  One step is one fused elementwise pass on
+   the device over a complex parameter of n elements, single precision as MATLAB's
+   gpuArray single, every scalar (lr, betas, Adam's bias) rounded from double. */
+typedef enum fpm_optimizer_kind {
+    /* optimizer_RMSprop.m:30-47 as written: squave = r1 + (1-r1)|g|^2 (recomputed
+       every step, no running average), centered: g0 = r1 g0 + (1-r1) g and
+       squave -= |g0|^2, then with momentum mum > 0: buffer = mum buffer +
+       g/(sqrt(squave)+1e-5), p -= lr buffer; else p -= lr g/(sqrt(squave)+1e-5).
+       A negative squave takes MATLAB's complex square root. */
+    FPM_OPT_RMSPROP = 0,
+    /* codes/func_ware/optimizers/optimizer_adam.m:25-38: mom1 = r1 mom1 + (1-r1) g,
+       mom2 = r2 mom2 + (1-r2)|g|^2, p -= lr sqrt(1-r2^t)/(1-r1^t) mom1/(sqrt(mom2)+1e-5) */
+    FPM_OPT_ADAM = 1,
+    /* codes_v2/func_ware/optimizers/optimizer_yogi.m:25-36: mom1 as Adam,
+       mom2 -= (1-r2) sign(mom2 - |g|^2)|g|^2 (sign(0) = 0), p -= lr mom1/(sqrt(mom2)+1e-5) */
+    FPM_OPT_YOGI = 2,
+    /* optimizer_sgd.m: p -= lr g (the class's step names an undefined variable
+       `update`, so MATLAB cannot run it; this is its evident intent) */
+    FPM_OPT_SGD = 3
+} fpm_optimizer_kind;
+
+typedef struct fpm_optimizer {
+    int32_t kind;          /* fpm_optimizer_kind */
+    int32_t centered;      /* RMSprop: 1 = centred */
+    double lr;
+    double beta1;          /* r1 (RMSprop, Adam, Yogi) */
+    double beta2;          /* r2 (Adam, Yogi) */
+    double momentum;       /* RMSprop mum; > 0 uses `buffer` */
+    int64_t iter;          /* Adam: step count t >= 1 of the bias correction */
+    /* state, updated in place; NULL where the kind does not use it.  MATLAB starts
+       every state at 0 (the classes are built with zeros): pass zeroed arrays. */
+    float *mom1;           /* complex n: Adam / Yogi first moment; RMSprop g0 (centered) */
+    float *mom2;           /* real n: Adam / Yogi second moment */
+    float *buffer;         /* complex n: RMSprop momentum buffer (momentum > 0) */
+    /* optional pupil clamp after the step (cuFPM_recon_2025_circular.m:183-186):
+       p = max(min(|p|, a + margin), a - margin) .* sign(p) .* a, sign(p) = p/|p|
+       (0 at 0); a: real n, NULL = no clamp */
+    const float *clamp_amp;
+    double clamp_margin;
+} fpm_optimizer;
+
+/* param (complex n) -= the step of opt for gradient grad (complex n).  Pointers
+   (param, grad, states, clamp_amp) follow `memory`; device pointers 8-byte aligned. */
+fpm_status fpm_optimizer_step(fpm_context *ctx, const fpm_optimizer *opt, float *param,
+                              const float *grad, size_t n, int32_t memory);
+
 void fpm_destroy(fpm_context *ctx);
 
 /* Per-stage device timing (no counterpart in the reference, which only times

@@ -371,6 +371,137 @@ def read_frame(path, row0: int, col0: int, h: int):
     return a
 
 
+# ---------------------------------------------------------------------------
+# the MATLAB optimiser classes of the script-level loop (single precision, one
+# rounding per MATLAB operation, double scalars rounded to single first)
+# ---------------------------------------------------------------------------
+
+def abs32(z):
+    """MATLAB ``abs`` of a complex single: hypot, correctly rounded (formed in double)."""
+    z = np.asarray(z, np.complex64)
+    re = z.real.astype(np.float64)
+    im = z.imag.astype(np.float64)
+    return np.sqrt(re * re + im * im).astype(np.float32)
+
+
+def _split(z):
+    z = np.asarray(z, np.complex64)
+    return z.real.astype(np.float32), z.imag.astype(np.float32)
+
+
+def _join(re, im):
+    out = np.empty(re.shape, np.complex64)
+    out.real = re
+    out.imag = im
+    return out
+
+
+def _f(x):
+    return np.float32(x)
+
+
+def _div_root(g, sq):
+    """g ./ (sqrt(sq) + 1e-5) with MATLAB's complex square root where sq < 0."""
+    gr, gi = _split(g)
+    sq = np.asarray(sq, np.float32)
+    neg = sq < 0
+    with np.errstate(invalid="ignore"):
+        d = np.sqrt(np.where(neg, _f(0), sq)) + _f(1e-5)
+    outr, outi = gr / d, gi / d
+    if neg.any():
+        dr = _f(1e-5)
+        di = np.sqrt(-sq[neg])
+        den = dr * dr + di * di
+        outr[neg] = (gr[neg] * dr + gi[neg] * di) / den
+        outi[neg] = (gi[neg] * dr - gr[neg] * di) / den
+    return _join(outr, outi)
+
+
+def rmsprop_class_step(p, g, r1, mum, centered, lr, g0=None, buffer=None):
+    """``optimizer_RMSprop.step`` (codes_v2/func_ware/optimizers/optimizer_RMSprop.m:30-47),
+    statement by statement as written: ``squave = r1 + (1 - r1) .* abs(grad).^2`` (no running
+    average), centred ``g0 = r1 .* g0 + (1 - r1) .* grad; squave = squave - abs(g0).^2``,
+    momentum ``buffer = mum .* buffer + grad ./ (sqrt(squave) + 1e-5); p = p - lr .* buffer``,
+    else ``p - lr .* (grad ./ (sqrt(squave) + 1e-5))``.  Returns (p, g0, buffer)."""
+    a = abs32(g)
+    sq = _f(r1) + _f(1.0 - r1) * (a * a)
+    if centered:
+        g0r, g0i = _split(g0)
+        gr, gi = _split(g)
+        g0 = _join(_f(r1) * g0r + _f(1.0 - r1) * gr, _f(r1) * g0i + _f(1.0 - r1) * gi)
+        b = abs32(g0)
+        sq = sq - b * b
+    u = _div_root(g, sq)
+    pr, pi = _split(p)
+    if mum > 0:
+        br, bi = _split(buffer)
+        ur, ui = _split(u)
+        buffer = _join(_f(mum) * br + ur, _f(mum) * bi + ui)
+        br, bi = _split(buffer)
+        p = _join(pr - _f(lr) * br, pi - _f(lr) * bi)
+    else:
+        ur, ui = _split(u)
+        p = _join(pr - _f(lr) * ur, pi - _f(lr) * ui)
+    return p, g0, buffer
+
+
+def _first_moment(mom1, g, r1):
+    mr, mi = _split(mom1)
+    gr, gi = _split(g)
+    return _join(_f(r1) * mr + _f(1.0 - r1) * gr, _f(r1) * mi + _f(1.0 - r1) * gi)
+
+
+def adam_class_step(p, g, mom1, mom2, r1, r2, lr, it):
+    """``optimizer_adam.step`` (codes/func_ware/optimizers/optimizer_adam.m:25-38); ``bias``
+    in double as MATLAB forms it from double scalars.  Returns (p, mom1, mom2)."""
+    a = abs32(g)
+    mom1 = _first_moment(mom1, g, r1)
+    mom2 = _f(r2) * np.asarray(mom2, np.float32) + _f(1.0 - r2) * (a * a)
+    bias = _f(np.sqrt(1.0 - r2 ** float(it)) / (1.0 - r1 ** float(it)))
+    mr, mi = _split(mom1)
+    d = np.sqrt(mom2) + _f(1e-5)
+    pr, pi = _split(p)
+    p = _join(pr - _f(lr) * ((bias * mr) / d), pi - _f(lr) * ((bias * mi) / d))
+    return p, mom1, mom2
+
+
+def yogi_class_step(p, g, mom1, mom2, r1, r2, lr):
+    """``optimizer_yogi.step`` (codes_v2/func_ware/optimizers/optimizer_yogi.m:25-36); MATLAB
+    ``sign`` (0 at 0).  Returns (p, mom1, mom2)."""
+    a = abs32(g)
+    g2 = a * a
+    mom1 = _first_moment(mom1, g, r1)
+    mom2 = np.asarray(mom2, np.float32)
+    mom2 = mom2 - (_f(1.0 - r2) * np.sign(mom2 - g2).astype(np.float32)) * g2
+    mr, mi = _split(mom1)
+    d = np.sqrt(mom2) + _f(1e-5)
+    pr, pi = _split(p)
+    p = _join(pr - _f(lr) * (mr / d), pi - _f(lr) * (mi / d))
+    return p, mom1, mom2
+
+
+def sgd_step(p, g, lr):
+    """``optimizer_sgd`` (codes/func_ware/optimizers/optimizer_sgd.m:17-22) as intended:
+    ``p - lr .* grad`` (the class's statement names an undefined ``update``)."""
+    pr, pi = _split(p)
+    gr, gi = _split(g)
+    return _join(pr - _f(lr) * gr, pi - _f(lr) * gi)
+
+
+def clamp_pupil_script(p, amp, ac):
+    """``max(min(abs(w2), Pupil0 + ac), Pupil0 - ac) .* sign(w2) .* Pupil0``
+    (benchmark/cuFPM_recon_2025_circular.m:183-186); sign(z) = z ./ abs(z), 0 at 0."""
+    amp = np.asarray(amp, np.float32)
+    w = abs32(p)
+    t = np.maximum(np.minimum(w, amp + _f(ac)), amp - _f(ac))
+    pr, pi = _split(p)
+    nz = w > 0
+    with np.errstate(invalid="ignore", divide="ignore"):
+        sr = np.where(nz, pr / w, _f(0))
+        si = np.where(nz, pi / w, _f(0))
+    return _join(np.where(nz, (t * sr) * amp, _f(0)), np.where(nz, (t * si) * amp, _f(0)))
+
+
 def _cubic(x, a=-0.5):
     ax = np.abs(x)
     ax2 = ax * ax

@@ -49,9 +49,10 @@ PROBE = r"""
 #include "fpm.h"
 #define F(T, f) printf(#T "." #f " %zu\n", offsetof(T, f));
 int main(void) {
-  printf("fpm_problem %zu\nfpm_result %zu\nfpm_device_opts %zu\nfpm_led_geometry %zu\n",
+  printf("fpm_problem %zu\nfpm_result %zu\nfpm_device_opts %zu\nfpm_led_geometry %zu\n"
+         "fpm_optimizer %zu\n",
          sizeof(fpm_problem), sizeof(fpm_result), sizeof(fpm_device_opts),
-         sizeof(fpm_led_geometry));
+         sizeof(fpm_led_geometry), sizeof(fpm_optimizer));
   F(fpm_problem, h) F(fpm_problem, n_leds) F(fpm_problem, pratio) F(fpm_problem, batch)
   F(fpm_problem, epochs) F(fpm_problem, lr) F(fpm_problem, beta) F(fpm_problem, eps)
   F(fpm_problem, pupil_margin) F(fpm_problem, lr_halve_after) F(fpm_problem, lr_decay)
@@ -65,6 +66,10 @@ int main(void) {
   F(fpm_led_geometry, led_height_um) F(fpm_led_geometry, camera_pixel_um)
   F(fpm_led_geometry, magnification) F(fpm_led_geometry, sample_dx_um)
   F(fpm_led_geometry, sample_dy_um)
+  F(fpm_optimizer, kind) F(fpm_optimizer, centered) F(fpm_optimizer, lr) F(fpm_optimizer, beta1)
+  F(fpm_optimizer, beta2) F(fpm_optimizer, momentum) F(fpm_optimizer, iter) F(fpm_optimizer, mom1)
+  F(fpm_optimizer, mom2) F(fpm_optimizer, buffer) F(fpm_optimizer, clamp_amp)
+  F(fpm_optimizer, clamp_margin)
   return 0;
 }
 """
@@ -82,8 +87,10 @@ def test_struct_layout_matches_c(tmp_path):
     assert int(got["fpm_result"]) == C.sizeof(api.Result)
     assert int(got["fpm_device_opts"]) == C.sizeof(api.DeviceOpts)
     assert int(got["fpm_led_geometry"]) == C.sizeof(api.LedGeometry)
+    assert int(got["fpm_optimizer"]) == C.sizeof(api.Optimizer)
     for cname, cls in (("fpm_problem", api.Problem), ("fpm_result", api.Result),
-                       ("fpm_device_opts", api.DeviceOpts), ("fpm_led_geometry", api.LedGeometry)):
+                       ("fpm_device_opts", api.DeviceOpts), ("fpm_led_geometry", api.LedGeometry),
+                       ("fpm_optimizer", api.Optimizer)):
         for fname, _ in cls._fields_:
             key = f"{cname}.{fname}"
             if key in got:
