@@ -271,3 +271,30 @@ def test_normalise_f32_on_device_bit_exact(engine, tmp_path):
     got = engine.normalise_stack(np.ascontiguousarray(Xn))
     np.testing.assert_array_equal(got, orc.normalise_stack_f32(Xn))
     np.testing.assert_array_equal(engine.normalise_stack(np.full((8, 8, 2), 7, np.float32)), 0)
+
+
+@pytest.mark.parametrize("shape,dtype", [((70, 50), np.uint16), ((33, 1000), np.uint16),
+                                         ((16, 16), np.uint8)])
+def test_package_writer_round_trips(lib, tmp_path, shape, dtype):
+    """fpm_b200.frames writes what both libfpm's reader and Pillow read back."""
+    from fpm_b200 import frames
+    a = rng_frames(13, 1, *shape, dtype=dtype)[0]
+    p = tmp_path / "w.tif"
+    frames.write_tiff(p, a)
+    np.testing.assert_array_equal(orc.read_frame(p, 0, 0, min(shape)), a[:min(shape), :min(shape)])
+    h = min(shape)
+    np.testing.assert_array_equal(lib.read_tiff_stack([p], h)[:, :, 0], a[:h, :h])
+
+
+def test_frame_names_and_uint16_conversion(tmp_path):
+    from fpm_b200 import frames
+    # spiral order of a 3 x 3 grid starts at the centre cell (2, 2): k = 2 + 1*3 = 5
+    ij = np.array([[2, 2], [2, 3], [1, 3]])
+    assert list(frames.frame_numbers(ij, 3)) == [5, 6, 3]
+    assert [p.name for p in frames.frame_paths(tmp_path, ij, 3)] == ["005.tif", "006.tif", "003.tif"]
+    x = np.array([[0.0, 0.5], [1.0, 2.0]])
+    u = frames.to_uint16_frames(x)
+    # (2^16-1) * [0, .25, .5, 1] rounded half away from zero: 16383.75 -> 16384, 32767.5 -> 32768
+    np.testing.assert_array_equal(u, [[0, 16384], [32768, 65535]])
+    paths = frames.write_frames(tmp_path / "d", np.stack([u, u[::-1]], axis=2))
+    assert [p.name for p in paths] == ["img1.tif", "img2.tif"]
