@@ -506,136 +506,6 @@ __global__ void __launch_bounds__(1024, 1)
 }
 
 // ---------------------------------------------------------------------------
-// L2 + L3 fused, small-CTA form: 512 threads (LIN = 512 / (N/16) lines), two CTAs per
-// SM so that one CTA's loads overlap the other's transforms.  The lines come straight
-// from global memory (a warp reads LIN consecutive rows of 32 / LIN columns: whole
-// 32-byte sectors), no tile is staged, and the residual rows live in the FFT exchange
-// area between the two transforms.  The partner CTA reads this CTA's boundary residual
-// rows, so the forward FFT (which reuses that area) starts only after the second
-// cluster barrier.
-// ---------------------------------------------------------------------------
-template <int N, int CL = 2>
-struct L23S {
-    static constexpr int THREADS = 512;
-    static constexpr int T = N / 16;
-    static constexpr int LIN = THREADS / T;            // lines per CTA
-    static constexpr int POUT = CL * LIN - 2;          // central lines per cluster
-    static constexpr int PAD = 16 / LIN > 0 ? 16 / LIN : 1;
-    static constexpr int STRIDE = N + PAD;             // FFT exchange line stride (float2)
-    // residual line stride (float): a warp's (line, t) pairs on distinct banks
-    static constexpr int RSTRIDE = N + (LIN >= 32 ? 1 : 32 / LIN);
-    static constexpr int LINE_BYTES = LIN * STRIDE * 8;
-    static constexpr int RES_BYTES = (LIN + 2) * RSTRIDE * 4;
-    static constexpr int SMEM = LINE_BYTES + 2 * 128 * 8;
-    static constexpr int PAIRS_PER_LED = (N + POUT - 1) / POUT;
-    static constexpr int CTAS_PER_LED = CL * PAIRS_PER_LED;
-    static constexpr int NHI = N / 128;
-    static_assert(N >= 1024 && N <= 2048, "small-CTA row pass: h of 1024 or 2048");
-    static_assert(RES_BYTES <= LINE_BYTES, "residual rows fit the exchange area");
-    static_assert(2 * (SMEM + 1024) <= 228 * 1024, "two CTAs per SM");
-};
-
-template <int N, int TYPE, int LOSS, int CL>
-__global__ void __launch_bounds__(512, 2)
-    k_lr_rows_fused_s(StackView Y, BatchGeom g, int l0, const float2 *__restrict__ T1,
-                      float2 *__restrict__ T2, double *__restrict__ parts,
-                      const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
-    using F = L23S<N, CL>;
-    constexpr int T = F::T;
-    extern __shared__ __align__(128) float2 smem[];
-    __shared__ double s_red[F::THREADS / 32];
-    float *res = reinterpret_cast<float *>(smem);      // between the two transforms
-    float2 *s_hi = smem + F::LIN * F::STRIDE;
-    const int k = threadIdx.x % F::LIN, t = threadIdx.x / F::LIN;
-    const unsigned j = blockIdx.x % CL;                 // rank in the cluster
-    const int pair = blockIdx.x / CL;
-    const int lloc = pair / F::PAIRS_PER_LED;
-    const int r0 = (pair % F::PAIRS_PER_LED) * F::POUT + (int)j * F::LIN;   // rows r0-1+k
-    const int zpage = g.z_off + l0 + lloc;
-    const int rraw = r0 - 1 + k;
-    const int r = rraw < 0 ? rraw + N : (rraw >= N ? rraw - N : rraw);
-    const int q = (int)j * F::LIN + k;                  // line within the cluster
-    const bool central = q >= 1 && q <= F::POUT && rraw < N;
-    float2 v[16];
-    {
-        const float2 *page = T1 + (size_t)lloc * N * N + r;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) v[m] = page[(size_t)(t + m * T) * N];
-    }
-    fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, F::NHI, 128);
-    __syncthreads();
-    fft::line_fft_regs<N, +1>(v, smem + k * F::STRIDE, s_hi, s_hi + 128, t);
-    float mn = 0.f, range = 0.f;
-    if (TYPE == kStackU16) {
-        mn = (float)Y.minmax[0];
-        range = (float)(Y.minmax[1] - Y.minmax[0]);
-    }
-    const float ratio = (float)((double)N * N * g.pratio * g.pratio);
-    const size_t ypage = (size_t)zpage * N * N + r;
-    float *rk = res + (k + 1) * F::RSTRIDE;
-    __syncthreads();                                    // last exchange reads done: area -> residuals
-#pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const float2 z = v[m];
-        rk[t + m * T] = sqrtf(z.x * z.x + z.y * z.y) / ratio -
-                        amplitude<TYPE>(Y, ypage + (size_t)(t + m * T) * N, mn, range);
-    }
-    __syncthreads();
-    cluster_arrive();
-    cluster_wait();
-    // ghost above: the last line of rank j-1; ghost below: the first line of rank j+1
-    for (int c = threadIdx.x; c < N; c += F::THREADS) {
-        if (j > 0) res[c] = cluster_load(res + F::LIN * F::RSTRIDE + c, j - 1);
-        if (j + 1 < CL) res[(F::LIN + 1) * F::RSTRIDE + c] = cluster_load(res + F::RSTRIDE + c, j + 1);
-    }
-    __syncthreads();
-    cluster_arrive();                                   // done with the partner's rows
-    double lsum = 0.0;
-    const float gscale = (float)(g.pratio * g.pratio);
-#pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const int c = t + m * T;
-        float2 o = make_float2(0.f, 0.f);
-        if (central) {
-            const int cp = c + 1 == N ? 0 : c + 1, cm = c == 0 ? N - 1 : c - 1;
-            const float d =
-                stencil<LOSS>(rk[c], rk[cp], rk[cm], rk[F::RSTRIDE + c], rk[c - F::RSTRIDE],
-                              LOSS == kLossAnisotropic ? 0.f : rk[F::RSTRIDE + cm],
-                              LOSS == kLossAnisotropic ? 0.f : rk[cp - F::RSTRIDE], lsum) *
-                gscale;
-            const float2 z = v[m];
-            const float mag = sqrtf(z.x * z.x + z.y * z.y);
-            if (mag > 0.f) {
-                const float inv = 1.0f / mag;
-                o.x = z.x * inv * d;
-                o.y = z.y * inv * d;
-            }
-        }
-        v[m] = o;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = lsum;
-    cluster_wait();                                     // the partner has read our rows
-    __syncthreads();                                    // every stencil read of ours is done
-    if (threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int w = 0; w < F::THREADS / 32; ++w) tot += s_red[w];
-        parts[blockIdx.x] = tot;
-    }
-    fft::line_fft_regs<N, -1>(v, smem + k * F::STRIDE, s_hi, s_hi + 128, t);
-    if (central) {   // only the columns the next pass transforms (pupil support, fftshifted)
-        float2 *dst = T2 + (size_t)lloc * N * N + r;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const int cf = t + m * T;
-            const int c = cf + N / 2 >= N ? cf - N / 2 : cf + N / 2;
-            if (c >= g.pc_lo && c < g.pc_hi) dst[(size_t)cf * N] = v[m];
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // L4: forward FFT along r (column lines, interleaved so the row-major store of
 // the fftshift'ed Xs writes LPC consecutive columns per row)
 // ---------------------------------------------------------------------------
@@ -718,7 +588,7 @@ __global__ void __launch_bounds__(256) k_lr_pupil_grad(const float2 *__restrict_
 // ---------------------------------------------------------------------------
 // Pass A: stitch the box rows of the gradient spectrum, inverse FFT along the row
 // ---------------------------------------------------------------------------
-template <int N, int E>
+template <int N, int E, bool OWNED>
 __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     k_big_rows_inv(BatchGeom g, const int2 *__restrict__ led, const float2 *__restrict__ Pt,
                    const float2 *__restrict__ Xs, float2 *__restrict__ Ur,
@@ -733,6 +603,55 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     const bool live = i < g.rspan;
     const int h = g.h;
     float2 v[E];
+    if constexpr (OWNED) {
+        // Per covering LED, only its supported crop columns: they land on the contiguous
+        // (mod N) line positions e = pc_lo + ab.y + Cu0 + idx.  Thread t owns the positions
+        // e = t (mod T), accumulated in LED order in this line's exchange area, so no two
+        // threads touch one position and no barrier is needed until the transform.
+        float2 *acc = smem + ln * G::STRIDE;
+#pragma unroll
+        for (int m = 0; m < E; ++m) acc[t + m * G::T] = make_float2(0.f, 0.f);
+        const int W = g.pc_hi - g.pc_lo;
+        for (int l = 0; live && l < g.nb; ++l) {
+            const int2 ab = s_ab[l];
+            int rr = i - ab.x;
+            if (rr < 0) rr += N;
+            if (rr < g.pr_lo || rr >= g.pr_hi) continue;   // pupil zero on that crop row
+            const float2 *xrow = Xs + ((size_t)l * h + rr) * h + g.pc_lo;
+            const float2 *prow = Pt + (size_t)rr * h + g.pc_lo;
+            const int es = (int)(((long long)g.pc_lo + ab.y + g.Cu0) % N);   // position of idx 0
+            // four positions in flight per pass: their loads issue together
+            for (int base = (t - es) & (G::T - 1); base < W; base += 4 * G::T) {
+                float2 x[4], pp[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int idx = base + u * G::T;
+                    x[u] = idx < W ? xrow[idx] : make_float2(0.f, 0.f);
+                    pp[u] = idx < W ? prow[idx] : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int idx = base + u * G::T;
+                    if (idx < W) {
+                        int e = es + idx;
+                        if (e >= N) e -= N;
+                        int j = e - g.Cu0;                  // box column
+                        if (j < 0) j += N;
+                        if (j < g.cspan) {
+                            const float2 pr = cmul(x[u], pp[u]);
+                            float2 a = acc[e];
+                            a.x += pr.x;
+                            a.y += pr.y;
+                            acc[e] = a;
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = acc[t + m * G::T];
+        __syncthreads();                        // every accumulator read before the exchanges
+    } else {
     // four elements per LED sweep: four independent gathers in flight per thread
 #pragma unroll
     for (int m0 = 0; m0 < E; m0 += 4) {
@@ -772,6 +691,7 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) v[m0 + k] = acc[k].s;
+    }
     }
     line_fft_e<N, +1, E>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
     if (live) {
@@ -1136,11 +1056,9 @@ bool lr_rows_fused_supported(int h) { return h >= 128 && h <= 2048 && (h & (h - 
 
 static int fused_cluster();
 
-static bool fused_small(int h);
-
-static int ctas_per_led_fused(int h) {   // L23<h, CL>::CTAS_PER_LED, or L23S<h, 2>'s
-    const int cl = fused_small(h) ? 2 : fused_cluster();
-    const int pout = cl * ((fused_small(h) ? 512 : 1024) / (h / 16)) - 2;
+static int ctas_per_led_fused(int h) {   // L23<h, CL>::CTAS_PER_LED
+    const int cl = fused_cluster();
+    const int pout = cl * (1024 / (h / 16)) - 2;
     return cl * ((h + pout - 1) / pout);
 }
 
@@ -1217,53 +1135,6 @@ static int fused_cluster() {
     return e && std::atoi(e) == 4 ? 4 : 2;
 }
 
-// small-CTA form of the fused row pass (h of 1024 or 2048): FPM_L23_SMALL=1
-static bool fused_small(int h) {
-    if (h != 1024 && h != 2048) return false;
-    const char *e = std::getenv("FPM_L23_SMALL");
-    return e && std::atoi(e) != 0;
-}
-
-template <int N, int TYPE, int LOSS>
-static cudaError_t launch_fused_s(int nl, StackView Y, const BatchGeom &g, int l0,
-                                  const BatchBufs &b, int part_off, const Twiddles &tw,
-                                  cudaStream_t st) {
-    if constexpr (N == 1024 || N == 2048) {
-        using F = L23S<N, 2>;
-        auto kern = k_lr_rows_fused_s<N, TYPE, LOSS, 2>;
-        cudaError_t e = set_smem(kern, F::SMEM);
-        if (e != cudaSuccess) return e;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(nl * F::CTAS_PER_LED));
-        cfg.blockDim = dim3(F::THREADS);
-        cfg.dynamicSmemBytes = F::SMEM;
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = 2;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, kern, Y, g, l0, (const float2 *)b.T1, b.T2,
-                                  b.parts + part_off, tw.lo_hi, tw.lo_lo);
-    } else {
-        return cudaErrorInvalidValue;
-    }
-}
-
-template <int N>
-static cudaError_t launch_fused_small(int nl, StackView Y, const BatchGeom &g, int l0,
-                                      const BatchBufs &b, int part_off, const Twiddles &tw,
-                                      cudaStream_t st) {
-    const bool iso = g.loss == kLossIsotropic;
-    if (Y.type == kStackU16)
-        return iso ? launch_fused_s<N, kStackU16, kLossIsotropic>(nl, Y, g, l0, b, part_off, tw, st)
-                   : launch_fused_s<N, kStackU16, kLossAnisotropic>(nl, Y, g, l0, b, part_off, tw, st);
-    return iso ? launch_fused_s<N, kStackF32, kLossIsotropic>(nl, Y, g, l0, b, part_off, tw, st)
-               : launch_fused_s<N, kStackF32, kLossAnisotropic>(nl, Y, g, l0, b, part_off, tw, st);
-}
-
 template <int N, int TYPE, int LOSS>
 static cudaError_t launch_fused_k(int nl, StackView Y, const BatchGeom &g, int l0,
                                   const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
@@ -1278,9 +1149,6 @@ cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_page
                                  cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     CUtensorMap tm_field{}, tm_stack{};
-    if (fused_small(g.h))
-        return g.h == 2048 ? launch_fused_small<2048>(nl, Y, g, l0, b, part_off, tw, st)
-                           : launch_fused_small<1024>(nl, Y, g, l0, b, part_off, tw, st);
 #define F(N)                                                                              \
     static_assert(L23<N, 2>::CTAS_PER_LED ==                                              \
                       2 * ((N + 2 * (1024 / (N / 16)) - 3) / (2 * (1024 / (N / 16)) - 2)),     \
@@ -1331,6 +1199,13 @@ cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs 
     return cudaGetLastError();
 }
 
+// Pass A's stitch over each LED's supported columns only, each line position owned by
+// one thread (FPM_STITCH_OWNED=1); otherwise every position loops over every LED
+static bool stitch_owned() {
+    const char *e = std::getenv("FPM_STITCH_OWNED");
+    return e && std::atoi(e) != 0;
+}
+
 template <int N, int E>
 static cudaError_t launch_rows_inv_e(const BatchGeom &g, const int2 *led, const float2 *Pt,
                                      const float2 *Xs, float2 *Ur, const Twiddles &tw,
@@ -1338,9 +1213,10 @@ static cudaError_t launch_rows_inv_e(const BatchGeom &g, const int2 *led, const 
     using G = fft::LG<N, E>;
     const int smem = G::SMEM + g.nb * (int)sizeof(int2);
     const int blocks = (g.rspan + G::LPC - 1) / G::LPC;
-    cudaError_t e = set_smem(k_big_rows_inv<N, E>, smem);
+    auto kern = stitch_owned() ? k_big_rows_inv<N, E, true> : k_big_rows_inv<N, E, false>;
+    cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
-    k_big_rows_inv<N, E><<<blocks, G::THREADS, smem, st>>>(g, led, Pt, Xs, Ur, tw.hi_hi, tw.hi_lo);
+    kern<<<blocks, G::THREADS, smem, st>>>(g, led, Pt, Xs, Ur, tw.hi_hi, tw.hi_lo);
     return cudaGetLastError();
 }
 

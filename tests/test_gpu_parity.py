@@ -525,27 +525,3 @@ def test_16384_columns_32_values_per_thread_match_16(engine):
     for a, b in zip(runs["0"], runs["1"]):
         assert orc.rel_err(a, b) < 3e-5, orc.rel_err(a, b)
 
-
-@pytest.mark.parametrize("h,loss", [(1024, "anisotropic"), (2048, "anisotropic"), (2048, "isotropic")])
-def test_small_cta_row_pass_is_bit_identical(engine, h, loss, monkeypatch):
-    """The 512-thread form of the fused row pass (FPM_L23_SMALL=1: two CTAs per SM, lines
-    loaded straight from memory, residuals in the exchange area) computes every line as
-    the 1024-thread form does: identical object and pupil, the loss summed in another
-    grouping of the same per-CTA partials."""
-    from fpm_b200 import synth
-    rng = np.random.default_rng(h)
-    p = 2
-    H = h * p
-    P0 = synth.pupil_circle(h, synth.Optics(led_grid=5)).astype(np.float32)
-    O0 = (0.5 + 0.5 * rng.random((H, H)) * np.exp(1j * rng.random((H, H)))).astype(np.complex64)
-    led = np.array([[1, 1], [H - 10, 3], [H // 2 - h // 2, H // 2 - h // 2], [20, H - 20],
-                    [H // 3, H // 5], [7, H // 2]], np.int32)
-    Y = rng.integers(0, 65536, size=(len(led), h, h)).astype(np.uint16)
-    args = (O0, P0.astype(np.complex64), to_matlab_stack(Y), led_matlab(led), P0, p, 1, 4)
-    monkeypatch.delenv("FPM_L23_SMALL", raising=False)
-    ref = engine.solve(*args, lr=1e-3, beta=0.9, eps=1e-4, loss=loss)
-    monkeypatch.setenv("FPM_L23_SMALL", "1")
-    got = engine.solve(*args, lr=1e-3, beta=0.9, eps=1e-4, loss=loss)
-    np.testing.assert_array_equal(got["object"], ref["object"])
-    np.testing.assert_array_equal(got["pupil"], ref["pupil"])
-    np.testing.assert_allclose(got["loss"], ref["loss"], rtol=1e-12)
