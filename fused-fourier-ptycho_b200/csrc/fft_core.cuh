@@ -19,6 +19,8 @@
 // powers W^(r m) beyond r = 1, 2, 4, 8 are products of table values.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace fpm {
@@ -171,10 +173,16 @@ __device__ __forceinline__ void dft(float2 (&v)[R]) {
     }
 }
 
+// Position of table entry i in shared memory: within each block of 16 entries the low
+// three bits are XORed with the block number, so that the strided lookups of a stage
+// (index stride 1 .. 64 across a warp) fall on distinct banks instead of piling up on
+// one (stride 16: eight entries on one bank pair without it).
+__device__ __forceinline__ int twpos(int i) { return i ^ ((i >> 4) & 7); }
+
 // W_N^m with the sign of DIR, from the two-level forward table (hi, lo).
 template <int DIR>
 __device__ __forceinline__ float2 twiddle(const float2 *hi, const float2 *lo, int m) {
-    float2 w = cmulf(hi[m >> 7], lo[m & 127]);
+    float2 w = cmulf(hi[twpos(m >> 7)], lo[twpos(m & 127)]);
     if (DIR > 0) w.y = -w.y;
     return w;
 }
@@ -236,9 +244,16 @@ __device__ __forceinline__ void apply_twiddles(float2 (&u)[R], const float2 *hi,
 // from global memory (16 independent loads per thread) and store it back, or
 // hand it to the next computation without a shared-memory round trip.
 // ---------------------------------------------------------------------------
-template <int N, int DIR, int P, int E>
+// Called by stages_regs between the last stage's reads of the exchange area and its
+// arithmetic, after a block barrier: from then on the area is free (e.g. for a copy
+// into it that overlaps the last stage's butterflies).
+struct NoHook {
+    __device__ void operator()() const {}
+};
+
+template <int N, int DIR, int P, int E, typename Hook = NoHook>
 __device__ __forceinline__ void stages_regs(float2 (&v)[E], float2 *s, const float2 *hi,
-                                            const float2 *lo, int t) {
+                                            const float2 *lo, int t, const Hook &hook = Hook{}) {
     constexpr int REM = N / P;
     constexpr int R = REM >= E ? E : REM;
     constexpr int T = N / E;
@@ -252,6 +267,10 @@ __device__ __forceinline__ void stages_regs(float2 (&v)[E], float2 *s, const flo
             for (int r = 0; r < R; ++r) v[j + r * NB] = s[swz_e<E>(t + j * T + r * (N / R))];
     }
     if constexpr (!LAST) __syncthreads();   // every read of s done before it is rewritten
+    if constexpr (LAST && !FIRST && !std::is_same<Hook, NoHook>::value) {
+        __syncthreads();                    // every read of s done: the area is free
+        hook();
+    }
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
         float2 u[R];
@@ -272,7 +291,7 @@ __device__ __forceinline__ void stages_regs(float2 (&v)[E], float2 *s, const flo
     }
     if constexpr (!LAST) {
         __syncthreads();
-        stages_regs<N, DIR, P * R, E>(v, s, hi, lo, t);
+        stages_regs<N, DIR, P * R, E, Hook>(v, s, hi, lo, t, hook);
     }
 }
 
@@ -288,19 +307,19 @@ __device__ __forceinline__ void line_fft_regs(float2 (&v)[16], float2 *s, const 
 
 // The same with 32 values per thread (t + m N/32, m < 32): radix-32 stages, one
 // exchange fewer for N = 16384 (32 x 32 x 16) at N/32 threads per line.
-template <int N, int DIR>
+template <int N, int DIR, typename Hook = NoHook>
 __device__ __forceinline__ void line_fft_regs32(float2 (&v)[32], float2 *s, const float2 *hi,
-                                                const float2 *lo, int t) {
+                                                const float2 *lo, int t, const Hook &hook = Hook{}) {
     static_assert(N >= 1024 && (N & (N - 1)) == 0, "power-of-two length >= 1024");
-    stages_regs<N, DIR, 1, 32>(v, s, hi, lo, t);
+    stages_regs<N, DIR, 1, 32, Hook>(v, s, hi, lo, t, hook);
 }
 
 // Copies the two-level twiddle table of length N into shared memory.
 // hi needs max(1, N/128) entries, lo min(N, 128).
 __device__ __forceinline__ void load_twiddles(float2 *s_hi, float2 *s_lo, const float2 *g_hi,
                                               const float2 *g_lo, int n_hi, int n_lo) {
-    for (int i = threadIdx.x; i < n_hi; i += blockDim.x) s_hi[i] = g_hi[i];
-    for (int i = threadIdx.x; i < n_lo; i += blockDim.x) s_lo[i] = g_lo[i];
+    for (int i = threadIdx.x; i < n_hi; i += blockDim.x) s_hi[twpos(i)] = g_hi[i];
+    for (int i = threadIdx.x; i < n_lo; i += blockDim.x) s_lo[twpos(i)] = g_lo[i];
 }
 
 // CTA shape for the register-resident kernels: LPC lines of length N per CTA,

@@ -790,7 +790,7 @@ constexpr int kColsUCap = 4096;   // gradient rows staged in shared memory (32 K
 
 template <int N, int E>
 struct ColsAsync {
-    static constexpr int SMEM = N * 8 + 2 * 128 * 8 + N * 4 + kColsUCap * 8 + 16;
+    static constexpr int SMEM = N * 8 + 2 * 128 * 8 + N * 4 + kColsUCap * 8 + 32;
     static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
     static_assert(fft::LG<N, E>::LPC == 1, "one line per CTA");
 };
@@ -804,7 +804,8 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
     float2 *s_hi = smem + N;
     float *mbuf = reinterpret_cast<float *>(smem + N + 256);
     float2 *ubuf = reinterpret_cast<float2 *>(mbuf + N);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(ubuf + kColsUCap);   // [0] moment, [1] rows
+    // [0] moment, [1] gradient rows, [2] object column (into the exchange area)
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ubuf + kColsUCap);
     const int t = threadIdx.x;
     const bool u_async = a.rspan > 0 && a.rspan <= kColsUCap;
     const uint32_t ubytes = (uint32_t)((a.rspan + 1) & ~1) * 8u;
@@ -812,6 +813,7 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
     if (t == 0) {
         tma::mbar_init(&bar[0], 1);
         tma::mbar_init(&bar[1], 1);
+        tma::mbar_init(&bar[2], 1);
         tma::fence_barrier_init();
         if (c < N) {
             tma::arrive_expect_tx(&bar[0], N * 4);
@@ -826,8 +828,8 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
     __syncthreads();
     // each barrier completes once per column: the parity of the copy in flight, and
     // whether one is in flight (block-uniform)
-    uint32_t pm = 0, pu = 0;
-    bool mp = c < N, up = c < N && u_async;
+    uint32_t pm = 0, pu = 0, po = 0;
+    bool mp = c < N, up = c < N && u_async, op = false;
     bool failed = false;
     const float omb = 1.0f - a.beta;
     for (; c < N; c += gridDim.x) {
@@ -863,11 +865,23 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
                 v[m] = i < a.rspan ? u[i] : make_float2(0.f, 0.f);
             }
         }
-        line_fft_e<N, +1, E>(v, line, s_hi, s_hi + 128, t);
-        failed = __syncthreads_or(!tma::mbar_wait(&bar[0], pm));
+        // once the inverse FFT's last stage has read the exchange area, the object column
+        // is copied into it while that stage's butterflies run
+        const float2 *ocol = a.O + col;
+        fft::line_fft_regs32<N, +1>(v, line, s_hi, s_hi + 128, t, [&] {
+            if (t == 0) {
+                tma::fence_proxy_async();
+                tma::arrive_expect_tx(&bar[2], N * 8);
+                tma::load_1d(line, ocol, N * 8, &bar[2]);
+            }
+        });
+        op = true;
+        failed = __syncthreads_or(!tma::mbar_wait(&bar[0], pm) || !tma::mbar_wait(&bar[2], po));
         if (failed) break;
         mp = false;
         pm ^= 1u;
+        op = false;
+        po ^= 1u;
         // RMSprop on the column (constrained_RMSprop_both, kernels.cuh:364-382)
 #pragma unroll
         for (int m0 = 0; m0 < E; m0 += 4) {
@@ -875,7 +889,7 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
             float mv[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                w[k] = a.O[col + t + (m0 + k) * G::T];
+                w[k] = line[t + (m0 + k) * G::T];
                 mv[k] = mbuf[t + (m0 + k) * G::T];
             }
 #pragma unroll
@@ -891,7 +905,7 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
                 v[m0 + k] = w[k];
             }
         }
-        __syncthreads();                               // the moment buffer is free
+        __syncthreads();                               // the moment buffer and the area are free
         if (cn < N) {
             if (t == 0) {
                 tma::fence_proxy_async();
@@ -914,6 +928,7 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
         atomicExch(a.err, 1);
         if (mp) tma::mbar_wait(&bar[0], pm);           // bounded drains of copies in flight
         if (up) tma::mbar_wait(&bar[1], pu);
+        if (op) tma::mbar_wait(&bar[2], po);
     }
 }
 
@@ -1200,10 +1215,11 @@ cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs 
 }
 
 // Pass A's stitch over each LED's supported columns only, each line position owned by
-// one thread (FPM_STITCH_OWNED=1); otherwise every position loops over every LED
+// one thread; FPM_STITCH_OWNED=0 (measurements) loops every position over every LED
+// with Kahan sums instead
 static bool stitch_owned() {
     const char *e = std::getenv("FPM_STITCH_OWNED");
-    return e && std::atoi(e) != 0;
+    return !(e && std::atoi(e) == 0);
 }
 
 template <int N, int E>
