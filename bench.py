@@ -137,7 +137,7 @@ def make_workload_gpu(cfg: Cfg, dev):
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes per launch of each stage (documented in DESIGN.md)
+# algorithmic bytes per launch of each stage
 # ---------------------------------------------------------------------------
 def pupil_support(circ):
     """Rows / columns [lo, hi) of the pupil's non-zero pixels (the engine prunes to them)."""
@@ -424,8 +424,7 @@ def run_ours(args, cfg: Cfg):
 
 
 # DRAM traffic / algorithmic bytes of a launch, from one ncu capture of the kernel on a
-# smaller case (profiles/ncu_full_big_cols_update_16384_batch8.md: 6.972 GB measured for
-# 7.024 GB algorithmic); the object and moment terms dominate and scale with the units
+# smaller case (25 LEDs, batch 8: 6.972 GB measured for 7.024 GB algorithmic); the object and moment terms dominate and scale with the units
 # processed, so the full-size launch's traffic is this ratio x its algorithmic bytes.
 TRAFFIC_RATIO = {"cols_update": 0.993}
 
