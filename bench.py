@@ -190,7 +190,7 @@ def stage_bytes(cfg: Cfg, led, sup=None):
     for bi, (nb, rspan, cspan) in enumerate(boxes):
         _, rn, cn = boxes[(bi + 1) % nbatch]
         px = h2 * nb
-        tot["lr_cols_inverse"] += (8 * fr * fc + 8) * px   # support crop r8, field w8
+        tot["lr_cols_inverse"] += (8 * fr * fc + 8 * fc) * px   # support crop r8, support columns w8
         tot["lr_rows_inverse"] += 22 * px      # field r8 w8, residual w4, stack r2
         tot["lr_rows_forward"] += 20 * px      # residual r4, field r8 w8
         tot["lr_rows_fused"] += (10 + 8 * fc) * px   # field r8, stack r2, support columns w8

@@ -18,6 +18,9 @@ struct StackView {
     const void *ptr = nullptr;
     int type = kStackF32;
     const unsigned *minmax = nullptr;  // device [min, max] for kStackU16
+    // device amplitude sqrt((v - min) / (max - min)) of every uint16 value v, the same
+    // float the formula gives (kStackU16; null: kernels evaluate the formula)
+    const float *lut = nullptr;
 };
 
 // Half-open box of centred-spectrum rows/cols [lo, lo + span) taken modulo H.
@@ -64,6 +67,8 @@ struct OptStep {
 };
 cudaError_t launch_optimizer_step(const OptStep &o, cudaStream_t st);
 
+// amplitude of each of the 65536 uint16 values for the stack's (min, max)
+cudaError_t launch_amplitude_lut(const unsigned *minmax, float *lut, cudaStream_t st);
 // float stack: min / max and normalise in two launches; mm: 2 unsigned of scratch
 cudaError_t launch_normalise_f32(const float *p, size_t n, unsigned *mm, float *out,
                                  cudaStream_t st);

@@ -156,7 +156,7 @@ struct fpm_context {
     FftEngine fft;
     // work buffers, kept between calls
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
-        minmax, spec, flag;
+        minmax, lut, spec, flag;
     DevBuf opt[6];   // device copies of an optimiser step's host arrays
 };
 
@@ -349,6 +349,9 @@ fpm_status stage_inputs(fpm_context *ctx, const fpm_problem *p, const Shape &s, 
         FPM_CK(launch_stack_minmax(static_cast<const uint16_t *>(in.Y.ptr), s.plane * s.L,
                                    ctx->minmax.as<unsigned>(), st));
         in.Y.minmax = ctx->minmax.as<unsigned>();
+        FPM_CK(ctx->lut.ensure(65536 * sizeof(float)));
+        FPM_CK(launch_amplitude_lut(in.Y.minmax, ctx->lut.as<float>(), st));
+        in.Y.lut = ctx->lut.as<float>();
     }
     return FPM_OK;
 }
@@ -440,6 +443,10 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const
     // fused L2 + L3 where its CTA shape exists; FPM_LR_FUSED=0 keeps the separate passes
     pl.fused_rows = lr_rows_fused_supported(s.h);
     if (const char *env = std::getenv("FPM_LR_FUSED")) pl.fused_rows = pl.fused_rows && std::atoi(env) != 0;
+    // with the fused row pass the field buffer is written by L1 alone: its unsupported
+    // columns, cleared once per solve, stay zero and L1 skips them
+    const bool pruned_cols = sup.c_lo > 0 || sup.c_hi < s.h;
+    for (BatchGeom &g : pl.geoms) g.t1_clean = pl.fused_rows && pruned_cols ? 1 : 0;
     int parts = 0;
     for (int l0 = 0; l0 < s.B; l0 += pl.group) {
         const int nl = std::min(pl.group, s.B - l0);
@@ -477,6 +484,8 @@ fpm_status alloc_pipeline(fpm_context *ctx, const fpm_problem *p, const Shape &s
     FPM_CK(ctx->Pt.ensure(s.plane * 8));
     FPM_CK(ctx->Xs.ensure(s.plane * 8 * s.B));
     FPM_CK(ctx->T1.ensure(s.plane * 8 * pl.group));
+    if (!pl.geoms.empty() && pl.geoms[0].t1_clean)
+        FPM_CK(cudaMemsetAsync(ctx->T1.p, 0, s.plane * 8 * pl.group, ctx->stream));
     if (pl.fused_rows)
         FPM_CK(ctx->T2.ensure(s.plane * 8 * pl.group));
     else
@@ -515,7 +524,8 @@ fpm_status rows_forward(fpm_context *ctx, const Plan &pl, const Twiddles &tw,
     FPM_STAGE(ST_TRANSPOSE, launch_transpose(ctx->V.as<float2>(), pl.ldU, W, gn.H, gn.H, gn.rspan,
                                              0.f, st));
     FPM_STAGE(ST_ROWS_FORWARD, launch_big_rows_fwd(gn.H, W, gn.rspan, gn.Cu0, gn.cspan,
-                                                   ctx->Sboxr.as<float2>(), tw, st));
+                                                   ctx->Sboxr.as<float2>(), tw, st,
+                                                   ctx->flag.as<int>()));
     FPM_STAGE(ST_TRANSPOSE, launch_transpose(ctx->Sboxr.as<float2>(), gn.cspan,
                                              ctx->Sbox.as<float2>(), gn.rspan, gn.rspan, gn.cspan,
                                              0.f, st));

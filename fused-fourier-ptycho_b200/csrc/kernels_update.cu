@@ -302,6 +302,22 @@ cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *mm, fl
 }
 
 
+// Amplitude of every uint16 count: one table lookup per pixel in the passes instead of
+// a division and a square root, with the very floats the formula gives.
+__global__ void __launch_bounds__(256) k_amplitude_lut(const unsigned *__restrict__ mm,
+                                                        float *__restrict__ lut) {
+    const float mn = (float)mm[0];
+    const float range = (float)(mm[1] - mm[0]);
+    const unsigned v = blockIdx.x * blockDim.x + threadIdx.x;
+    const float x = (float)v - mn;
+    lut[v] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+}
+
+cudaError_t launch_amplitude_lut(const unsigned *mm, float *lut, cudaStream_t st) {
+    k_amplitude_lut<<<65536 / 256, 256, 0, st>>>(mm, lut);
+    return cudaGetLastError();
+}
+
 // Float stacks (multi-sample frames averaged on ingest): the same min / max and
 // sqrt((x - min) / (max - min)), min / max over order-preserving integer keys
 // of the float bits (NaN skipped, as MATLAB's min / max omit NaN).

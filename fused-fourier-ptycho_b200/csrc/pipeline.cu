@@ -97,6 +97,7 @@ __device__ __forceinline__ float stencil(float a, float right, float left, float
 template <int TYPE>
 __device__ __forceinline__ float amplitude(const StackView &Y, size_t idx, float mn, float range) {
     if (TYPE == kStackF32) return static_cast<const float *>(Y.ptr)[idx];
+    if (Y.lut) return Y.lut[static_cast<const uint16_t *>(Y.ptr)[idx]];
     const float x = (float)static_cast<const uint16_t *>(Y.ptr)[idx] - mn;
     return range > 0.f ? sqrtf(x / range) : sqrtf(x);
 }
@@ -160,10 +161,10 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
         }
     }
     // columns outside the support transform zeros: a CTA holding only such lines skips
-    // the transform and writes the zeros
+    // the transform and writes the zeros (none when the buffer already holds them)
     if (__syncthreads_or(nz))
         fft::line_fft_regs<N, +1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
-    if (live) {
+    if (live && (nz || !g.t1_clean)) {
         float2 *dst = T1 + (size_t)gl * N;
 #pragma unroll
         for (int m = 0; m < 16; ++m) dst[t + m * G::T] = v[m];
@@ -198,7 +199,8 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
         mn = (float)Y.minmax[0];
         range = (float)(Y.minmax[1] - Y.minmax[0]);
     }
-    const float ratio = (float)((double)N * N * g.pratio * g.pratio);
+    // 1 / (h^2 p^2): a power of two, so the product equals the quotient exactly
+    const float inv_ratio = (float)(1.0 / ((double)N * N * g.pratio * g.pratio));
     const size_t ypage = (size_t)(g.z_off + l0 + lloc) * N * N + r;
     float *rs = Rs + (size_t)lloc * N * N + r;
     float y[16];
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
         const size_t off = (size_t)(t + m * G::T) * N;
         const float2 z = v[m];
         page[off] = z;
-        rs[off] = sqrtf(z.x * z.x + z.y * z.y) / ratio - y[m];
+        rs[off] = sqrtf(z.x * z.x + z.y * z.y) * inv_ratio - y[m];
     }
 }
 
@@ -411,7 +413,8 @@ __global__ void __launch_bounds__(1024, 1)
             mn = (float)Y.minmax[0];
             range = (float)(Y.minmax[1] - Y.minmax[0]);
         }
-        const float ratio = (float)((double)N * N * g.pratio * g.pratio);
+        // 1 / (h^2 p^2): a power of two, so the product equals the quotient exactly
+    const float inv_ratio = (float)(1.0 / ((double)N * N * g.pratio * g.pratio));
         const size_t ypage = (size_t)zpage * N * N + r;
         float y[16];
         if (TYPE == kStackU16) {
@@ -426,8 +429,12 @@ __global__ void __launch_bounds__(1024, 1)
                     const int c = t + m * T;
                     const uint16_t raw = wrapped ? static_cast<const uint16_t *>(Y.ptr)[ypage + (size_t)c * N]
                                                  : ytile[c * F::YR + (rraw - y0)];
-                    const float x = (float)raw - mn;
-                    y[m] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+                    if (Y.lut) {
+                        y[m] = Y.lut[raw];
+                    } else {
+                        const float x = (float)raw - mn;
+                        y[m] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+                    }
                 }
             }
             __syncthreads();                            // the stack tile area becomes residuals
@@ -440,7 +447,7 @@ __global__ void __launch_bounds__(1024, 1)
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
                 const float2 z = v[m];
-                rk[t + m * T] = sqrtf(z.x * z.x + z.y * z.y) / ratio - y[m];
+                rk[t + m * T] = sqrtf(z.x * z.x + z.y * z.y) * inv_ratio - y[m];
             }
         }
         __syncthreads();
@@ -961,6 +968,65 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     }
 }
 
+// Pass C persistent (16384-point rows, 32 values per thread): a CTA per SM walks the
+// rows i = blockIdx.x + k gridDim.x; the next row is copied into the exchange area
+// while the current row's last FFT stage runs (bounded waits, device flag on failure).
+template <int N, int E>
+__global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
+    k_big_rows_fwd_async(const float2 *__restrict__ Vr, int rspan_n, int Cu0n, int cspan_n,
+                         float2 *__restrict__ Sboxr, int *__restrict__ err,
+                         const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
+    using G = fft::LG<N, E>;
+    static_assert(G::LPC == 1 && E == 32, "one 32-values-per-thread line per CTA");
+    extern __shared__ __align__(128) float2 smem[];
+    float2 *line = smem;
+    float2 *s_hi = smem + N;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(s_hi + 256);
+    const int t = threadIdx.x;
+    int i = blockIdx.x;
+    if (t == 0) {
+        tma::mbar_init(bar, 1);
+        tma::fence_barrier_init();
+        if (i < rspan_n) {
+            tma::arrive_expect_tx(bar, N * 8);
+            tma::load_1d(line, Vr + (size_t)i * N, N * 8, bar);
+        }
+    }
+    fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, G::NHI, G::NLO);
+    __syncthreads();
+    uint32_t parity = 0;
+    bool pending = i < rspan_n, failed = false;
+    for (; i < rspan_n; i += gridDim.x) {
+        failed = __syncthreads_or(!tma::mbar_wait(bar, parity));
+        if (failed) break;
+        pending = false;
+        parity ^= 1u;
+        float2 v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = line[t + m * G::T];
+        __syncthreads();                               // every read before the first exchange
+        const int in = i + gridDim.x;
+        fft::line_fft_regs32<N, -1>(v, line, s_hi, s_hi + 128, t, [&] {
+            if (t == 0 && in < rspan_n) {
+                tma::fence_proxy_async();
+                tma::arrive_expect_tx(bar, N * 8);
+                tma::load_1d(line, Vr + (size_t)in * N, N * 8, bar);
+            }
+        });
+        pending = in < rspan_n;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            int j = t + m * G::T - Cu0n;
+            if (j < 0) j += N;
+            if (j < cspan_n) Sboxr[(size_t)i * cspan_n + j] = v[m];
+        }
+    }
+    if (failed && t == 0) {
+        atomicExch(err, 1);
+        if (pending) tma::mbar_wait(bar, parity);      // bounded drain of the copy in flight
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1323,8 +1389,22 @@ static cudaError_t launch_rows_fwd_e(int rspan_n, int Cu0n, int cspan_n, const f
 }
 
 cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, int cspan_n,
-                                float2 *Sboxr, const Twiddles &tw, cudaStream_t st) {
+                                float2 *Sboxr, const Twiddles &tw, cudaStream_t st, int *err) {
     cudaError_t e = cudaSuccess;
+    if (H == 16384 && !cols_e16() && err && cols_async() && rspan_n > 0) {
+        using G = fft::LG<16384, 32>;
+        constexpr int smem = 16384 * 8 + 256 * 8 + 16;
+        e = set_smem(k_big_rows_fwd_async<16384, 32>, smem);
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        const int grid = rspan_n < sms ? rspan_n : sms;
+        k_big_rows_fwd_async<16384, 32><<<grid, G::THREADS, smem, st>>>(
+            Vr, rspan_n, Cu0n, cspan_n, Sboxr, err, tw.hi_hi, tw.hi_lo);
+        return cudaGetLastError();
+    }
 #define F(N)                                                                                  \
     if (N == 16384 && !cols_e16())                                                            \
         e = launch_rows_fwd_e<N, (N == 16384 ? 32 : 16)>(rspan_n, Cu0n, cspan_n, Vr, Sboxr, tw, st); \

@@ -22,6 +22,9 @@ struct BatchGeom {
     // spectrum there is never used, so the box above covers only this part of each crop
     int pr_lo = 0, pr_hi = 0, pc_lo = 0, pc_hi = 0;
     int loss = 0;   // LossKind
+    // the per-LED field buffer already holds zeros in the crop columns outside
+    // [pc_lo, pc_hi) (cleared once per solve), so L1 writes only the supported columns
+    int t1_clean = 0;
 };
 
 // Two-level twiddle tables (fft_core.cuh) for the low-res length h and the large length H.
@@ -94,7 +97,9 @@ cudaError_t launch_big_cols(const ColsArgs &a, const Twiddles &tw, cudaStream_t 
 
 // Pass C: rows i < rspan_n of Vr [rspan_n][H] -> FFT along the rows ->
 // Sboxr[i][j] = row[(Cu0n + j) mod H] (row-major, leading dim cspan_n).
+// err: device flag for the persistent form's bounded waits (null: the one-row-per-CTA form)
 cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, int cspan_n,
-                                float2 *Sboxr, const Twiddles &tw, cudaStream_t st);
+                                float2 *Sboxr, const Twiddles &tw, cudaStream_t st,
+                                int *err = nullptr);
 
 }  // namespace fpm
