@@ -619,39 +619,76 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
 #pragma unroll
         for (int m = 0; m < E; ++m) acc[t + m * G::T] = make_float2(0.f, 0.f);
         const int W = g.pc_hi - g.pc_lo;
-        for (int l = 0; live && l < g.nb; ++l) {
+        // one covering LED's share of this line: its rows of Xs and Pt and the position
+        // of its first supported column; four of this thread's positions per pass
+        struct Src {
+            const float2 *x = nullptr, *p = nullptr;
+            int es = 0, base = 0x7fffffff;
+        };
+        auto src_of = [&](int l) {
+            Src q;
             const int2 ab = s_ab[l];
             int rr = i - ab.x;
             if (rr < 0) rr += N;
-            if (rr < g.pr_lo || rr >= g.pr_hi) continue;   // pupil zero on that crop row
-            const float2 *xrow = Xs + ((size_t)l * h + rr) * h + g.pc_lo;
-            const float2 *prow = Pt + (size_t)rr * h + g.pc_lo;
-            const int es = (int)(((long long)g.pc_lo + ab.y + g.Cu0) % N);   // position of idx 0
-            // four positions in flight per pass: their loads issue together
-            for (int base = (t - es) & (G::T - 1); base < W; base += 4 * G::T) {
-                float2 x[4], pp[4];
+            if (rr < g.pr_lo || rr >= g.pr_hi) return q;   // pupil zero on that crop row
+            q.x = Xs + ((size_t)l * h + rr) * h + g.pc_lo;
+            q.p = Pt + (size_t)rr * h + g.pc_lo;
+            q.es = (int)(((long long)g.pc_lo + ab.y + g.Cu0) % N);   // position of idx 0
+            q.base = (t - q.es) & (G::T - 1);
+            return q;
+        };
+        auto load4 = [&](const Src &q, int base, float2 (&x)[4], float2 (&pp)[4]) {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int idx = base + u * G::T;
-                    x[u] = idx < W ? xrow[idx] : make_float2(0.f, 0.f);
-                    pp[u] = idx < W ? prow[idx] : make_float2(0.f, 0.f);
-                }
+            for (int u = 0; u < 4; ++u) {
+                const int idx = base + u * G::T;
+                x[u] = idx < W ? q.x[idx] : make_float2(0.f, 0.f);
+                pp[u] = idx < W ? q.p[idx] : make_float2(0.f, 0.f);
+            }
+        };
+        auto add4 = [&](const Src &q, int base, const float2 (&x)[4], const float2 (&pp)[4]) {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int idx = base + u * G::T;
-                    if (idx < W) {
-                        int e = es + idx;
-                        if (e >= N) e -= N;
-                        int j = e - g.Cu0;                  // box column
-                        if (j < 0) j += N;
-                        if (j < g.cspan) {
-                            const float2 pr = cmul(x[u], pp[u]);
-                            float2 a = acc[e];
-                            a.x += pr.x;
-                            a.y += pr.y;
-                            acc[e] = a;
-                        }
+            for (int u = 0; u < 4; ++u) {
+                const int idx = base + u * G::T;
+                if (idx < W) {
+                    int e = q.es + idx;
+                    if (e >= N) e -= N;
+                    int j = e - g.Cu0;                  // box column
+                    if (j < 0) j += N;
+                    if (j < g.cspan) {
+                        const float2 pr = cmul(x[u], pp[u]);
+                        float2 a = acc[e];
+                        a.x += pr.x;
+                        a.y += pr.y;
+                        acc[e] = a;
                     }
+                }
+            }
+        };
+        if (W <= 4 * G::T) {
+            // every LED in one pass: two covering LEDs' loads in flight together, each
+            // position still summed in LED order
+            int l = 0;
+            while (live) {
+                Src qa, qb;
+                for (; l < g.nb && !(qa = src_of(l)).x; ++l) {}
+                if (l >= g.nb) break;
+                for (++l; l < g.nb && !(qb = src_of(l)).x; ++l) {}
+                ++l;
+                float2 xa[4], pa[4], xb[4], pb[4];
+                load4(qa, qa.base, xa, pa);
+                if (qb.x) load4(qb, qb.base, xb, pb);
+                add4(qa, qa.base, xa, pa);
+                if (qb.x) add4(qb, qb.base, xb, pb);
+                if (!qb.x) break;
+            }
+        } else {
+            for (int l = 0; live && l < g.nb; ++l) {
+                const Src q = src_of(l);
+                if (!q.x) continue;
+                for (int base = q.base; base < W; base += 4 * G::T) {
+                    float2 x[4], pp[4];
+                    load4(q, base, x, pp);
+                    add4(q, base, x, pp);
                 }
             }
         }
