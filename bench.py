@@ -11,7 +11,7 @@ noise at 3e4 peak counts) generated on the GPU before timing.
 A step is one epoch (361 LEDs in 14 mini-batches).  ``value`` is the time of
 the 10-epoch reconstruction (10 x the measured seconds per epoch) with every
 input resident in HBM; ``e2e`` is the same 10-epoch job through the C ABI with
-pinned host buffers (stack in, object + spectrum + pupil + loss out, copies
+pinned host buffers (stack in, object + pupil + loss out as the mex returns, copies
 inside the timed region).  ``--impl reference`` times the CPU restatement of the
 reference algorithm (FP32 numpy/pocketfft, all host cores) on a bounded sample
 of the same workload (one mini-batch per step) and projects the 10-epoch time.
@@ -393,11 +393,12 @@ def run_ours(args, cfg: Cfg):
                        wl["led_np"], _support_of(wl)), wl, rank, world
     pin = lambda x: x.cpu().pin_memory()
     hs, hl, hp, ha = pin(wl["stack"]), pin(wl["led"]), pin(wl["P0c"]), pin(wl["P0"])
+    # the outputs of the reference's mex call, [O, P] (cuFPM_pure_v3.cu plhs[0..1]), plus
+    # the per-epoch loss (80 bytes); the centred spectrum is an extra of this engine
     hO = torch.empty((H, H), dtype=torch.complex64).pin_memory()
-    hS = torch.empty((H, H), dtype=torch.complex64).pin_memory()
     hP = torch.empty((h, h), dtype=torch.complex64).pin_memory()
     hL = torch.empty(JOB_EPOCHS, dtype=torch.float64).pin_memory()
-    hres = api.Result(object=hO.data_ptr(), spectrum=hS.data_ptr(), pupil=hP.data_ptr(),
+    hres = api.Result(object=hO.data_ptr(), spectrum=None, pupil=hP.data_ptr(),
                       loss=hL.data_ptr())
     hprob = problem(JOB_EPOCHS, api.MEM_HOST, hs.data_ptr(), hl.data_ptr(), hp.data_ptr(),
                     ha.data_ptr())
@@ -412,11 +413,11 @@ def run_ours(args, cfg: Cfg):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_s = float(t.item())
     h2d = sum(x.numel() * x.element_size() for x in (hs, hl, hp, ha))
-    d2h = sum(x.numel() * x.element_size() for x in (hO, hS, hP, hL))
+    d2h = sum(x.numel() * x.element_size() for x in (hO, hP, hL))
     e2e = {"value": round(e2e_s, 4), "unit": "s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h,
            "note": "one 10-epoch job per step through fpm_solve with pinned host buffers; "
-                   "stack/LEDs/pupil in, object+spectrum+pupil+loss out"}
+                   "stack/LEDs/pupil in, object+pupil+loss out (the mex's outputs)"}
     out = _report(args, cfg, rank, world, ms, ms_step, stages, clocks, epoch_loss, e2e,
                   wl["led_np"], _support_of(wl))
     eng.close()
