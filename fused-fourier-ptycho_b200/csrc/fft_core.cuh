@@ -298,11 +298,11 @@ __device__ __forceinline__ void stages_regs(float2 (&v)[E], float2 *s, const flo
 // Unnormalised DFT of a line held in canonical registers (see above).  Must be
 // reached by every thread of the block when N > 16 (it synchronises); the
 // shared-memory line s must not be in use by other threads on entry.
-template <int N, int DIR>
+template <int N, int DIR, typename Hook = NoHook>
 __device__ __forceinline__ void line_fft_regs(float2 (&v)[16], float2 *s, const float2 *hi,
-                                              const float2 *lo, int t) {
+                                              const float2 *lo, int t, const Hook &hook = Hook{}) {
     static_assert(N >= 16 && (N & (N - 1)) == 0, "power-of-two length >= 16");
-    stages_regs<N, DIR, 1, 16>(v, s, hi, lo, t);
+    stages_regs<N, DIR, 1, 16, Hook>(v, s, hi, lo, t, hook);
 }
 
 // The same with 32 values per thread (t + m N/32, m < 32): radix-32 stages, one

@@ -548,6 +548,89 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
     }
 }
 
+// L4 persistent (h of 2048): a CTA walks groups of LPC consecutive columns (skipping
+// groups with no supported column); the next group's columns are copied into the
+// exchange area while this group's last FFT stage runs.  Two CTAs per SM.
+template <int N>
+__global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
+    k_lr_cols_fwd_async(BatchGeom g, int l0, int nl, const float2 *__restrict__ T1,
+                        float2 *__restrict__ Xs, int *__restrict__ err,
+                        const float2 *__restrict__ thi, const float2 *__restrict__ tlo) {
+    using G = fft::LG<N>;
+    static_assert(G::LPC > 1 && (G::STRIDE * 8) % 16 == 0, "16-byte aligned line starts");
+    extern __shared__ __align__(128) float2 smem[];
+    constexpr int hh = N / 2;
+    const int ngroups = nl * N / G::LPC;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(G::tw_hi(smem) + 256);
+    // first group at or after q holding a supported column (block-uniform)
+    auto next_group = [&](int q) {
+        for (; q < ngroups; q += gridDim.x) {
+            const int cf0 = (int)(((long long)q * G::LPC) % N);
+            for (int k = 0; k < G::LPC; ++k) {
+                const int cf = cf0 + k;
+                const int c = cf + hh >= N ? cf + hh - N : cf + hh;
+                if (c >= g.pc_lo && c < g.pc_hi) return q;
+            }
+        }
+        return ngroups;
+    };
+    auto fetch = [&](int q) {   // one thread: the LPC columns of group q into the lines
+        tma::arrive_expect_tx(bar, G::LPC * N * 8);
+        for (int k = 0; k < G::LPC; ++k)
+            tma::load_1d(smem + k * G::STRIDE, T1 + ((size_t)q * G::LPC + k) * N, N * 8, bar);
+    };
+    const int ln = G::iline(), t = G::it();
+    int q = next_group(blockIdx.x);
+    if (threadIdx.x == 0) {
+        tma::mbar_init(bar, 1);
+        tma::fence_barrier_init();
+        if (q < ngroups) fetch(q);
+    }
+    fft::load_twiddles(G::tw_hi(smem), G::tw_hi(smem) + 128, thi, tlo, G::NHI, G::NLO);
+    __syncthreads();
+    uint32_t parity = 0;
+    bool pending = q < ngroups, failed = false;
+    while (q < ngroups) {
+        failed = __syncthreads_or(!tma::mbar_wait(bar, parity));
+        if (failed) break;
+        pending = false;
+        parity ^= 1u;
+        const long long gl = (long long)q * G::LPC + ln;
+        const int cf = (int)(gl % N);
+        const int c = cf + hh >= N ? cf + hh - N : cf + hh;
+        const bool need = c >= g.pc_lo && c < g.pc_hi;
+        float2 v[16];
+        const float2 *line = smem + ln * G::STRIDE;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[m] = need ? line[t + m * G::T] : make_float2(0.f, 0.f);
+        __syncthreads();                                // every read before the first exchange
+        const int qn = next_group(q + gridDim.x);
+        fft::line_fft_regs<N, -1>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128,
+                                  t, [&] {
+                                      if (threadIdx.x == 0 && qn < ngroups) {
+                                          tma::fence_proxy_async();
+                                          fetch(qn);
+                                      }
+                                  });
+        pending = qn < ngroups;
+        if (need) {
+            const int lloc = (int)(gl / N);
+            float2 *xs = Xs + (size_t)(l0 + lloc) * N * N + c;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int e = t + m * G::T;             // frequency row of X
+                const int r = e + hh >= N ? e + hh - N : e + hh;
+                xs[(size_t)r * N] = v[m];
+            }
+        }
+        q = qn;
+    }
+    if (failed && threadIdx.x == 0) {
+        atomicExch(err, 1);
+        if (pending) tma::mbar_wait(bar, parity);      // bounded drain of the copies in flight
+    }
+}
+
 // ---------------------------------------------------------------------------
 // pupil gradient: 32 x 32 tiles, LED loop inside, Kahan accumulation
 // ---------------------------------------------------------------------------
@@ -1296,10 +1379,27 @@ cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_page
     return cudaGetLastError();
 }
 
+static bool cols_async();
+
 cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs b, int l0,
                                int nl, const Twiddles &tw, cudaStream_t st) {
     const int blocks = lr_blocks(g.h, nl);
     cudaError_t e = cudaSuccess;
+    if (g.h == 2048 && b.flag && cols_async()) {
+        using G = fft::LG<2048>;
+        constexpr int smem = G::SMEM + 16;
+        e = set_smem(k_lr_cols_fwd_async<2048>, smem);
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        const int ngroups = nl * 2048 / G::LPC;
+        const int grid = ngroups < 2 * sms ? ngroups : 2 * sms;
+        k_lr_cols_fwd_async<2048><<<grid, G::THREADS, smem, st>>>(g, l0, nl, src, b.Xs, b.flag,
+                                                                  tw.lo_hi, tw.lo_lo);
+        return cudaGetLastError();
+    }
 #define F(N)                                                                              \
     e = set_smem(k_lr_cols_fwd<N>, smem_bytes<N>());                                      \
     if (e != cudaSuccess) return e;                                                       \
