@@ -1196,6 +1196,8 @@ int lr_blocks(int h, int nl) {
     return (int)((lines + lpc - 1) / lpc);
 }
 
+static bool cols_async();
+
 cudaError_t launch_lr_cols_inv(const BatchGeom &g, const int2 *led, const float2 *P, BatchBufs b,
                                int l0, int nl, const Twiddles &tw, cudaStream_t st) {
     const int blocks = lr_blocks(g.h, nl);
@@ -1378,8 +1380,6 @@ cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_page
 #undef F
     return cudaGetLastError();
 }
-
-static bool cols_async();
 
 cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs b, int l0,
                                int nl, const Twiddles &tw, cudaStream_t st) {

@@ -525,3 +525,40 @@ def test_16384_columns_32_values_per_thread_match_16(engine):
     for a, b in zip(runs["0"], runs["1"]):
         assert orc.rel_err(a, b) < 3e-5, orc.rel_err(a, b)
 
+
+
+def test_prefetching_passes_equal_plain_loads(engine):
+    """The persistent passes that copy their next input into shared memory during the
+    last FFT stage (column update, next-box rows, and at h = 2048 the low-resolution
+    forward column pass) compute what their plain-load forms (FPM_COLS_ASYNC=0) compute: a
+    2048^2 -> 16384^2 solve over two batches with uint16 frames, whose LED crops sit off
+    the box edge, must be bit-identical (the loss to double rounding of its partials)."""
+    import os
+    import torch
+    from fpm_b200 import synth
+    h, p = 2048, 8
+    H = h * p
+    optics = synth.Optics(led_grid=3)
+    circ = synth.pupil_circle(h, optics)
+    led = led_matlab(synth.led_indices(h, p, optics)[:5])
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    Y = torch.randint(0, 40000, (5, h, h), generator=g, device="cuda",
+                      dtype=torch.int32).to(torch.uint16).permute(1, 2, 0)
+    O0 = torch.polar(torch.ones((H, H), device="cuda"),
+                     0.1 * torch.randn((H, H), generator=g, device="cuda")).contiguous()
+    P0c = torch.from_numpy(circ.astype(np.complex64)).cuda()
+    P0 = torch.from_numpy(circ).cuda()
+    ledt = torch.from_numpy(led).cuda()
+    runs = {}
+    for flag in ("1", "0"):
+        os.environ["FPM_COLS_ASYNC"] = flag
+        try:
+            r = engine.solve(O0, P0c, Y, ledt, P0, p, 2, 3, lr=1e-3, spectrum=False)
+            runs[flag] = (r["object"].cpu().numpy(), r["pupil"].cpu().numpy(),
+                          np.asarray(r["loss"].cpu() if hasattr(r["loss"], "cpu") else r["loss"]))
+        finally:
+            del os.environ["FPM_COLS_ASYNC"]
+    np.testing.assert_array_equal(runs["1"][0], runs["0"][0])
+    np.testing.assert_array_equal(runs["1"][1], runs["0"][1])
+    np.testing.assert_allclose(runs["1"][2], runs["0"][2], rtol=1e-12)
