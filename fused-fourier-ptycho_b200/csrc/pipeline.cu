@@ -647,20 +647,32 @@ __global__ void __launch_bounds__(256) k_lr_pupil_grad(const float2 *__restrict_
     // outside the pupil support the gradient is never used (the amplitude clamp keeps
     // the pupil at zero there): tiles beyond it only write zeros
     const bool any = r0 < g.pr_hi && r0 + 32 > g.pr_lo && c0 < g.pc_hi && c0 + 32 > g.pc_lo;
-    for (int l = 0; any && l < g.nb; ++l) {
+    // LED l's tile values into registers; LED l + 1's loads are in flight while LED l's
+    // products are summed
+    float2 na[4], nx[4];
+    auto load = [&](int l) {
         const int2 ab = led_box_offset(led, l, g);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int cl = ty + 8 * k;
             const int r = r0 + tx, c = c0 + cl;       // sub: coalesced along r
             const bool a_in = r >= g.pr_lo && r < g.pr_hi && c >= g.pc_lo && c < g.pc_hi;
-            sA[cl][tx] = a_in ? Sbox[(size_t)box_index(ab.y, c, g.H) * g.rspan + box_index(ab.x, r, g.H)]
-                              : make_float2(0.f, 0.f);
+            na[k] = a_in ? Sbox[(size_t)box_index(ab.y, c, g.H) * g.rspan + box_index(ab.x, r, g.H)]
+                         : make_float2(0.f, 0.f);
             const int rr = r0 + cl, cc = c0 + tx;     // Xs: coalesced along c
             const bool b_in = rr >= g.pr_lo && rr < g.pr_hi && cc >= g.pc_lo && cc < g.pc_hi;
-            sB[cl][tx] = b_in ? Xs[((size_t)l * h + rr) * h + cc] : make_float2(0.f, 0.f);
+            nx[k] = b_in ? Xs[((size_t)l * h + rr) * h + cc] : make_float2(0.f, 0.f);
+        }
+    };
+    if (any && g.nb > 0) load(0);
+    for (int l = 0; any && l < g.nb; ++l) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            sA[ty + 8 * k][tx] = na[k];
+            sB[ty + 8 * k][tx] = nx[k];
         }
         __syncthreads();
+        if (l + 1 < g.nb) load(l + 1);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int cl = ty + 8 * k;
@@ -749,7 +761,7 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
         };
         if (W <= 4 * G::T) {
             // every LED in one pass: two covering LEDs' loads in flight together, each
-            // position still summed in LED order
+            // position still summed in LED order (four in flight measured no faster)
             int l = 0;
             while (live) {
                 Src qa, qb;
