@@ -327,6 +327,19 @@ def cpu_inputs_from_gpu(cfg: Cfg, eng, wl, nled: int):
 
 
 # ---------------------------------------------------------------------------
+def replica_max(value: float, world: int, device=None) -> float:
+    """The slowest replica's figure: every rank runs its own reconstruction (no shard of
+    one reconstruction, no collective on the data path), and a job of N replicas takes
+    as long as its slowest rank.  All ranks must call it (one all-reduce)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, cfg: Cfg):
     import torch
     import torch.distributed as dist
@@ -380,10 +393,7 @@ def run_ours(args, cfg: Cfg):
     ms = e0.elapsed_time(e1)
     stages = eng.stage_times()
     eng.set_profiling(False)
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = replica_max(ms, world, dev)
     ms_step = ms / args.steps
     epoch_loss = loss[: args.steps].cpu().numpy()
 
@@ -408,10 +418,7 @@ def run_ours(args, cfg: Cfg):
     w0 = time.perf_counter()
     eng._check(eng.solve_raw(hprob, hres))
     e2e_s = time.perf_counter() - w0       # the call returns after its final synchronisation
-    t = torch.tensor([e2e_s], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_s = float(t.item())
+    e2e_s = replica_max(e2e_s, world, dev)
     h2d = sum(x.numel() * x.element_size() for x in (hs, hl, hp, ha))
     d2h = sum(x.numel() * x.element_size() for x in (hO, hP, hL))
     e2e = {"value": round(e2e_s, 4), "unit": "s", "h2d_bytes_per_step": h2d,
