@@ -562,3 +562,29 @@ def test_prefetching_passes_equal_plain_loads(engine):
     np.testing.assert_array_equal(runs["1"][0], runs["0"][0])
     np.testing.assert_array_equal(runs["1"][1], runs["0"][1])
     np.testing.assert_allclose(runs["1"][2], runs["0"][2], rtol=1e-12)
+
+
+def test_large_lowres_side_two_pass_rows_vs_oracle(engine):
+    """h = 4096 (beyond the fused row pass: the two-pass L2 / L3 form), pratio 2 ->
+    8192², one batch of three LEDs with one crop past the spectrum edge, one update,
+    against the FP64 oracle."""
+    from fpm_b200 import synth
+    rng = np.random.default_rng(41)
+    h, p = 4096, 2
+    H = h * p
+    P0 = synth.pupil_circle(h, synth.Optics(led_grid=3)).astype(np.float32)
+    O0 = (0.5 + 0.5 * rng.random((H, H)) * np.exp(1j * rng.random((H, H)))).astype(np.complex64)
+    led = np.array([[H // 2 - h // 2 + 1, H // 2 - h // 2 + 1], [H - 100, 50], [700, 1900]],
+                   np.int32)
+    Y = rng.random((3, h, h)).astype(np.float32)
+    opt = (1e-3, 0.999, 1e-4)
+    r = engine.solve(O0, P0.astype(np.complex64), to_matlab_stack(Y), led_matlab(led), P0, p, 1, 3,
+                     lr=opt[0], beta=opt[1], eps=opt[2])
+    args = (O0, P0.astype(np.complex64), Y, led, P0, p, 1, 3)
+    o = orc.cufpm_pure_v3(*args, opt=opt, workers=orc.default_workers())
+    # FP32 rounding of 4096² and 8192² transforms: the bar is the FP32 twin's own distance
+    o32 = orc.cufpm_pure_v3(*args, opt=opt, dtype=np.float32, workers=orc.default_workers())
+    for k in ("object", "pupil"):
+        e, e32 = orc.rel_err(r[k], getattr(o, k)), orc.rel_err(getattr(o32, k), getattr(o, k))
+        assert e < max(TIGHT, 3 * e32), (k, e, e32)
+    np.testing.assert_allclose(r["loss"], o.loss, rtol=1e-5)
