@@ -362,14 +362,25 @@ __global__ void __launch_bounds__(1024, 1)
     const int x0 = r0 - 2;                      // first tile row (even: 16-byte TMA rule)
     const int y0 = (r0 - 1) & ~7;               // first stack tile row (8 x 2 bytes)
     const int zpage = g.z_off + l0 + lloc;
+    // boxes of CB stored columns holding a supported crop column; with a field buffer
+    // whose other columns are known zeros (t1_clean) only those are copied
+    unsigned boxes = 0;
+#pragma unroll
+    for (int q = 0; q < N / F::CB; ++q) {
+        const int lo = (q * F::CB + N / 2) % N, hi = lo + F::CB;   // crop columns of box q
+        const bool sup = hi <= N ? (lo < g.pc_hi && hi > g.pc_lo)
+                                 : (lo < g.pc_hi || hi - N > g.pc_lo);
+        if (sup || !g.t1_clean) boxes |= 1u << q;
+    }
     if (threadIdx.x == 0) {
         tma::mbar_init(&bar[0], 1);
         tma::mbar_init(&bar[1], 1);
         tma::fence_barrier_init();
-        tma::arrive_expect_tx(&bar[0], F::XR * N * 8);
+        tma::arrive_expect_tx(&bar[0], (uint32_t)__popc(boxes) * F::XR * F::CB * 8);
 #pragma unroll 1
         for (int q = 0; q < N / F::CB; ++q)
-            tma::load_3d(smem + q * F::CB * F::XR, &tm_field, x0, q * F::CB, lloc, &bar[0]);
+            if (boxes >> q & 1u)
+                tma::load_3d(smem + q * F::CB * F::XR, &tm_field, x0, q * F::CB, lloc, &bar[0]);
     }
     fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, F::NHI, F::NLO);
     __syncthreads();                                    // barriers initialised before any wait
@@ -396,7 +407,9 @@ __global__ void __launch_bounds__(1024, 1)
     if (!failed) {
         if (!wrapped) {
 #pragma unroll
-            for (int m = 0; m < 16; ++m) v[m] = tile[(t + m * T) * F::XR + (rraw - x0)];
+            for (int m = 0; m < 16; ++m)
+                v[m] = boxes >> ((t + m * T) / F::CB) & 1u ? tile[(t + m * T) * F::XR + (rraw - x0)]
+                                                          : make_float2(0.f, 0.f);
         }
         __syncthreads();                                // the tile area becomes FFT scratch
         if (TYPE == kStackU16 && threadIdx.x == 0) {

@@ -5,9 +5,9 @@ kernels plus cuFFT, driven by the replica of cuFPM_v3/cuFPM_pure_v3.cu:75-207 in
 oracle/ref_harness.cu) and times its epoch loop with CUDA events (``ms[0]`` of
 ``ref_solve``: allocation, cuFFT planning and host copies excluded) on the
 workload bench.py times: 19 x 19 LEDs of 2048^2 -> 16384^2, LED batch 26.  The
-pixel values do not change the timing of either implementation, so the stack is
+pixel values do not change the timing of the reference's kernels, so the stack is
 the seeded random uint16 stack of ``bench.py --quick-data``, normalised to
-amplitudes on the GPU the way the engine does in-kernel.
+amplitudes on the GPU as the reference's driver does before its call.
 
     python oracle/time_ref.py [--epochs 3] [--h 2048 --pratio 8 --grid 19 --batch 26]
 
