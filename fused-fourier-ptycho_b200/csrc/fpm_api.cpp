@@ -156,7 +156,7 @@ struct fpm_context {
     FftEngine fft;
     // work buffers, kept between calls
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
-        minmax, lut, spec, flag;
+        minmax, lut, spec, flag, pie;
     DevBuf opt[6];   // device copies of an optimiser step's host arrays
 };
 
@@ -276,6 +276,8 @@ fpm_status validate(fpm_context *ctx, const fpm_problem *p, bool need_batch) {
                     std::min(p->batch, p->n_leds));
     if (p->loss_kind != FPM_LOSS_ANISOTROPIC && p->loss_kind != FPM_LOSS_ISOTROPIC)
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "loss_kind %d", p->loss_kind);
+    if (p->pie_weights < FPM_PIE_NONE || p->pie_weights > FPM_PIE_TPIE)
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pie_weights %d", p->pie_weights);
     if (p->memory != FPM_MEM_HOST && p->memory != FPM_MEM_DEVICE)
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", p->memory);
     if (p->stack_type != FPM_STACK_F32_AMPLITUDE && p->stack_type != FPM_STACK_U16_COUNTS)
@@ -365,6 +367,8 @@ fpm_status pupil_support(fpm_context *ctx, const fpm_problem *p, const Shape &s,
     sup.r_hi = sup.c_hi = s.h;
     if (const char *env = std::getenv("FPM_PUPIL_SUPPORT"))
         if (std::atoi(env) == 0) return FPM_OK;
+    // ePIE scales each pupil term by the maximum over the LED's whole crop
+    if (p->pie_weights == FPM_PIE_EPIE) return FPM_OK;
     int box[4] = {s.h, -1, s.h, -1};
     if (p->memory == FPM_MEM_HOST) {
         const float *P = p->pupil_init, *A = p->pupil_amp;
@@ -405,7 +409,7 @@ struct Plan {
 
 
 Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const Support &sup,
-               int loss) {
+               int loss, int pie) {
     Plan pl;
     for (int cur = 0; cur < s.L; cur += batch) {
         const int nb = std::min(batch, s.L - cur);
@@ -427,6 +431,7 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const
         g.pc_lo = sup.c_lo;
         g.pc_hi = sup.c_hi;
         g.loss = loss == FPM_LOSS_ISOTROPIC ? kLossIsotropic : kLossAnisotropic;
+        g.pie = pie;
         pl.geoms.push_back(g);
         pl.ldU = std::max(pl.ldU, (g.rspan + 3) & ~3);   // columns 32-byte aligned (bulk copies)
         pl.sbox = std::max(pl.sbox, (size_t)g.rspan * g.cspan);
@@ -570,10 +575,17 @@ fpm_status lowres_and_stitch(fpm_context *ctx, const Plan &pl, const Twiddles &t
         }
     }
     FPM_STAGE(ST_LOSS, launch_loss_accumulate(b.parts, part_off, loss_slot, st));
-    FPM_STAGE(ST_PUPIL_GRAD, launch_lr_pupil_grad(g, in.led, b, ctx->dP.as<float2>(), st));
+    unsigned *pie = nullptr;
+    if (g.pie != FPM_PIE_NONE) {   // ePIE / tPIE weights of the two gradient terms
+        FPM_CK(ctx->pie.ensure(sizeof(unsigned) * (1 + (size_t)g.nb)));
+        pie = ctx->pie.as<unsigned>();
+        FPM_STAGE(ST_PUPIL_GRAD, launch_pie_prepare(g, P, in.led, b.Sbox, pie, st));
+    }
+    FPM_STAGE(ST_PUPIL_GRAD, launch_lr_pupil_grad(g, in.led, b, ctx->dP.as<float2>(), st, pie));
     // conj(P) / H^2, row-major, for coalesced pupil reads in the stitch
     FPM_STAGE(ST_TRANSPOSE, launch_transpose(P, g.h, ctx->Pt.as<float2>(), g.h, g.h, g.h,
                                              (float)(1.0 / ((double)g.H * g.H)), st));
+    if (pie) FPM_STAGE(ST_TRANSPOSE, launch_pie_object_weights(g, ctx->Pt.as<float2>(), pie, st));
     float2 *W = ctx->W.as<float2>();
     FPM_STAGE(ST_ROWS_INV, launch_big_rows_inv(g, in.led, ctx->Pt.as<float2>(), b.Xs, W, tw, st));
     FPM_STAGE(ST_TRANSPOSE, launch_transpose(W, g.H, ctx->U.as<float2>(), pl.ldU, g.rspan, g.H,
@@ -763,7 +775,7 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     Support sup;
     rc = pupil_support(ctx, p, s, sup);
     if (rc != FPM_OK) return rc;
-    const Plan pl = make_plan(s, led_host, p->batch, sup, p->loss_kind);
+    const Plan pl = make_plan(s, led_host, p->batch, sup, p->loss_kind, p->pie_weights);
     rc = alloc_pipeline(ctx, p, s, pl, res->spectrum != nullptr);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;
@@ -925,7 +937,7 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
     if (rc != FPM_OK) return rc;
     Support full;   // the pupil gradient is an output here: whole crops
     full.r_hi = full.c_hi = s.h;
-    const Plan pl = make_plan(s, led_host, s.L, full, p->loss_kind);
+    const Plan pl = make_plan(s, led_host, s.L, full, p->loss_kind, p->pie_weights);
     rc = alloc_pipeline(ctx, p, s, pl, true);
     if (rc != FPM_OK) return rc;
     cudaStream_t st = ctx->stream;

@@ -28,6 +28,8 @@
 #include "engine.h"
 #include "fft_core.cuh"
 #include "pipeline.h"
+
+#include <algorithm>
 #include "tma.cuh"
 
 #include <cudaTypedefs.h>
@@ -650,7 +652,8 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 __global__ void __launch_bounds__(256) k_lr_pupil_grad(const float2 *__restrict__ Sbox,
                                                         const float2 *__restrict__ Xs,
                                                         const int2 *__restrict__ led, BatchGeom g,
-                                                        float2 *__restrict__ dP) {
+                                                        float2 *__restrict__ dP,
+                                                        const unsigned *__restrict__ pie) {
     __shared__ float2 sA[32][33];   // sub: [c][r]
     __shared__ float2 sB[32][33];   // Xs:  [r][c]
     const int h = g.h;
@@ -686,10 +689,18 @@ __global__ void __launch_bounds__(256) k_lr_pupil_grad(const float2 *__restrict_
         }
         __syncthreads();
         if (l + 1 < g.nb) load(l + 1);
+        // ePIE: the LED's term over max|sub_l|^2 of its whole crop
+        const float emax = g.pie == 1 ? __uint_as_float(pie[1 + l]) : 1.f;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int cl = ty + 8 * k;
-            acc[k].add(cmul_conj(sB[tx][cl], sA[cl][tx]));
+            const float2 a = sA[cl][tx];
+            float2 term = cmul_conj(sB[tx][cl], a);
+            if (g.pie != 0) {   // deconv_pie (fpm_forward_GPU.m:64-76): conj(sub) X ./ weight
+                const float den = g.pie == 1 ? emax : a.x * a.x + a.y * a.y + 1e-5f;
+                term = make_float2(term.x / den, term.y / den);
+            }
+            acc[k].add(term);
         }
         __syncthreads();
     }
@@ -1436,9 +1447,81 @@ cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs 
 }
 
 cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs b, float2 *dP,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, const unsigned *pie_scratch) {
+    if (g.pie == 1 && !pie_scratch) return cudaErrorInvalidValue;
     const int t = (g.h + 31) / 32;
-    k_lr_pupil_grad<<<dim3(t, t), 256, 0, st>>>(b.Sbox, b.Xs, led, g, dP);
+    k_lr_pupil_grad<<<dim3(t, t), 256, 0, st>>>(b.Sbox, b.Xs, led, g, dP, pie_scratch);
+    return cudaGetLastError();
+}
+
+// max |x|^2 of non-negative floats through integer atomics on their bit patterns
+__device__ __forceinline__ void max_abs2(unsigned *slot, float v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(slot, __float_as_uint(v));
+}
+
+__global__ void __launch_bounds__(256) k_pupil_abs2_max(const float2 *__restrict__ P, int n,
+                                                         unsigned *__restrict__ slot) {
+    float m = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float2 p = P[i];
+        m = fmaxf(m, p.x * p.x + p.y * p.y);
+    }
+    max_abs2(slot, m);
+}
+
+// per LED of the batch (blockIdx.y): max |sub|^2 over its whole h x h crop of the box
+__global__ void __launch_bounds__(256) k_crop_abs2_max(const float2 *__restrict__ Sbox,
+                                                        const int2 *__restrict__ led, BatchGeom g,
+                                                        unsigned *__restrict__ slots) {
+    const int l = blockIdx.y;
+    const int2 ab = led_box_offset(led, l, g);
+    const int n = g.h * g.h;
+    float m = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int r = i % g.h, c = i / g.h;
+        const float2 v = Sbox[(size_t)box_index(ab.y, c, g.H) * g.rspan + box_index(ab.x, r, g.H)];
+        m = fmaxf(m, v.x * v.x + v.y * v.y);
+    }
+    max_abs2(&slots[l], m);
+}
+
+// object term: Pt = conj(P) / H^2 (row-major) over max|P|^2 (ePIE) or (|P|^2 + 1e-5) (tPIE)
+__global__ void __launch_bounds__(256) k_pie_object_weights(float2 *__restrict__ Pt, int n,
+                                                             float H2, int pie,
+                                                             const unsigned *__restrict__ scratch) {
+    const float pmax = __uint_as_float(scratch[0]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float2 w = Pt[i];
+        float den = pmax;
+        if (pie == 2) {   // |P|^2 from conj(P) / H^2: H^2 is a power of two, so exactly
+            const float ax = w.x * H2, ay = w.y * H2;
+            den = ax * ax + ay * ay + 1e-5f;
+        }
+        Pt[i] = make_float2(w.x / den, w.y / den);
+    }
+}
+
+cudaError_t launch_pie_prepare(const BatchGeom &g, const float2 *P, const int2 *led,
+                               const float2 *Sbox, unsigned *scratch, cudaStream_t st) {
+    if (g.pie != 1) return cudaSuccess;   // tPIE needs no reductions
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned) * (1 + g.nb), st);
+    if (e != cudaSuccess) return e;
+    const int n = g.h * g.h;
+    const int gx = std::min((n + 255) / 256, kB200SMs * 4);
+    k_pupil_abs2_max<<<gx, 256, 0, st>>>(P, n, scratch);
+    k_crop_abs2_max<<<dim3(std::min((n + 255) / 256, 64), g.nb), 256, 0, st>>>(Sbox, led, g,
+                                                                             scratch + 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pie_object_weights(const BatchGeom &g, float2 *Pt, const unsigned *scratch,
+                                      cudaStream_t st) {
+    if (g.pie == 0) return cudaSuccess;
+    const int n = g.h * g.h;
+    const int gx = std::min((n + 255) / 256, kB200SMs * 8);
+    k_pie_object_weights<<<gx, 256, 0, st>>>(Pt, n, (float)((double)g.H * g.H), g.pie, scratch);
     return cudaGetLastError();
 }
 

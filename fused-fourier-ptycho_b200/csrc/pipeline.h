@@ -25,6 +25,8 @@ struct BatchGeom {
     // the per-LED field buffer already holds zeros in the crop columns outside
     // [pc_lo, pc_hi) (cleared once per solve), so L1 writes only the supported columns
     int t1_clean = 0;
+    // weights of the gradient terms (fpm_pie_weights): 0 none, 1 ePIE, 2 tPIE
+    int pie = 0;
 };
 
 // Two-level twiddle tables (fft_core.cuh) for the low-res length h and the large length H.
@@ -64,8 +66,16 @@ cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_page
 // L4 over src (T1 after separate L2, L3; T2 after the fused pass) -> Xs
 cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs b, int l0,
                                int nl, const Twiddles &tw, cudaStream_t st);
+// ePIE / tPIE weights of the gradient terms (fpm_forward_GPU.m:64-76).  scratch: 1 + nb
+// unsigned, zeroed by launch_pie_prepare; [0] max|P|^2, [1 + l] max|sub_l|^2 (float bits)
+cudaError_t launch_pie_prepare(const BatchGeom &g, const float2 *P, const int2 *led,
+                               const float2 *Sbox, unsigned *scratch, cudaStream_t st);
+// Pt (row-major conj(P)/H^2) times the object-term weight of g.pie
+cudaError_t launch_pie_object_weights(const BatchGeom &g, float2 *Pt, const unsigned *scratch,
+                                      cudaStream_t st);
 cudaError_t launch_lr_pupil_grad(const BatchGeom &g, const int2 *led, BatchBufs b, float2 *dP,
-                                 cudaStream_t st);
+                                 cudaStream_t st,
+                                 const unsigned *pie_scratch = nullptr);
 
 // Pass A: gradient spectrum rows of the box -> inverse FFT along the rows ->
 // Ur [rspan][H] (row-major).  Pt is the conjugated pupil transposed to row-major

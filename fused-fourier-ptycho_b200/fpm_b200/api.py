@@ -34,6 +34,8 @@ MEM_HOST, MEM_DEVICE = 0, 1
 STACK_F32, STACK_U16 = 0, 1
 LOSS_ANISOTROPIC, LOSS_ISOTROPIC = 0, 1
 _LOSS = {"anisotropic": LOSS_ANISOTROPIC, "isotropic": LOSS_ISOTROPIC}
+PIE_NONE, PIE_EPIE, PIE_TPIE = 0, 1, 2
+_PIE = {"none": PIE_NONE, "ePIE": PIE_EPIE, "tPIE": PIE_TPIE}
 
 # Every symbol include/fpm.h declares.
 EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_stack",
@@ -85,7 +87,8 @@ class Problem(C.Structure):
                 ("lr_decay", C.c_float), ("loss_kind", C.c_int32), ("memory", C.c_int32),
                 ("stack_type", C.c_int32),
                 ("stack", C.c_void_p), ("led_idx", C.c_void_p), ("pupil_init", C.c_void_p),
-                ("pupil_amp", C.c_void_p), ("object_init", C.c_void_p)]
+                ("pupil_amp", C.c_void_p), ("object_init", C.c_void_p),
+                ("pie_weights", C.c_int32), ("reserved0", C.c_int32)]
 
 
 class StageTime(C.Structure):
@@ -251,7 +254,7 @@ class Engine:
 
     # -- MATLAB-shaped entry points --------------------------------------------
     def _problem(self, O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr, beta, eps, am,
-                 lr_halve_after, lr_decay, loss="anisotropic"):
+                 lr_halve_after, lr_decay, loss="anisotropic", pie="none"):
         keep = []
         y_is_u16 = (str(getattr(Y, "dtype", "")).endswith("uint16"))
         ydt = np.uint16 if y_is_u16 else np.float32
@@ -277,16 +280,17 @@ class Engine:
                        lr=lr, beta=beta, eps=eps, pupil_margin=am, lr_halve_after=lr_halve_after,
                        lr_decay=lr_decay, loss_kind=_LOSS[loss], memory=ymem,
                        stack_type=STACK_U16 if y_is_u16 else STACK_F32, stack=ys, led_idx=ls,
-                       pupil_init=ps, pupil_amp=as_, object_init=os_)
+                       pupil_init=ps, pupil_amp=as_, object_init=os_, pie_weights=_PIE[pie])
         return prob, keep, ymem
 
     def solve(self, O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr=5e-4, beta=0.999,
               eps=1e-4, am=0.2, lr_halve_after=12, lr_decay=0.5, spectrum=True,
-              loss="anisotropic"):
+              loss="anisotropic", pie="none"):
         """Full reconstruction; returns dict(object, pupil, spectrum, loss) in MATLAB order.
-        loss: "anisotropic" (the v3 mex) or "isotropic" (ret_loss.m)."""
+        loss: "anisotropic" (the v3 mex) or "isotropic" (ret_loss.m); pie: "none" (the v3
+        mex), "ePIE" or "tPIE" (the deconv_pie weights of fpm_forward_GPU.m)."""
         prob, keep, mem = self._problem(O0, P0c, Y, led_idx, P0, pratio, epochs, batch, lr,
-                                        beta, eps, am, lr_halve_after, lr_decay, loss)
+                                        beta, eps, am, lr_halve_after, lr_decay, loss, pie)
         h = prob.h
         H = h * prob.pratio
         like = Y if mem == MEM_DEVICE else None
@@ -302,10 +306,10 @@ class Engine:
         del keep
         return {"object": o, "pupil": p, "spectrum": s, "loss": loss[: int(epochs)]}
 
-    def batch_gradients(self, O, P, Y, led_idx, P0, pratio, loss="anisotropic"):
+    def batch_gradients(self, O, P, Y, led_idx, P0, pratio, loss="anisotropic", pie="none"):
         """v3 gradients of one LED batch (the fullyfusedFPM contract): (dO, dP, loss)."""
         prob, keep, mem = self._problem(O, P, Y, led_idx, P0, pratio, 0, 1, 0.0, 0.0, 0.0, 0.0,
-                                        12, 0.5, loss)
+                                        12, 0.5, loss, pie)
         h = prob.h
         H = h * prob.pratio
         like = Y if mem == MEM_DEVICE else None

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define FPM_ABI_VERSION 1
+#define FPM_ABI_VERSION 2
 
 typedef enum fpm_status {
     FPM_OK = 0,
@@ -80,6 +80,18 @@ typedef enum fpm_loss_kind {
     FPM_LOSS_ISOTROPIC = 1
 } fpm_loss_kind;
 
+/* Weights of the two gradient terms, the `type` of deconv_pie in the reference's
+   conventional MATLAB gradient (benchmark/func_ware/fpm_forward_GPU.m:48,60,64-76),
+   applied to the gradients of the v3 mex: object term conj(P) X / H^2, pupil term
+   sum_l conj(sub_l) X_l. */
+typedef enum fpm_pie_weights {
+    FPM_PIE_NONE = 0,  /* 'none': the v3 mex's gradients */
+    FPM_PIE_EPIE = 1,  /* 'ePIE': object term / max|P|^2, each pupil term / max|sub_l|^2
+                          over the LED's whole crop (disables pupil-support pruning) */
+    FPM_PIE_TPIE = 2   /* 'tPIE': object term / (|P|^2 + 1e-5), pupil term
+                          / (|sub_l|^2 + 1e-5), per pixel */
+} fpm_pie_weights;
+
 typedef struct fpm_device_opts {
     int32_t device;          /* CUDA device ordinal */
     int32_t reserved0;
@@ -112,6 +124,8 @@ typedef struct fpm_problem {
     const float *object_init;/* complex H*H initial object O0 (prhs[0]); NULL = bicubic
                                 up-sampling of stack page 0 with zero phase
                                 (codes_v2/main_run_FPM.m:48) */
+    int32_t pie_weights;     /* fpm_pie_weights; FPM_PIE_NONE for the mex's behaviour */
+    int32_t reserved0;
 } fpm_problem;
 
 /* Outputs.  Any pointer may be NULL to skip that output.  Pointers follow the

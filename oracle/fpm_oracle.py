@@ -206,15 +206,33 @@ def pupil_clamp(w, P0, am, dtype):
 # one LED batch (cuFPM_pure_v3.cu:135-199)
 # ---------------------------------------------------------------------------
 
+def _deconv_pie(x, ker, pie: str, dtype):
+    """``deconv_pie(in, ker, type)`` (benchmark/func_ware/fpm_forward_GPU.m:64-76) for
+    'none', 'ePIE' and 'tPIE': ``conj(ker) .* in`` divided by 1, ``max(max(abs(ker).^2))`` or
+    ``abs(ker).^2 + 1e-5``."""
+    num = np.conj(ker) * x
+    if pie == "none":
+        return num
+    k2 = (ker.real.astype(dtype) ** 2 + ker.imag.astype(dtype) ** 2).astype(dtype)
+    if pie == "ePIE":
+        return num / k2.max()
+    if pie == "tPIE":
+        return num / (k2 + dtype(1e-5))
+    raise ValueError(pie)
+
+
 def batch_gradients(S, P, Y_b, leds_b, pratio: int, dtype, workers: int = 1,
-                    loss_kind: str = "anisotropic"):
+                    loss_kind: str = "anisotropic", pie: str = "none"):
     """Gradients of one LED batch at the current object spectrum ``S``.
 
     ``S`` is the *un-shifted* FFT2 of the object (``cuFPM_pure_v3.cu:135-140``).
     Returns ``(G, dP, loss)`` where ``G`` is the un-shifted gradient spectrum
     already divided by ``H²`` (``kernels.cuh:114-116``), ``dP`` the pupil
     gradient (``kernels.cuh:118-128``, no normalisation) and ``loss`` the
-    feature-domain loss of the batch.
+    feature-domain loss of the batch.  ``pie`` weighs the two terms as ``deconv_pie``
+    of ``benchmark/func_ware/fpm_forward_GPU.m:64-76`` does ('ePIE': over max|ker|^2 of
+    the whole kernel, 'tPIE': over |ker|^2 + 1e-5 per pixel; ker = P for the object term,
+    the LED's crop for the pupil term).
     """
     ctype = np.complex64 if dtype == np.float32 else np.complex128
     H = S.shape[0]
@@ -239,8 +257,8 @@ def batch_gradients(S, P, Y_b, leds_b, pratio: int, dtype, workers: int = 1,
         # K5: unnormalised forward FFT (cuFPM_pure_v3.cu:164-169), read shifted
         X = shift_half(_fft2(rec, workers).astype(ctype, copy=False))
         # K7: G += conj(P)·X / H² at the crop; dP += conj(sub)·X (kernels.cuh:95-128)
-        G[np.ix_(rr, cc)] += (np.conj(P) * X) * inv_H2
-        dP += np.conj(sub) * X
+        G[np.ix_(rr, cc)] += _deconv_pie(X, P, pie, dtype) * inv_H2
+        dP += _deconv_pie(X, sub, pie, dtype)
     return G, dP, loss
 
 
@@ -261,7 +279,7 @@ class OracleResult:
 def cufpm_pure_v3(O0, P0c, Y, led_idx, P0, pratio: int, epochs: int, batch: int,
                   opt=(5e-4, 0.999, 1e-4), am: float = 0.2, lr_halve_after: int = 12,
                   dtype=np.float64, workers: int | None = None,
-                  loss_kind: str = "anisotropic") -> OracleResult:
+                  loss_kind: str = "anisotropic", pie: str = "none") -> OracleResult:
     """Oracle of ``[O, P] = cuFPM_pure_v3(O0, P0c, Y, ledIdx, P0, pratio, epochs, B, [lr beta eps])``.
 
     ``Y`` is ``(L, h, h)`` amplitude (page ``l`` = LED ``l``, the reference's
@@ -269,7 +287,8 @@ def cufpm_pure_v3(O0, P0c, Y, led_idx, P0, pratio: int, epochs: int, batch: int,
     hyper-parameters are rounded to float32 first, as the mex does
     (``cuFPM_pure_v3.cu:63-65``).  Returns the object, pupil, the centred
     spectrum ``fftshift(fft2(O))`` and the per-epoch loss.  ``loss_kind``
-    "isotropic" swaps the v3 loss for :func:`feature_grad_isotropic`.
+    "isotropic" swaps the v3 loss for :func:`feature_grad_isotropic`; ``pie`` weighs
+    the gradient terms (:func:`batch_gradients`).
     """
     if workers is None:
         workers = default_workers()
@@ -294,7 +313,7 @@ def cufpm_pure_v3(O0, P0c, Y, led_idx, P0, pratio: int, epochs: int, batch: int,
             nb = min(batch, L - cur)
             S = _fft2(O, workers).astype(ctype, copy=False)
             G, dP, lv = batch_gradients(S, P, Y[cur:cur + nb], led_idx[cur:cur + nb],
-                                        pratio, dtype, workers, loss_kind)
+                                        pratio, dtype, workers, loss_kind, pie)
             losses[ep] += lv
             # K8: unnormalised inverse FFT of G (the 1/H² is already inside G)
             g = (_ifft2(G, workers) * ctype(H * H)).astype(ctype, copy=False)

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = fpm_b200.load_library()
-    assert lib.fpm_abi_version() == 1
+    assert lib.fpm_abi_version() == 2
     assert lib.fpm_status_string(0) == b"ok"
     assert lib.fpm_status_string(3) == b"out of device memory"
     assert lib.fpm_status_string(99) == b"unknown status"
@@ -58,7 +58,7 @@ int main(void) {
   F(fpm_problem, pupil_margin) F(fpm_problem, lr_halve_after) F(fpm_problem, lr_decay)
   F(fpm_problem, loss_kind) F(fpm_problem, memory) F(fpm_problem, stack_type)
   F(fpm_problem, stack) F(fpm_problem, led_idx) F(fpm_problem, pupil_init)
-  F(fpm_problem, pupil_amp) F(fpm_problem, object_init)
+  F(fpm_problem, pupil_amp) F(fpm_problem, object_init) F(fpm_problem, pie_weights)
   F(fpm_result, object) F(fpm_result, spectrum) F(fpm_result, pupil) F(fpm_result, loss)
   F(fpm_device_opts, device) F(fpm_device_opts, mem_limit_bytes) F(fpm_device_opts, stream)
   F(fpm_led_geometry, grid) F(fpm_led_geometry, h) F(fpm_led_geometry, pratio)

@@ -588,3 +588,47 @@ def test_large_lowres_side_two_pass_rows_vs_oracle(engine):
         e, e32 = orc.rel_err(r[k], getattr(o, k)), orc.rel_err(getattr(o32, k), getattr(o, k))
         assert e < max(TIGHT, 3 * e32), (k, e, e32)
     np.testing.assert_allclose(r["loss"], o.loss, rtol=1e-5)
+
+
+@pytest.mark.parametrize("pie", ["ePIE", "tPIE"])
+def test_pie_weights_gradients_and_solve(engine, ds_small, ds_a, pie):
+    """The deconv_pie weights of the conventional MATLAB gradient (fpm_forward_GPU.m:64-76)
+    on the v3 gradient terms, against the FP64 oracle: gradients of one batch (whole
+    crops) and a two-epoch solve (pruned to the pupil support for tPIE, whole crops for
+    ePIE), with the isotropic loss so that no sign decision separates the FP32 engine from
+    the oracle."""
+    for ds in (ds_small, ds_a):
+        H = ds.h * ds.pratio
+        rng = np.random.default_rng(33)
+        O = (ds.O0 * np.exp(1j * 0.2 * rng.standard_normal((H, H)))).astype(np.complex64)
+        P = ds.pupil_true
+        sel = slice(0, 9)
+        dO, dP, loss = engine.batch_gradients(O, P, to_matlab_stack(ds.Y[sel]),
+                                              led_matlab(ds.led_idx[sel]), ds.pupil0, ds.pratio,
+                                              loss="isotropic", pie=pie)
+        G, dP64, l64 = orc.batch_gradients(np.fft.fft2(O.astype(np.complex128)),
+                                           P.astype(np.complex128), ds.Y[sel].astype(np.float64),
+                                           ds.led_idx[sel], ds.pratio, np.float64,
+                                           loss_kind="isotropic", pie=pie)
+        # tPIE divides by |ker|^2 + 1e-5 pixel by pixel, which magnifies the rounding of
+        # small spectrum values: the bar is the FP32 oracle twin's own distance
+        G32, dP32, _ = orc.batch_gradients(np.fft.fft2(O), P.astype(np.complex64),
+                                           ds.Y[sel].astype(np.float32), ds.led_idx[sel],
+                                           ds.pratio, np.float32, loss_kind="isotropic", pie=pie)
+        bar_o = max(TIGHT, 3 * orc.rel_err(np.fft.ifft2(G32.astype(np.complex128)), np.fft.ifft2(G)))
+        bar_p = max(TIGHT, 3 * orc.rel_err(dP32, dP64))
+        assert abs(loss - l64) < 1e-6 * abs(l64)
+        e_o = orc.rel_err(dO, np.fft.ifft2(G) * H * H)
+        assert e_o < bar_o, (e_o, bar_o)
+        assert orc.rel_err(dP, dP64) < bar_p, (orc.rel_err(dP, dP64), bar_p)
+        opt = (1e-3, 0.999, 1e-4)
+        r = engine.solve(ds.O0, ds.P0c, to_matlab_stack(ds.Y[:16]), led_matlab(ds.led_idx[:16]),
+                         ds.pupil0, ds.pratio, 2, 8, lr=opt[0], beta=opt[1], eps=opt[2],
+                         loss="isotropic", pie=pie)
+        args = (ds.O0, ds.P0c, ds.Y[:16], ds.led_idx[:16], ds.pupil0, ds.pratio, 2, 8)
+        o = orc.cufpm_pure_v3(*args, opt=opt, loss_kind="isotropic", pie=pie)
+        o32 = orc.cufpm_pure_v3(*args, opt=opt, loss_kind="isotropic", pie=pie, dtype=np.float32)
+        for k in ("object", "pupil"):
+            e, e32 = orc.rel_err(r[k], getattr(o, k)), orc.rel_err(getattr(o32, k), getattr(o, k))
+            assert e < max(TIGHT, 3 * e32), (k, e, e32)
+        np.testing.assert_allclose(r["loss"], o.loss, rtol=1e-6)

@@ -303,3 +303,17 @@ def test_oracle_tracks_reference_solver(name):
                           workers=1)
     assert orc.rel_err(g["ref_object"], r.object) < float(g["tol"])
     assert orc.rel_err(g["ref_pupil"], r.pupil) < float(g["tol"])
+
+
+def test_deconv_pie_weights_match_the_matlab_statements():
+    """deconv_pie (benchmark/func_ware/fpm_forward_GPU.m:64-76) as the oracle restates it."""
+    g = np.random.default_rng(12)
+    x = (g.standard_normal((3, 8, 8)) + 1j * g.standard_normal((3, 8, 8)))
+    ker = (g.standard_normal((3, 8, 8)) + 1j * g.standard_normal((3, 8, 8)))
+    for l in range(3):
+        np.testing.assert_allclose(orc._deconv_pie(x[l], ker[l], "none", np.float64),
+                                   np.conj(ker[l]) * x[l])
+        np.testing.assert_allclose(orc._deconv_pie(x[l], ker[l], "ePIE", np.float64),
+                                   np.conj(ker[l]) * x[l] / np.max(np.abs(ker[l]) ** 2))
+        np.testing.assert_allclose(orc._deconv_pie(x[l], ker[l], "tPIE", np.float64),
+                                   np.conj(ker[l]) * x[l] / (np.abs(ker[l]) ** 2 + 1e-5))
