@@ -11,11 +11,16 @@
 //                  [--row0 0 --col0 0] [--tiff-type u16|f32])
 //                 --led ledIdx.i32 --pupil P0c.c64 --pupil-amp P0.f32 [--object O0.c64]
 //                 [--lr 5e-4 --beta 0.999 --eps 1e-4 --margin 0.2]
+//                 [--loss anisotropic|isotropic] [--pie none|ePIE|tPIE]
 //                 [--out-object O.c64] [--out-spectrum S.c64] [--out-pupil P.c64]
 //                 [--out-loss loss.f64] [--device 0] [--profile]
 //
 //   fpm_cli ingest --tiff-list frames.txt --h 2048 [--row0 0 --col0 0]
 //                  [--tiff-type u16|f32] --out Y.u16
+//
+//   fpm_cli leds --grid 19 --h 2048 --pratio 8 --wavelength 0.532 --pitch 4000
+//                --height 90000 --pixel 6.5 --mag 4 --out-led ledIdx.i32
+//                [--out-frames frames.txt --frames-dir raw_images/green]
 //
 // A frame list is a text file naming one TIFF per line, in LED order (the
 // reference loads raw_images/<colour>/<k>.tif in its spiral order,
@@ -47,11 +52,15 @@ int usage(const char *msg) {
                  "                      --tiff-list FILE [--row0 R --col0 C] [--tiff-type u16|f32])\n"
                  "                     --led FILE --pupil FILE --pupil-amp FILE [--object FILE]\n"
                  "                     [--lr X --beta X --eps X --margin X]\n"
+                 "                     [--loss anisotropic|isotropic] [--pie none|ePIE|tPIE]\n"
                  "                     [--out-object FILE] [--out-spectrum FILE]\n"
                  "                     [--out-pupil FILE] [--out-loss FILE]\n"
                  "                     [--device D] [--profile]\n"
                  "       fpm_cli ingest --tiff-list FILE --h N [--row0 R --col0 C]\n"
-                 "                      [--tiff-type u16|f32] --out FILE\n");
+                 "                      [--tiff-type u16|f32] --out FILE\n"
+                 "       fpm_cli leds --grid G --h N --pratio P --wavelength UM --pitch UM\n"
+                 "                    --height UM --pixel UM --mag M [--dx UM --dy UM]\n"
+                 "                    --out-led FILE [--out-frames FILE --frames-dir DIR]\n");
     return 2;
 }
 
@@ -214,7 +223,12 @@ int cmd_solve(const Options &opt, bool profile) {
     pr.pupil_margin = (float)num(opt, "margin", 0.2);
     pr.lr_halve_after = 12;
     pr.lr_decay = 0.5f;
-    pr.loss_kind = FPM_LOSS_ANISOTROPIC;
+    const std::string lk = need("loss") ? *need("loss") : "anisotropic";
+    if (lk != "anisotropic" && lk != "isotropic") return usage("--loss is anisotropic or isotropic");
+    pr.loss_kind = lk == "isotropic" ? FPM_LOSS_ISOTROPIC : FPM_LOSS_ANISOTROPIC;
+    const std::string pie = need("pie") ? *need("pie") : "none";
+    if (pie != "none" && pie != "ePIE" && pie != "tPIE") return usage("--pie is none, ePIE or tPIE");
+    pr.pie_weights = pie == "ePIE" ? FPM_PIE_EPIE : pie == "tPIE" ? FPM_PIE_TPIE : FPM_PIE_NONE;
     pr.memory = FPM_MEM_HOST;
     pr.stack_type = u16 ? FPM_STACK_U16_COUNTS : FPM_STACK_F32_AMPLITUDE;
     pr.stack = stack.data();
@@ -278,12 +292,66 @@ int cmd_solve(const Options &opt, bool profile) {
     return ok ? 0 : 2;
 }
 
+// LED crop corners of a square LED array (fpm_led_indices), written as the ledIdx file
+// of `solve`, and optionally the frame list of the reference's file naming: in LED
+// order, <dir>/<k>.tif with k = j + (i - 1) grid (codes_v2/main_run_FPM.m:33-35).
+int cmd_leds(const Options &opt) {
+    for (const char *k : {"grid", "h", "pratio", "wavelength", "pitch", "height", "pixel", "mag",
+                          "out-led"})
+        if (!find(opt, k)) return usage((std::string("missing --") + k).c_str());
+    fpm_led_geometry geo;
+    std::memset(&geo, 0, sizeof(geo));
+    geo.grid = (int32_t)num(opt, "grid", 0);
+    geo.h = (int32_t)num(opt, "h", 0);
+    geo.pratio = (int32_t)num(opt, "pratio", 0);
+    geo.wavelength_um = num(opt, "wavelength", 0);
+    geo.led_pitch_um = num(opt, "pitch", 0);
+    geo.led_height_um = num(opt, "height", 0);
+    geo.camera_pixel_um = num(opt, "pixel", 0);
+    geo.magnification = num(opt, "mag", 0);
+    geo.sample_dx_um = num(opt, "dx", -0.0);
+    geo.sample_dy_um = num(opt, "dy", -0.0);
+    if (geo.grid <= 0 || geo.grid > 255) return usage("--grid is 1..255");
+    const size_t L = (size_t)geo.grid * geo.grid;
+    std::vector<int32_t> led(2 * L), pos(2 * L);
+    fpm_device_opts dopt;
+    std::memset(&dopt, 0, sizeof(dopt));
+    dopt.device = (int32_t)num(opt, "device", 0);
+    fpm_context *ctx = nullptr;
+    fpm_status rc = fpm_create(&ctx, &dopt);
+    if (rc != FPM_OK) {
+        std::fprintf(stderr, "fpm_cli: %s\n", fpm_status_string(rc));
+        return 3 + (int)rc;
+    }
+    rc = fpm_led_indices(ctx, &geo, led.data(), pos.data());
+    if (rc != FPM_OK) {
+        std::fprintf(stderr, "fpm_cli: %s: %s\n", fpm_status_string(rc), fpm_last_error(ctx));
+        fpm_destroy(ctx);
+        return 3 + (int)rc;
+    }
+    fpm_destroy(ctx);
+    if (!write_file(*find(opt, "out-led"), led.data(), led.size() * sizeof(int32_t))) return 2;
+    if (const std::string *fl = find(opt, "out-frames")) {
+        const std::string dir = find(opt, "frames-dir") ? *find(opt, "frames-dir") : ".";
+        std::string text;
+        char name[32];
+        for (size_t l = 0; l < L; ++l) {
+            const int k = pos[2 * l + 1] + (pos[2 * l] - 1) * geo.grid;
+            std::snprintf(name, sizeof name, "%03d.tif", k);
+            text += dir + "/" + name + "\n";
+        }
+        if (!write_file(*fl, text.data(), text.size())) return 2;
+    }
+    std::printf("leds: %zu LEDs of a %d x %d array\n", L, geo.grid, geo.grid);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
     if (argc < 2) return usage(nullptr);
     const std::string cmd = argv[1];
-    if (cmd != "solve" && cmd != "ingest") return usage("unknown command");
+    if (cmd != "solve" && cmd != "ingest" && cmd != "leds") return usage("unknown command");
     Options opt;
     bool profile = false;
     for (int i = 2; i < argc; ++i) {
@@ -295,5 +363,6 @@ int main(int argc, char **argv) {
         if (k.rfind("--", 0) != 0 || i + 1 >= argc) return usage(("bad argument " + k).c_str());
         opt[k.substr(2)] = argv[++i];
     }
+    if (cmd == "leds") return cmd_leds(opt);
     return cmd == "solve" ? cmd_solve(opt, profile) : cmd_ingest(opt);
 }

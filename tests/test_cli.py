@@ -108,3 +108,51 @@ def test_cli_solve_from_tiff_frames_equals_library_solve(tmp_path, engine):
     ref = engine.solve(None, ds.P0c, to_matlab_stack(ds.raw[:L]), led_matlab(ds.led_idx[:L]),
                        ds.pupil0, 4, E, B)
     np.testing.assert_array_equal(O, ref["object"])
+
+
+def test_cli_leds_usage_and_no_device(tmp_path):
+    r = run("leds", "--grid", 5, "--h", 64)
+    assert r.returncode == 2 and "missing --pratio" in r.stderr
+    args = ["leds", "--grid", 5, "--h", 64, "--pratio", 4, "--wavelength", 0.532, "--pitch", 4000,
+            "--height", 90000, "--pixel", 6.5, "--mag", 4, "--out-led", tmp_path / "l.i32"]
+    r = run(*args[:2], 300, *args[3:])
+    assert r.returncode == 2 and "--grid" in r.stderr
+    if not has_gpu():
+        r = run(*args)
+        assert r.returncode == 3 + 6                      # FPM_ERR_NO_DEVICE
+
+
+@pytest.mark.gpu
+def test_cli_leds_equals_library_geometry(tmp_path, engine):
+    from fpm_b200 import frames
+    geo = dict(grid=7, h=256, pratio=4, wavelength_um=0.532, led_pitch_um=4000.0,
+               led_height_um=90000.0, camera_pixel_um=6.5, magnification=4.0)
+    r = run("leds", "--grid", 7, "--h", 256, "--pratio", 4, "--wavelength", 0.532, "--pitch", 4000,
+            "--height", 90000, "--pixel", 6.5, "--mag", 4, "--out-led", tmp_path / "l.i32",
+            "--out-frames", tmp_path / "f.txt", "--frames-dir", "raw_images/green")
+    assert r.returncode == 0, r.stderr
+    led, order = engine.led_indices(geo["grid"], geo["h"], geo["pratio"], geo["wavelength_um"],
+                                    geo["led_pitch_um"], geo["led_height_um"],
+                                    geo["camera_pixel_um"], geo["magnification"])
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "l.i32", "<i4").reshape(-1, 2), led)
+    names = (tmp_path / "f.txt").read_text().split()
+    assert names == [str(p) for p in frames.frame_paths("raw_images/green", order, 7)]
+
+
+@pytest.mark.gpu
+def test_cli_loss_and_weights_options_equal_library(tmp_path, engine):
+    ds = dataset(64, 4, 5, seed=3, aberration=True)
+    L = 12
+    f = _inputs(tmp_path, ds, L)
+    out = tmp_path / "O.c64"
+    r = run("solve", "--h", 64, "--leds", L, "--pratio", 4, "--batch", 6, "--epochs", 1,
+            "--loss", "isotropic", "--pie", "tPIE", "--out-object", out,
+            *sum(([f"--{k}", v] for k, v in f.items()), []))
+    assert r.returncode == 0, r.stderr
+    O = np.fromfile(out, np.complex64).reshape(256, 256).T
+    ref = engine.solve(None, ds.P0c, to_matlab_stack(ds.raw[:L]), led_matlab(ds.led_idx[:L]),
+                       ds.pupil0, 4, 1, 6, loss="isotropic", pie="tPIE")
+    np.testing.assert_array_equal(O, ref["object"])
+    bad = run("solve", "--h", 64, "--leds", L, "--pratio", 4, "--batch", 6, "--epochs", 1,
+              "--pie", "rPIE", *sum(([f"--{k}", v] for k, v in f.items()), []))
+    assert bad.returncode == 2 and "--pie" in bad.stderr
