@@ -32,6 +32,23 @@ def led_matlab(led):
     return np.ascontiguousarray(np.asarray(led, np.int32).T)
 
 
+def torch_forward_model(O, P, led, pratio):
+    """Checker for sizes the FP64 oracle cannot reach: the forward model of
+    benchmark/gen_img_batch.m:178-201 in plain torch complex64 (amplitudes), on
+    whatever device O lives.  O (H, H) and P (h, h) complex tensors, led (L, 2) rows
+    (kl, kt) 1-based; returns (L, h, h) [l, r, c]."""
+    import torch
+    H, h = O.shape[0], P.shape[0]
+    F = torch.fft.fftshift(torch.fft.fft2(O))
+    ar = torch.arange(h, device=O.device)
+    out = []
+    for kl, kt in np.asarray(led):
+        rows, cols = (int(kt) - 1 + ar) % H, (int(kl) - 1 + ar) % H
+        sub = F.index_select(0, rows).index_select(1, cols) * P
+        out.append(torch.fft.ifft2(torch.fft.ifftshift(sub)).abs() / (pratio * pratio))
+    return torch.stack(out)
+
+
 _CACHE = {}
 
 

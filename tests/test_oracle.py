@@ -255,6 +255,24 @@ def test_forward_model_matches_generator_statements():
                                rtol=1e-12)
 
 
+def test_torch_forward_model_checker_matches_oracle():
+    """The torch complex64 forward model that checks the device simulator at sizes the
+    FP64 oracle cannot reach agrees with the oracle (crops inside and past the edge)."""
+    import torch
+    from conftest import torch_forward_model
+    rng = np.random.default_rng(8)
+    h, p = 64, 4
+    H = h * p
+    O = np.exp(1j * 0.3 * rng.standard_normal((H, H)))
+    P = synth.pupil_circle(h, synth.Optics(led_grid=3)) * np.exp(0.2j * rng.standard_normal((h, h)))
+    led = np.array([[90, 97], [1, 1], [H - 20, 30], [H, H]], np.int32)
+    ref = orc.forward_model(O, P, led, p, amplitude=True)
+    got = torch_forward_model(torch.from_numpy(O.astype(np.complex64)),
+                              torch.from_numpy(P.astype(np.complex64)), led, p).numpy()
+    for l in range(len(led)):
+        assert orc.rel_err(got[l], ref[l]) < 2e-6, l
+
+
 def test_bicubic_restatements_agree_and_keep_constants():
     rng = np.random.default_rng(7)
     img = rng.random((12, 12))
