@@ -15,7 +15,7 @@ Tolerances (relative L2 error, complex, no phase alignment):
 import numpy as np
 import pytest
 
-from conftest import led_matlab, to_matlab_stack, dataset
+from conftest import led_matlab, to_matlab_stack, dataset, torch_forward_model
 from oracle import fpm_oracle as orc
 import fpm_b200
 
@@ -632,3 +632,45 @@ def test_pie_weights_gradients_and_solve(engine, ds_small, ds_a, pie):
             e, e32 = orc.rel_err(r[k], getattr(o, k)), orc.rel_err(getattr(o32, k), getattr(o, k))
             assert e < max(TIGHT, 3 * e32), (k, e, e32)
         np.testing.assert_allclose(r["loss"], o.loss, rtol=1e-6)
+
+
+def test_full_size_forward_model_and_zero_residual(engine):
+    """At the bench's size (2048² frames, pratio 8 -> a 16384² object), where the FP64
+    oracle is too slow, two size-independent properties:
+    (1) the device forward model (benchmark/gen_img_batch.m:178-201) equals a plain torch
+        complex64 restatement of it (cuFFT) to 2e-5 relative L2 per LED, crops inside
+        and past the spectrum edge;
+    (2) frames simulated from (O, P) are explained by (O, P): the batch loss there is
+        below 1e-3 of the loss at the same object with 0.05 rad of phase noise added."""
+    import torch
+    from fpm_b200 import synth
+    h, p = 2048, 8
+    H = h * p
+    optics = synth.Optics(led_grid=3)
+    led = np.concatenate([synth.led_indices(h, p, optics)[:5],
+                          np.array([[H - h // 2, 3]])]).astype(np.int32)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    O = torch.polar(torch.ones((H, H), device="cuda"),
+                    0.2 * torch.randn((H, H), generator=g, device="cuda")).contiguous()
+    circ = synth.pupil_circle(h, optics)
+    ab = np.exp(0.3j * np.random.default_rng(3).standard_normal((h, h)))
+    P = torch.from_numpy((circ * ab).astype(np.complex64)).cuda()
+    ledt = torch.from_numpy(led_matlab(led)).cuda()
+    Y = engine.simulate(O, P, ledt, p, amplitude=True)            # (h, h, L) on the device
+    assert tuple(Y.shape) == (h, h, len(led))
+
+    ref = torch_forward_model(O, P, led, p)                       # (L, h, h), cuFFT
+    for l in range(len(led)):
+        err = (torch.linalg.vector_norm(Y[:, :, l] - ref[l]) / torch.linalg.vector_norm(ref[l])).item()
+        assert err < 2e-5, (l, err)
+    del ref
+
+    P0 = torch.from_numpy(circ).cuda()
+    scalar = lambda x: float(torch.as_tensor(x).reshape(-1)[0])
+    _, _, loss_true = engine.batch_gradients(O, P, Y, ledt, P0, p)
+    noise = torch.polar(torch.ones((H, H), device="cuda"),
+                        0.05 * torch.randn((H, H), generator=g, device="cuda"))
+    _, _, loss_pert = engine.batch_gradients((O * noise).contiguous(), P, Y, ledt, P0, p)
+    assert scalar(loss_pert) > 0
+    assert scalar(loss_true) < 1e-3 * scalar(loss_pert), (scalar(loss_true), scalar(loss_pert))
