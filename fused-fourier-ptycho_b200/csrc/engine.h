@@ -29,7 +29,7 @@ struct Box {
 };
 
 // ---- low-resolution (per-LED) stages -------------------------------------
-int feature_grad_blocks_per_image(int h);
+long long feature_grad_blocks_per_image(int h);
 cudaError_t launch_feature_grad(const float2 *Z, StackView Y, int z_off, int nb, int h,
                                 int pratio, float2 *out, double *loss_part, cudaStream_t st);
 

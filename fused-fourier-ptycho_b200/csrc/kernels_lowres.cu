@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(256) k_feature_grad(const float2 *__restrict__
     }
 }
 
-int feature_grad_blocks_per_image(int h) {
-    const int t = (h + kTR - 1) / kTR;
+long long feature_grad_blocks_per_image(int h) {
+    const long long t = ((long long)h + kTR - 1) / kTR;   // 64-bit: t * t overflows int past h ~ 1.48e6
     return t * t;
 }
 

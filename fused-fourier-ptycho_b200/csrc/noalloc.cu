@@ -69,9 +69,12 @@ extern "C" fpm_status fpm_feature_gradient_noalloc(const float *z, const float *
                                                    float *gradient, double *loss, void *stream) {
     if (!z || !amplitude || !gradient || !loss) return FPM_ERR_INVALID_ARGUMENT;
     if (h < 2 || (h & 1) || n_images < 1 || pratio < 1) return FPM_ERR_INVALID_ARGUMENT;
-    // size limit of the fixed scratch, checked before anything touches the device
+    // size limit of the fixed scratch, checked before anything touches the device; the
+    // side bound keeps the 64-bit tile count and the launch grid far from any overflow
+    // whatever h the caller passes (a single image of 8192^2 already fills the array)
+    if (h > FPM_NOALLOC_MAX_SIDE || n_images > 65535) return FPM_ERR_UNSUPPORTED;
     const long long tiles = (long long)n_images * fpm::feature_grad_blocks_per_image(h);
-    if (tiles > FPM_NOALLOC_MAX_TILES || n_images > 65535) return FPM_ERR_UNSUPPORTED;
+    if (tiles < 1 || tiles > FPM_NOALLOC_MAX_TILES) return FPM_ERR_UNSUPPORTED;
     if (!on_current_device(z) || !on_current_device(amplitude) || !on_current_device(gradient) ||
         !on_current_device(loss))
         return FPM_ERR_INVALID_ARGUMENT;

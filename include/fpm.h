@@ -213,11 +213,13 @@ fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, in
    (512 KiB), held by every GPU that loads the library until exit.  The first
    call on a device looks up its address (cudaGetSymbolAddress, with that device
    current); make that first call before any stream capture.  Limit: n_images *
-   ceil(h/32)^2 <= FPM_NOALLOC_MAX_TILES (e.g. 16 images of 2048^2, 256 of 512^2)
-   and n_images <= 65535, else FPM_ERR_UNSUPPORTED before any device work.  Every
-   call shares the one array: calls whose work overlaps on the GPU (other
-   streams, other host threads) race and must be serialised by the caller. */
+   ceil(h/32)^2 <= FPM_NOALLOC_MAX_TILES (e.g. 16 images of 2048^2, 256 of 512^2),
+   h <= FPM_NOALLOC_MAX_SIDE and n_images <= 65535, else FPM_ERR_UNSUPPORTED
+   before any device work.  Every call shares the one array: calls whose work
+   overlaps on the GPU (other streams, other host threads) race and must be
+   serialised by the caller. */
 #define FPM_NOALLOC_MAX_TILES 65536
+#define FPM_NOALLOC_MAX_SIDE 8192
 fpm_status fpm_feature_gradient_noalloc(const float *z, const float *amplitude, int32_t h,
                                         int32_t n_images, int32_t pratio, float *gradient,
                                         double *loss, void *stream);

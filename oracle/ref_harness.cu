@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <vector>
+
 #include "kernels.cuh"
 
 namespace {
@@ -212,6 +214,155 @@ int ref_gradients(int h, int H, int L, int pratio, const float *O, const float *
     cufftDestroy(planLarge);
     b.free_all();
     return rc;
+}
+
+// Diagnostic twin of ref_solve for locating writes outside a buffer: every device
+// buffer gets a 64 KiB sentinel band before and after it, and after each operation of
+// the first `max_steps` operations of the loop (9 per batch: the forward FFT, the crop,
+// the batched inverse FFT, the loss stencil, the batched forward FFT, the two memsets,
+// the stitch, the inverse FFT, the RMSprop) the stream is synchronised, the number of
+// changed sentinel bytes of each of the 12 buffers is written to guards[step * 12 + i]
+// (order O, P, latentZ, recordZ, subwave, dldw1, dldw2, mom1, mom2, Y, P0, led) and the
+// pupil (complex h x h) to P_trace[step].  Returns the number of steps recorded, or a
+// negative line number on a failed CUDA call.  Reads only; writes nothing outside the
+// buffers it owns.
+int ref_solve_trace(int h, int H, int L, int pratio, int epochs, int batch, float lr, float beta,
+                    float eps, const float *O0, const float *P0c, const float *Y, const int *led,
+                    const float *P0, float *O_out, float *P_out, float *P_trace, int *guards,
+                    int max_steps) {
+    const size_t G = 64 * 1024;
+    const size_t plane = (size_t)h * h, big = (size_t)H * H, arraysize = plane * batch;
+    const size_t sizes[12] = {big * 8, plane * 8, arraysize * 8, arraysize * 8, arraysize * 8,
+                              big * 8, plane * 8, big * 4, plane * 4, plane * L * 4, plane * 4,
+                              (size_t)L * 8};
+    char *base[12] = {};
+    auto release = [&]() {
+        for (char *b : base)
+            if (b) cudaFree(b);
+    };
+#define TCK(x)                 \
+    do {                       \
+        if ((x) != 0) {        \
+            release();         \
+            return -__LINE__;  \
+        }                      \
+    } while (0)
+    for (int i = 0; i < 12; ++i) {
+        TCK(cudaMalloc(&base[i], sizes[i] + 2 * G));
+        TCK(cudaMemset(base[i], 0xA5, G));
+        TCK(cudaMemset(base[i] + G + sizes[i], 0xA5, G));
+    }
+    auto buf = [&](int i) { return static_cast<void *>(base[i] + G); };
+    creal32_t *O = (creal32_t *)buf(0), *P = (creal32_t *)buf(1), *latentZ = (creal32_t *)buf(2),
+              *recordZ = (creal32_t *)buf(3), *subwave = (creal32_t *)buf(4),
+              *dldw1 = (creal32_t *)buf(5), *dldw2 = (creal32_t *)buf(6);
+    real32_T *mom1 = (real32_T *)buf(7), *mom2 = (real32_T *)buf(8), *dY = (real32_T *)buf(9),
+             *dP0 = (real32_T *)buf(10);
+    int2 *dled = (int2 *)buf(11);
+    TCK(cudaMemcpy(O, O0, big * 8, cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(P, P0c, plane * 8, cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(dY, Y, plane * L * 4, cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(dP0, P0, plane * 4, cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(dled, led, (size_t)L * 8, cudaMemcpyHostToDevice));
+    TCK(cudaMemset(mom1, 0, big * 4));
+    TCK(cudaMemset(mom2, 0, plane * 4));
+    dim3 imLs_sz = dims_of(h, h, L);
+    dim3 imHs_sz = dims_of(H, H, 1);
+    dim3 N_THREADS = {BLOCK_X, BLOCK_Y, 1};
+    dim3 N_BLOCKS_L = {(imHs_sz.x + BLOCK_X - 1) / BLOCK_X, (imHs_sz.y + BLOCK_Y - 1) / BLOCK_Y, 1};
+    dim3 N_BLOCKS = {(imLs_sz.x + BLOCK_X - 1) / BLOCK_X, (imLs_sz.y + BLOCK_Y - 1) / BLOCK_Y, 1};
+    const int led_total = (int)imLs_sz.z;
+    int inembed[2] = {(int)imLs_sz.x, (int)imLs_sz.y};
+    imLs_sz.z = batch;
+    cufftHandle planLarge, planBatch;
+    if (cufftPlan2d(&planLarge, imHs_sz.x, imHs_sz.y, CUFFT_C2C) != CUFFT_SUCCESS) {
+        release();
+        return -1;
+    }
+    if (cufftPlanMany(&planBatch, 2, inembed, inembed, 1, (int)plane, inembed, 1, (int)plane,
+                      CUFFT_C2C, batch) != CUFFT_SUCCESS) {
+        cufftDestroy(planLarge);
+        release();
+        return -2;
+    }
+    std::vector<unsigned char> g(G);
+    int step = 0;
+    auto record = [&]() -> int {
+        if (step >= max_steps) return 0;
+        if (cudaDeviceSynchronize() != cudaSuccess) return -__LINE__;
+        for (int i = 0; i < 12; ++i) {
+            int changed = 0;
+            for (int side = 0; side < 2; ++side) {
+                const char *src = side == 0 ? base[i] : base[i] + G + sizes[i];
+                if (cudaMemcpy(g.data(), src, G, cudaMemcpyDeviceToHost) != cudaSuccess)
+                    return -__LINE__;
+                for (size_t k = 0; k < G; ++k) changed += g[k] != 0xA5;
+            }
+            guards[step * 12 + i] = changed;
+        }
+        if (cudaMemcpy(P_trace + (size_t)step * plane * 2, P, plane * 8,
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            return -__LINE__;
+        ++step;
+        return 0;
+    };
+    int rc = 0;
+#define TREC()                                  \
+    do {                                        \
+        rc = record();                          \
+        if (rc) goto done;                      \
+    } while (0)
+    for (int epoch = 0; epoch < epochs; ++epoch) {
+        int remain = led_total, curr = 0;
+        while (remain > 0) {
+            remain -= batch;
+            cufftExecC2C(planLarge, (cufftComplex *)O, (cufftComplex *)dldw1, CUFFT_FORWARD);
+            TREC();
+            N_BLOCKS.z = (unsigned)(min(curr + batch - 1, led_total - 1) - curr + 1);
+            fused_getSubpupil_shifted<<<N_BLOCKS, N_THREADS>>>(curr, dldw1, P, dled, imLs_sz,
+                                                              imHs_sz, subwave, latentZ);
+            TREC();
+            cufftExecC2C(planBatch, (cufftComplex *)latentZ, (cufftComplex *)latentZ,
+                         CUFFT_INVERSE);
+            TREC();
+            differenceKernel_acc<<<N_BLOCKS, N_THREADS>>>(curr, imLs_sz, pratio, dY, latentZ,
+                                                          recordZ);
+            TREC();
+            cufftExecC2C(planBatch, (cufftComplex *)recordZ, (cufftComplex *)latentZ,
+                         CUFFT_FORWARD);
+            TREC();
+            cudaMemset(dldw1, 0, big * 8);
+            cudaMemset(dldw2, 0, plane * 8);
+            TREC();
+            fused_deconvPIE_shifted<<<N_BLOCKS, N_THREADS>>>(curr, latentZ, subwave, dled, P,
+                                                             imLs_sz, imHs_sz, dldw1, dldw2);
+            TREC();
+            cufftExecC2C(planLarge, (cufftComplex *)dldw1, (cufftComplex *)dldw1, CUFFT_INVERSE);
+            TREC();
+            constrained_RMSprop_both<<<N_BLOCKS_L, N_THREADS>>>(dldw1, dldw2, beta, lr, eps,
+                                                                imHs_sz, imLs_sz, mom1, mom2, O, P,
+                                                                dP0, 0.2f);
+            TREC();
+            curr += batch;
+            cudaDeviceSynchronize();
+        }
+        if (epoch > 12) lr = lr * 0.5;
+    }
+    rc = (int)cudaDeviceSynchronize();
+    if (rc == 0) {
+        cudaMemcpy(O_out, O, big * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(P_out, P, plane * 8, cudaMemcpyDeviceToHost);
+        rc = step;
+    } else {
+        rc = -rc;
+    }
+done:
+    cufftDestroy(planBatch);
+    cufftDestroy(planLarge);
+    release();
+    return rc;
+#undef TREC
+#undef TCK
 }
 
 }  // extern "C"

@@ -76,11 +76,14 @@ def ref_solve(lib, O0, P0c, Y, led, P0, pratio, epochs, batch, opt):
     O = np.empty((H, H), np.complex64, order="F")
     P = np.empty((h, h), np.complex64, order="F")
     ms = np.zeros(3, np.float32)
+    # the converted inputs must stay referenced for the whole call: `.ctypes.data` of a
+    # temporary is a dangling address once the temporary is collected
+    ins = [_colmajor(O0, np.complex64), _colmajor(P0c, np.complex64), _stack(Y),
+           np.ascontiguousarray(led, np.int32), _colmajor(P0, np.float32)]
     rc = lib.ref_solve(h, H, L, pratio, epochs, batch, opt[0], opt[1], opt[2],
-                       _colmajor(O0, np.complex64).ctypes.data, _colmajor(P0c, np.complex64).ctypes.data,
-                       _stack(Y).ctypes.data, np.ascontiguousarray(led, np.int32).ctypes.data,
-                       _colmajor(P0, np.float32).ctypes.data, O.ctypes.data, P.ctypes.data,
+                       *[a.ctypes.data for a in ins], O.ctypes.data, P.ctypes.data,
                        ms.ctypes.data)
+    del ins
     assert rc == 0, rc
     return O, P, ms
 

@@ -335,3 +335,61 @@ def test_deconv_pie_weights_match_the_matlab_statements():
                                    np.conj(ker[l]) * x[l] / np.max(np.abs(ker[l]) ** 2))
         np.testing.assert_allclose(orc._deconv_pie(x[l], ker[l], "tPIE", np.float64),
                                    np.conj(ker[l]) * x[l] / (np.abs(ker[l]) ** 2 + 1e-5))
+
+
+# ---------------------------------------------------------------------------
+# the torch restatement (the checker at full size, on the GPU) pinned to the oracle
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("loss_kind", ["anisotropic", "isotropic"])
+def test_torch_checker_gradients_match_oracle(ds_small, loss_kind):
+    """oracle/torch_ref.batch_gradients in complex128 = the FP64 oracle (crops inside and
+    past the spectrum edge, LEDs in uneven chunks)."""
+    import torch
+    from oracle import torch_ref as tr
+    ds = ds_small
+    H = ds.h * ds.pratio
+    rng = np.random.default_rng(9)
+    O = (ds.O0 * np.exp(1j * 0.2 * rng.standard_normal((H, H)))).astype(np.complex64)
+    led = np.concatenate([ds.led_idx, np.array([[H - 20, 3], [H, H], [1, H - 40]], np.int32)])
+    Y = np.concatenate([ds.Y, ds.Y[:3]])
+    G, dP, l64 = orc.batch_gradients(np.fft.fft2(O.astype(np.complex128)),
+                                     ds.pupil_true.astype(np.complex128), Y.astype(np.float64),
+                                     led, ds.pratio, np.float64, loss_kind=loss_kind)
+    Gt, dPt, lt = tr.batch_gradients(torch.fft.fft2(torch.from_numpy(O).to(torch.complex128)),
+                                     torch.from_numpy(ds.pupil_true), torch.from_numpy(Y), led,
+                                     ds.pratio, loss_kind, chunk=7)
+    assert orc.rel_err(Gt.numpy(), G) < 1e-13
+    assert orc.rel_err(dPt.numpy(), dP) < 1e-13
+    assert abs(lt - l64) <= 1e-12 * abs(l64)
+
+
+def test_torch_checker_solve_matches_oracle(ds_small):
+    """oracle/torch_ref.cufpm_pure_v3: complex128 = the FP64 oracle over two epochs with a
+    ragged last batch; complex64 stays as close to FP64 as the numpy FP32 twin does."""
+    import torch
+    from oracle import torch_ref as tr
+    ds = ds_small
+    opt = (1e-3, 0.999, 1e-4)
+    args = (ds.O0, ds.P0c, ds.Y, ds.led_idx, ds.pupil0, ds.pratio, 2, 8)
+    r64 = orc.cufpm_pure_v3(*args, opt=opt, workers=1)
+    r32 = orc.cufpm_pure_v3(*args, opt=opt, workers=1, dtype=np.float32)
+    targs = (torch.from_numpy(ds.O0), torch.from_numpy(ds.P0c), torch.from_numpy(ds.Y),
+             ds.led_idx, torch.from_numpy(ds.pupil0), ds.pratio, 2, 8)
+    seen = []
+    t64 = tr.cufpm_pure_v3(*targs, opt=opt, on_epoch=lambda ep, O, P, l: seen.append(ep))
+    t32 = tr.cufpm_pure_v3(*targs, opt=opt, ctype=torch.complex64)
+    assert seen == [0, 1]
+    for k in ("object", "pupil", "spectrum"):
+        assert orc.rel_err(t64[k].numpy(), getattr(r64, k)) < 1e-13, k
+        e_t = orc.rel_err(t32[k].numpy(), getattr(r64, k))
+        e_n = orc.rel_err(getattr(r32, k), getattr(r64, k))
+        assert e_t < max(1e-6, 3 * e_n), (k, e_t, e_n)
+    np.testing.assert_allclose(t64["loss"], r64.loss, rtol=1e-12)
+
+
+def test_torch_checker_normalise_is_bit_exact():
+    import torch
+    from oracle import torch_ref as tr
+    raw = np.random.default_rng(8).integers(100, 60000, size=(4, 32, 32)).astype(np.uint16)
+    np.testing.assert_array_equal(tr.normalise_u16(torch.from_numpy(raw)).numpy(),
+                                  orc.normalise_stack_u16(raw))
