@@ -30,8 +30,10 @@ struct Box {
 
 // ---- low-resolution (per-LED) stages -------------------------------------
 long long feature_grad_blocks_per_image(int h);
+// loss: 0 anisotropic (the v3 loss), 1 isotropic
 cudaError_t launch_feature_grad(const float2 *Z, StackView Y, int z_off, int nb, int h,
-                                int pratio, float2 *out, double *loss_part, cudaStream_t st);
+                                int pratio, float2 *out, double *loss_part, cudaStream_t st,
+                                int loss = 0);
 
 // ---- large-array stages ---------------------------------------------------
 cudaError_t launch_rmsprop_pupil(const float2 *dP, float2 *P, float *m, const float *P0, int n,

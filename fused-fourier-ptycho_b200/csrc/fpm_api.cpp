@@ -25,6 +25,7 @@
 
 #include "engine.h"
 #include "fft.h"
+#include "generic.h"
 #include "pipeline.h"
 #include "tiff.h"
 
@@ -77,14 +78,19 @@ namespace {
 enum Stage : int {
     ST_COLS_FORWARD, ST_ROWS_FORWARD, ST_LR_COLS_INV, ST_LR_ROWS_INV, ST_LR_ROWS_FWD,
     ST_LR_COLS_FWD, ST_LOSS, ST_PUPIL_GRAD, ST_ROWS_INV, ST_COLS_UPDATE, ST_RMS_PUPIL,
-    ST_SPECTRUM, ST_TRANSPOSE, ST_LR_ROWS_FUSED, ST_SIM_ROWS_INV, ST_SIM_MAGNITUDE, ST_COUNT
+    ST_SPECTRUM, ST_TRANSPOSE, ST_LR_ROWS_FUSED, ST_SIM_ROWS_INV, ST_SIM_MAGNITUDE, ST_H2D,
+    ST_D2H, ST_GEN_LR_FFT, ST_GEN_LOSS, ST_GEN_STITCH, ST_GEN_OBJ_FFT, ST_GEN_RMS_OBJ, ST_COUNT
 };
 const char *const kStageName[ST_COUNT] = {
     "cols_forward", "rows_forward", "lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
     "lr_cols_forward", "loss_reduce", "pupil_grad", "rows_inverse_stitch", "cols_update",
     "rmsprop_pupil", "spectrum_fft2", "transpose", "lr_rows_fused", "sim_rows_inverse",
-    "sim_magnitude"};
-const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+    "sim_magnitude", "copy_inputs_h2d", "copy_outputs_d2h", "any_size_lr_fft2",
+    "any_size_loss_gradient", "any_size_stitch", "any_size_object_fft2",
+    "any_size_rmsprop_object"};
+// 0: a host <-> device copy of the caller's buffers (host-memory calls), not a kernel
+const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0,
+                                 1, 1, 1, 1, 1};
 
 struct Profiler {
     bool on = false;
@@ -154,6 +160,7 @@ struct fpm_context {
     size_t mem_limit = 0;
     std::string err;
     FftEngine fft;
+    GenFft gfft;   // line FFTs of lengths that are not powers of two
     // work buffers, kept between calls
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
         minmax, lut, spec, flag, pie;
@@ -255,10 +262,14 @@ fpm_status validate(fpm_context *ctx, const fpm_problem *p, bool need_batch) {
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "h = %d: must be even and >= 2", p->h);
     if (p->pratio < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "pratio = %d < 1", p->pratio);
     const long long H = (long long)p->h * p->pratio;
-    if (H > kMaxFftLen || !pipeline_supported(p->h, (int)H))
+    if (H > kMaxFftLen ||
+        !(pipeline_supported(p->h, (int)H) || (gen_fft_supported(p->h) && gen_fft_supported((int)H))))
         return fail(ctx, FPM_ERR_UNSUPPORTED,
-                    "h = %d, H = %lld: this build needs powers of two, 16 <= h <= 8192, H <= %d",
+                    "h = %d, H = %lld: h and H must have no prime factor above 7, H <= %d",
                     p->h, H, kMaxFftLen);
+    if (!pipeline_supported(p->h, (int)H) && p->pie_weights != FPM_PIE_NONE)
+        return fail(ctx, FPM_ERR_UNSUPPORTED,
+                    "ePIE / tPIE weights need power-of-two sizes (h = %d, H = %lld)", p->h, H);
     if (p->n_leds < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "n_leds = %d < 1", p->n_leds);
     if (need_batch) {
         if (p->batch < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "batch = %d < 1", p->batch);
@@ -335,10 +346,10 @@ fpm_status stage_inputs(fpm_context *ctx, const fpm_problem *p, const Shape &s, 
     if (rc != FPM_OK) return rc;
     if (p->memory == FPM_MEM_HOST) {
         FPM_CK(ctx->Y.ensure(ybytes));
-        FPM_CK(cudaMemcpyAsync(ctx->Y.p, p->stack, ybytes, cudaMemcpyHostToDevice, st));
+        FPM_STAGE(ST_H2D, cudaMemcpyAsync(ctx->Y.p, p->stack, ybytes, cudaMemcpyHostToDevice, st));
         FPM_CK(ctx->led.ensure(2 * sizeof(int32_t) * s.L));
-        FPM_CK(cudaMemcpyAsync(ctx->led.p, p->led_idx, 2 * sizeof(int32_t) * s.L,
-                               cudaMemcpyHostToDevice, st));
+        FPM_STAGE(ST_H2D, cudaMemcpyAsync(ctx->led.p, p->led_idx, 2 * sizeof(int32_t) * s.L,
+                                          cudaMemcpyHostToDevice, st));
         in.Y.ptr = ctx->Y.p;
         in.led = ctx->led.as<int2>();
     } else {
@@ -744,6 +755,212 @@ static fpm_status centred_spectrum(fpm_context *ctx, const Shape &s, const float
     return FPM_OK;
 }
 
+// Copy of a caller's input into a work buffer; host-to-device copies are timed as the
+// copy_inputs_h2d stage when profiling.
+static cudaError_t copy_in(fpm_context *ctx, void *dst, const void *src, size_t bytes,
+                           cudaMemcpyKind kind) {
+    const bool timed = kind == cudaMemcpyHostToDevice;
+    if (timed) ctx->prof.begin(ctx->stream);
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, ctx->stream);
+    if (timed && e == cudaSuccess) ctx->prof.end(ST_H2D, ctx->stream);
+    return e;
+}
+
+// ---------------------------------------------------------------------------
+// Any-size path (generic.cu): sides h, H with prime factors up to 7 that are not both
+// powers of two.  Per batch, the reference's structure (cuFPM_pure_v3.cu:135-199) with
+// the engine's own transforms: S = FFT2(O); per LED crop x pupil, inverse FFT2, loss
+// gradient, forward FFT2; stitch of the gradient spectrum (an LED-ordered compensated
+// gather over the batch's box, no atomics) and pupil gradient; g = IFFT2(G); RMSprop.
+// Work buffers: S in ctx->S, G in ctx->U, the large transposes' scratch in ctx->W, the
+// per-LED fields in ctx->T1 / ctx->T2 and their transposes' scratch in ctx->Xs.
+// ---------------------------------------------------------------------------
+static size_t gen_loss_parts(int h, int nb) {
+    return (size_t)nb * (size_t)feature_grad_blocks_per_image(h);
+}
+
+static fpm_status gen_alloc(fpm_context *ctx, const fpm_problem *p, const Shape &s, bool host,
+                            bool spec) {
+    size_t need = s.big * 8 * 3 + s.plane * 8 * (size_t)s.B * 3 + s.plane * (8 * 3 + 4 * 2) +
+                  sizeof(double) * gen_loss_parts(s.h, s.B);
+    need += s.big * (8 + 4);                         // O, m1
+    if (spec) need += s.big * 8;
+    if (host) need += s.plane * s.L * (p->stack_type == FPM_STACK_U16_COUNTS ? 2 : 4);
+    if (ctx->mem_limit && need > ctx->mem_limit)
+        return fail(ctx, FPM_ERR_OUT_OF_MEMORY,
+                    "solve needs %zu bytes of device memory, limit is %zu", need, ctx->mem_limit);
+    FPM_CK(ctx->S.ensure(s.big * 8));
+    FPM_CK(ctx->U.ensure(s.big * 8));
+    FPM_CK(ctx->W.ensure(s.big * 8));
+    FPM_CK(ctx->T1.ensure(s.plane * 8 * s.B));
+    FPM_CK(ctx->T2.ensure(s.plane * 8 * s.B));
+    FPM_CK(ctx->Xs.ensure(s.plane * 8 * s.B));
+    FPM_CK(ctx->dP.ensure(s.plane * 8));
+    FPM_CK(ctx->parts.ensure(sizeof(double) * std::max<size_t>(gen_loss_parts(s.h, s.B), 1)));
+    FPM_CK(ctx->flag.ensure(sizeof(int) * 4));
+    FPM_CK(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), ctx->stream));
+    return FPM_OK;
+}
+
+// Gradients of LEDs [z_off, z_off + nb) at (O, P): the object gradient g = IFFT2(G) in
+// ctx->U, the pupil gradient in ctx->dP, the batch loss added to *loss_slot.
+static fpm_status gen_batch(fpm_context *ctx, const Shape &s, const Inputs &in, const float2 *O,
+                            const float2 *P, int z_off, int nb, const Box &box, double *loss_slot,
+                            int loss) {
+    cudaStream_t st = ctx->stream;
+    float2 *S = ctx->S.as<float2>(), *G = ctx->U.as<float2>(), *W = ctx->W.as<float2>();
+    float2 *T1 = ctx->T1.as<float2>(), *T2 = ctx->T2.as<float2>(), *Tt = ctx->Xs.as<float2>();
+    FPM_STAGE(ST_SPECTRUM, ctx->gfft.fft2(O, S, W, s.H, 1, kForward, st));   // K1
+    FPM_STAGE(ST_LR_COLS_INV, launch_gen_crop_pupil(S, s.H, P, s.h, in.led, z_off, nb, T1, st));
+    FPM_STAGE(ST_GEN_LR_FFT, ctx->gfft.fft2(T1, T1, Tt, s.h, nb, kInverse, st));        // K3
+    FPM_STAGE(ST_GEN_LOSS, launch_feature_grad(T1, in.Y, z_off, nb, s.h, s.pratio, T2,
+                                               ctx->parts.as<double>(), st, loss));     // K4
+    FPM_STAGE(ST_LOSS, launch_loss_accumulate(ctx->parts.as<double>(),
+                                              (int)gen_loss_parts(s.h, nb), loss_slot, st));
+    FPM_STAGE(ST_GEN_LR_FFT, ctx->gfft.fft2(T2, T2, Tt, s.h, nb, kForward, st));        // K5
+    FPM_CK(cudaMemsetAsync(G, 0, s.big * 8, st));
+    FPM_STAGE(ST_GEN_STITCH, launch_gen_stitch(T2, s.h, P, in.led, z_off, nb, s.H, box.r_lo,
+                                               box.r_span, box.c_lo, box.c_span, G, st));
+    FPM_STAGE(ST_PUPIL_GRAD,
+              launch_gen_pupil_grad(S, s.H, T2, s.h, in.led, z_off, nb, ctx->dP.as<float2>(), st));
+    FPM_STAGE(ST_GEN_OBJ_FFT, ctx->gfft.fft2(G, G, W, s.H, 1, kInverse, st));            // K8
+    return FPM_OK;
+}
+
+static fpm_status solve_generic(fpm_context *ctx, const fpm_problem *p, fpm_result *res,
+                                const Shape &s, const std::vector<int32_t> &led_host) {
+    const bool dev = p->memory == FPM_MEM_DEVICE;
+    fpm_status rc = gen_alloc(ctx, p, s, !dev, res->spectrum != nullptr);
+    if (rc != FPM_OK) return rc;
+    cudaStream_t st = ctx->stream;
+    ctx->prof.reset();
+    Inputs in;
+    rc = stage_inputs(ctx, p, s, in);
+    if (rc != FPM_OK) return rc;
+    float2 *O, *P;
+    if (dev && res->object) {
+        O = reinterpret_cast<float2 *>(res->object);
+    } else {
+        FPM_CK(ctx->O.ensure(s.big * 8));
+        O = ctx->O.as<float2>();
+    }
+    if (dev && res->pupil) {
+        P = reinterpret_cast<float2 *>(res->pupil);
+    } else {
+        FPM_CK(ctx->P.ensure(s.plane * 8));
+        P = ctx->P.as<float2>();
+    }
+    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (p->object_init) {
+        if ((const void *)p->object_init != (const void *)O)
+            FPM_CK(copy_in(ctx, O, p->object_init, s.big * 8, kin));
+    } else {
+        FPM_CK(ctx->Rs.ensure(bicubic_work_bytes(s.h, s.pratio)));
+        FPM_CK(launch_bicubic_init(in.Y, s.h, s.pratio, O, ctx->Rs.p, st));
+    }
+    if ((const void *)p->pupil_init != (const void *)P)
+        FPM_CK(copy_in(ctx, P, p->pupil_init, s.plane * 8, kin));
+    const float *P0;
+    if (dev) {
+        P0 = p->pupil_amp;
+    } else {
+        FPM_CK(ctx->P0.ensure(s.plane * 4));
+        FPM_CK(copy_in(ctx, ctx->P0.p, p->pupil_amp, s.plane * 4, kin));
+        P0 = ctx->P0.as<float>();
+    }
+    FPM_CK(ctx->m1.ensure(s.big * 4));
+    FPM_CK(ctx->m2.ensure(s.plane * 4));
+    FPM_CK(cudaMemsetAsync(ctx->m1.p, 0, s.big * 4, st));
+    FPM_CK(cudaMemsetAsync(ctx->m2.p, 0, s.plane * 4, st));
+    const int E = p->epochs;
+    FPM_CK(ctx->loss.ensure(sizeof(double) * std::max(E, 1)));
+    FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double) * std::max(E, 1), st));
+    Support whole;
+    whole.r_hi = whole.c_hi = s.h;
+    float lr = p->lr;
+    for (int ep = 0; ep < E; ++ep) {
+        for (int cur = 0; cur < s.L; cur += s.B) {          // cuFPM_pure_v3.cu:131-141
+            const int nb = std::min(s.B, s.L - cur);
+            const Box box = batch_box(led_host, cur, nb, whole, s.H);
+            rc = gen_batch(ctx, s, in, O, P, cur, nb, box, ctx->loss.as<double>() + ep,
+                           p->loss_kind);
+            if (rc != FPM_OK) return rc;
+            FPM_STAGE(ST_GEN_RMS_OBJ, launch_rmsprop_object(O, ctx->m1.as<float>(),
+                                                            ctx->U.as<float2>(), s.big, lr,
+                                                            p->beta, p->eps, st));
+            FPM_STAGE(ST_RMS_PUPIL,
+                      launch_rmsprop_pupil(ctx->dP.as<float2>(), P, ctx->m2.as<float>(), P0,
+                                           (int)s.plane, lr, p->beta, p->eps, p->pupil_margin,
+                                           st));
+        }
+        if (ep > p->lr_halve_after) lr = (float)(lr * (double)p->lr_decay);
+    }
+    if (res->spectrum) {
+        float2 *dst = reinterpret_cast<float2 *>(res->spectrum);
+        if (!dev) {
+            FPM_CK(ctx->S.ensure(s.big * 8));
+            dst = ctx->S.as<float2>();
+        }
+        FPM_STAGE(ST_SPECTRUM, ctx->gfft.fft2(O, dst, ctx->W.as<float2>(), s.H, 1, kForward, st));
+        FPM_CK(launch_centre_in_place(dst, s.H, st));
+        if (!dev)
+            FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->spectrum, dst, s.big * 8,
+                                              cudaMemcpyDeviceToHost, st));
+    }
+    if (!dev && res->object)
+        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->object, O, s.big * 8, cudaMemcpyDeviceToHost, st));
+    if (!dev && res->pupil)
+        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->pupil, P, s.plane * 8, cudaMemcpyDeviceToHost, st));
+    std::vector<double> loss_h(std::max(E, 1));
+    FPM_CK(cudaMemcpyAsync(loss_h.data(), ctx->loss.p, sizeof(double) * std::max(E, 1),
+                           cudaMemcpyDeviceToHost, st));
+    if (res->loss && dev && E > 0)
+        FPM_CK(cudaMemcpyAsync(res->loss, ctx->loss.p, sizeof(double) * E,
+                               cudaMemcpyDeviceToDevice, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    FPM_CK(cudaGetLastError());
+    ctx->prof.collect();
+    if (res->loss && !dev) std::memcpy(res->loss, loss_h.data(), sizeof(double) * E);
+    for (int ep = 0; ep < E; ++ep)
+        if (!std::isfinite(loss_h[ep]))
+            return fail(ctx, FPM_ERR_NONFINITE, "loss of epoch %d is not finite", ep);
+    return FPM_OK;
+}
+
+static fpm_status gradients_generic(fpm_context *ctx, const fpm_problem *p, const Shape &s,
+                                    const std::vector<int32_t> &led_host, float *d_object,
+                                    float *d_pupil, double *loss) {
+    const bool dev = p->memory == FPM_MEM_DEVICE;
+    fpm_status rc = gen_alloc(ctx, p, s, !dev, false);
+    if (rc != FPM_OK) return rc;
+    cudaStream_t st = ctx->stream;
+    ctx->prof.reset();
+    Inputs in;
+    rc = stage_inputs(ctx, p, s, in);
+    if (rc != FPM_OK) return rc;
+    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    FPM_CK(ctx->O.ensure(s.big * 8));
+    FPM_CK(ctx->P.ensure(s.plane * 8));
+    FPM_CK(copy_in(ctx, ctx->O.p, p->object_init, s.big * 8, kin));
+    FPM_CK(copy_in(ctx, ctx->P.p, p->pupil_init, s.plane * 8, kin));
+    FPM_CK(ctx->loss.ensure(sizeof(double)));
+    FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double), st));
+    Support whole;
+    whole.r_hi = whole.c_hi = s.h;
+    const Box box = batch_box(led_host, 0, s.L, whole, s.H);
+    rc = gen_batch(ctx, s, in, ctx->O.as<float2>(), ctx->P.as<float2>(), 0, s.L, box,
+                   ctx->loss.as<double>(), p->loss_kind);
+    if (rc != FPM_OK) return rc;
+    const cudaMemcpyKind kout = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (d_object) FPM_CK(cudaMemcpyAsync(d_object, ctx->U.p, s.big * 8, kout, st));
+    if (d_pupil) FPM_CK(cudaMemcpyAsync(d_pupil, ctx->dP.p, s.plane * 8, kout, st));
+    if (loss) FPM_CK(cudaMemcpyAsync(loss, ctx->loss.p, sizeof(double), kout, st));
+    FPM_CK(cudaStreamSynchronize(st));
+    FPM_CK(cudaGetLastError());
+    ctx->prof.collect();
+    return FPM_OK;
+}
+
 fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
     ctx->err.clear();
@@ -772,6 +989,7 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     std::vector<int32_t> led_host;
     rc = fetch_leds(ctx, p, s, led_host);
     if (rc != FPM_OK) return rc;
+    if (!pipeline_supported(s.h, s.H)) return solve_generic(ctx, p, res, s, led_host);
     Support sup;
     rc = pupil_support(ctx, p, s, sup);
     if (rc != FPM_OK) return rc;
@@ -804,19 +1022,19 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
     const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if (p->object_init) {
         if ((const void *)p->object_init != (const void *)O)
-            FPM_CK(cudaMemcpyAsync(O, p->object_init, s.big * 8, kin, st));
+            FPM_CK(copy_in(ctx, O, p->object_init, s.big * 8, kin));
     } else {
         FPM_CK(ctx->T2.ensure(bicubic_work_bytes(s.h, s.pratio)));   // scratch before the loop
         FPM_CK(launch_bicubic_init(in.Y, s.h, s.pratio, O, ctx->T2.p, st));
     }
     if ((const void *)p->pupil_init != (const void *)P)
-        FPM_CK(cudaMemcpyAsync(P, p->pupil_init, s.plane * 8, kin, st));
+        FPM_CK(copy_in(ctx, P, p->pupil_init, s.plane * 8, kin));
     const float *P0;
     if (dev) {
         P0 = p->pupil_amp;
     } else {
         FPM_CK(ctx->P0.ensure(s.plane * 4));
-        FPM_CK(cudaMemcpyAsync(ctx->P0.p, p->pupil_amp, s.plane * 4, kin, st));
+        FPM_STAGE(ST_H2D, cudaMemcpyAsync(ctx->P0.p, p->pupil_amp, s.plane * 4, kin, st));
         P0 = ctx->P0.as<float>();
     }
     FPM_CK(ctx->m1.ensure(s.big * 4));
@@ -880,12 +1098,13 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
         rc = centred_spectrum(ctx, s, O, dst);
         if (rc != FPM_OK) return rc;
         if (!dev)
-            FPM_CK(cudaMemcpyAsync(res->spectrum, dst, s.big * 8, cudaMemcpyDeviceToHost, st));
+            FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->spectrum, dst, s.big * 8,
+                                              cudaMemcpyDeviceToHost, st));
     }
     if (!dev && res->object)
-        FPM_CK(cudaMemcpyAsync(res->object, O, s.big * 8, cudaMemcpyDeviceToHost, st));
+        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->object, O, s.big * 8, cudaMemcpyDeviceToHost, st));
     if (!dev && res->pupil)
-        FPM_CK(cudaMemcpyAsync(res->pupil, P, s.plane * 8, cudaMemcpyDeviceToHost, st));
+        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->pupil, P, s.plane * 8, cudaMemcpyDeviceToHost, st));
     std::vector<double> loss_h(std::max(E, 1));
     FPM_CK(cudaMemcpyAsync(loss_h.data(), ctx->loss.p, sizeof(double) * std::max(E, 1),
                            cudaMemcpyDeviceToHost, st));
@@ -935,6 +1154,8 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
     std::vector<int32_t> led_host;
     rc = fetch_leds(ctx, p, s, led_host);
     if (rc != FPM_OK) return rc;
+    if (!pipeline_supported(s.h, s.H))
+        return gradients_generic(ctx, p, s, led_host, d_object, d_pupil, loss);
     Support full;   // the pupil gradient is an output here: whole crops
     full.r_hi = full.c_hi = s.h;
     const Plan pl = make_plan(s, led_host, s.L, full, p->loss_kind, p->pie_weights);
@@ -990,8 +1211,9 @@ fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, in
     ctx->err.clear();
     if (!in || !out || count < 1 || (direction != -1 && direction != 1))
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "bad fft2 arguments");
-    if (!fft_supported(n))
-        return fail(ctx, FPM_ERR_UNSUPPORTED, "n = %d: powers of two from 16 to %d", n, kMaxFftLen);
+    if (!fft_supported(n) && !gen_fft_supported(n))
+        return fail(ctx, FPM_ERR_UNSUPPORTED, "n = %d: 2 <= n <= %d with no prime factor above 7",
+                    n, kMaxFftLen);
     if (memory != FPM_MEM_DEVICE && memory != FPM_MEM_HOST)
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", memory);
     FPM_CK(cudaSetDevice(ctx->device));
@@ -1018,7 +1240,13 @@ fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, in
         FPM_CK(cudaMemcpyAsync(ctx->spec.p, in, bytes, cudaMemcpyHostToDevice, st));
         src = dst = ctx->spec.as<float2>();
     }
-    FPM_CK(ctx->fft.run(src, dst, n, count, direction < 0 ? kForward : kInverse, st));
+    const FftDir fdir = direction < 0 ? kForward : kInverse;
+    if (fft_supported(n)) {
+        FPM_CK(ctx->fft.run(src, dst, n, count, fdir, st));
+    } else {   // any-size transform: its transposes need a scratch of the same size
+        FPM_CK(ctx->W.ensure(bytes));
+        FPM_CK(ctx->gfft.fft2(src, dst, ctx->W.as<float2>(), n, count, fdir, st));
+    }
     if (!dev) FPM_CK(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, st));
     FPM_CK(cudaStreamSynchronize(st));
     return FPM_OK;

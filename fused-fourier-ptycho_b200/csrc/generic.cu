@@ -1,0 +1,459 @@
+// Any-size path (generic.h): mixed-radix line FFT and the per-batch stages for image
+// sides that are not powers of two.
+//
+// Line FFT: a CTA transforms LPC contiguous lines of n values held in shared memory,
+// T = ceil(n/16) threads per line.  Each stage is a radix-R Stockham step (self-sorting,
+// natural order in and out, as in fft_core.cuh):
+//
+//   butterfly j in [0, n/R), k = j mod p (p = product of the radices done):
+//     inputs   x[j + r n/R]                          r = 0..R-1
+//     twiddle  x_r *= W_{pR}^{r k} = W_n^{r k n/(pR)}
+//     outputs  y[(j - k) R + k + r p] = DFT_R(x)_r
+//
+// A thread holds its butterflies' inputs in registers across a block barrier, so the
+// stage runs in place in one shared-memory line.  Twiddles come from a table of W_n^m,
+// m < n, built on the host in double precision and read through the read-only cache.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "fft_core.cuh"
+#include "generic.h"
+
+namespace fpm {
+
+namespace {
+
+// cos / sin of 2 pi m / R for the odd radices (m = 1 .. (R-1)/2)
+template <int R>
+__device__ __forceinline__ float cos_r(int m) {
+    if constexpr (R == 3) {
+        return -0.5f;
+    } else if constexpr (R == 5) {
+        return m == 1 ? 0.30901699437494745f : -0.8090169943749473f;
+    } else {
+        return m == 1 ? 0.6234898018587336f : m == 2 ? -0.22252093395631434f : -0.900968867902419f;
+    }
+}
+template <int R>
+__device__ __forceinline__ float sin_r(int m) {
+    if constexpr (R == 3) {
+        return 0.8660254037844387f;
+    } else if constexpr (R == 5) {
+        return m == 1 ? 0.9510565162951535f : 0.5877852522924732f;
+    } else {
+        return m == 1 ? 0.7818314824680298f : m == 2 ? 0.9749279121818236f : 0.43388373911755823f;
+    }
+}
+
+// DFT of odd length R in {3, 5, 7}: with a_j = v_j + v_{R-j}, b_j = v_j - v_{R-j},
+//   out_k     = v_0 + sum_j a_j cos(2 pi j k / R) + i DIR sum_j b_j sin(2 pi j k / R)
+//   out_{R-k} = the same with the sine term negated.
+template <int R, int DIR>
+__device__ __forceinline__ void dft_odd(float2 (&v)[R]) {
+    constexpr int H = (R - 1) / 2;
+    float2 a[H], b[H];
+#pragma unroll
+    for (int j = 1; j <= H; ++j) {
+        a[j - 1] = make_float2(v[j].x + v[R - j].x, v[j].y + v[R - j].y);
+        b[j - 1] = make_float2(v[j].x - v[R - j].x, v[j].y - v[R - j].y);
+    }
+    float2 out[R];
+    float2 s0 = v[0];
+#pragma unroll
+    for (int j = 0; j < H; ++j) s0 = make_float2(s0.x + a[j].x, s0.y + a[j].y);
+    out[0] = s0;
+#pragma unroll
+    for (int k = 1; k <= H; ++k) {
+        float2 t1 = v[0], t2 = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int j = 1; j <= H; ++j) {
+            const int m = (j * k) % R;                       // compile-time after unrolling
+            const int mm = m <= H ? m : R - m;
+            const float c = cos_r<R>(mm);
+            const float s = m <= H ? sin_r<R>(mm) : -sin_r<R>(mm);
+            t1 = make_float2(fmaf(a[j - 1].x, c, t1.x), fmaf(a[j - 1].y, c, t1.y));
+            t2 = make_float2(fmaf(b[j - 1].x, s, t2.x), fmaf(b[j - 1].y, s, t2.y));
+        }
+        // i DIR t2 = DIR (-t2.y, t2.x)
+        const float2 it2 = DIR < 0 ? make_float2(t2.y, -t2.x) : make_float2(-t2.y, t2.x);
+        out[k] = make_float2(t1.x + it2.x, t1.y + it2.y);
+        out[R - k] = make_float2(t1.x - it2.x, t1.y - it2.y);
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = out[k];
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft_any(float2 (&v)[R]) {
+    if constexpr (R == 3 || R == 5 || R == 7) {
+        dft_odd<R, DIR>(v);
+    } else {
+        fft::dft<R, DIR>(v);
+    }
+}
+
+__device__ __forceinline__ float2 cmul2(float2 w, float2 v) {
+    return make_float2(w.x * v.x - w.y * v.y, w.x * v.y + w.y * v.x);
+}
+
+// One radix-R stage over a line of n values at s (shared memory), T = ceil(n/V) threads,
+// thread t.
+template <int R, int DIR, int V>
+__device__ __noinline__ void gen_stage(float2 *s, int n, int p, int T, int t,
+                                          const float2 *__restrict__ tw) {
+    constexpr int KMAX = (V + R - 1) / R;    // ceil(n/R / ceil(n/V)) <= ceil(V/R)
+    const int nbf = n / R;
+    float2 v[KMAX][R];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        const int j = t + k * T;
+        if (j < nbf) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[k][r] = s[j + r * nbf];
+        }
+    }
+    __syncthreads();
+    const int step = n / (p * R);
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        const int j = t + k * T;
+        if (j < nbf) {
+            const int kk = j % p;
+            if (p > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = __ldg(tw + r * kk * step);   // < n: (R-1)(p-1) n/(pR) < n
+                    if (DIR > 0) w.y = -w.y;
+                    v[k][r] = cmul2(w, v[k][r]);
+                }
+            }
+            dft_any<R, DIR>(v[k]);
+            const int base = (j - kk) * R + kk;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[base + r * p] = v[k][r];
+        }
+    }
+    __syncthreads();
+}
+
+struct GenPlan {
+    int n = 0, nst = 0, T = 0, lpc = 1, v = 8;
+    int radix[16] = {};
+};
+
+// V values per thread: 8 up to n = 4096, 16 up to 8192, 32 beyond (at most 512 threads
+// per line, so that a thread may use up to 128 registers)
+template <int DIR, int V>
+__global__ void __launch_bounds__(512, 1) k_gen_lines(const float2 *__restrict__ in,
+                                                    float2 *__restrict__ out, long long count,
+                                                    size_t ld, GenPlan pl,
+                                                    const float2 *__restrict__ tw) {
+    extern __shared__ float2 smem[];
+    const int n = pl.n, T = pl.T, lpc = pl.lpc;
+    const long long g0 = (long long)blockIdx.x * lpc;
+    const int nl = (int)min((long long)lpc, count - g0);
+    // coalesced copy of the CTA's lines into shared memory
+    for (int q = threadIdx.x; q < nl * n; q += blockDim.x) {
+        const int l = q / n, i = q - l * n;
+        smem[l * n + i] = in[(size_t)(g0 + l) * ld + i];
+    }
+    __syncthreads();
+    const int line = threadIdx.x / T, t = threadIdx.x - line * T;
+    // threads of a line past the last one (the CTA's tail) still join every barrier
+    float2 *s = smem + (size_t)min(line, lpc - 1) * n;
+    const bool live = line < nl;
+    int p = 1;
+    for (int st = 0; st < pl.nst; ++st) {
+        const int R = pl.radix[st];
+        const int tt = live ? t : (1 << 29);   // idle threads skip every butterfly
+        switch (R) {
+            case 2: gen_stage<2, DIR, V>(s, n, p, T, tt, tw); break;
+            case 3: gen_stage<3, DIR, V>(s, n, p, T, tt, tw); break;
+            case 4: gen_stage<4, DIR, V>(s, n, p, T, tt, tw); break;
+            case 5: gen_stage<5, DIR, V>(s, n, p, T, tt, tw); break;
+            case 7: gen_stage<7, DIR, V>(s, n, p, T, tt, tw); break;
+            default: gen_stage<8, DIR, V>(s, n, p, T, tt, tw); break;
+        }
+        p *= R;
+    }
+    for (int q = threadIdx.x; q < nl * n; q += blockDim.x) {
+        const int l = q / n, i = q - l * n;
+        out[(size_t)(g0 + l) * ld + i] = smem[l * n + i];
+    }
+}
+
+GenPlan make_plan(int n) {
+    GenPlan pl;
+    pl.n = n;
+    const std::vector<int> rad = gen_fft_radices(n);
+    pl.nst = (int)rad.size();
+    for (int i = 0; i < pl.nst; ++i) pl.radix[i] = rad[i];
+    pl.v = n <= 4096 ? 8 : n <= 8192 ? 16 : 32;
+    pl.T = (n + pl.v - 1) / pl.v;
+    // lines per CTA: up to 16, within 512 threads and 96 KiB of shared memory
+    int lpc = 1;
+    while (lpc < 16 && (lpc * 2) * pl.T <= 512 && (size_t)(lpc * 2) * n * 8 <= 96 * 1024) lpc *= 2;
+    pl.lpc = lpc;
+    return pl;
+}
+
+__global__ void __launch_bounds__(256) k_transpose_pages(const float2 *__restrict__ in,
+                                                         float2 *__restrict__ out, int n) {
+    __shared__ float2 tile[32][33];
+    const size_t page = (size_t)blockIdx.z * n * n;
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    // in[page][c][r]: element (r, c) at c*n + r
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int c = c0 + ty + 8 * k, r = r0 + tx;
+        if (r < n && c < n) tile[ty + 8 * k][tx] = in[page + (size_t)c * n + r];
+    }
+    __syncthreads();
+    // out[page][r][c] = element (r, c) at r*n + c
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = r0 + ty + 8 * k, c = c0 + tx;
+        if (r < n && c < n) out[page + (size_t)r * n + c] = tile[tx][ty + 8 * k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// per-batch stages
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_gen_crop_pupil(const float2 *__restrict__ S, int H,
+                                                        const float2 *__restrict__ P, int h,
+                                                        const int2 *__restrict__ led, int z_off,
+                                                        float2 *__restrict__ out) {
+    const int l = blockIdx.y;
+    const size_t plane = (size_t)h * h;
+    const int2 k = led[z_off + l];                 // (kl, kt), 1-based
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < plane;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i % h), c = (int)(i / h);
+        const int R = (k.y - 1 + r + H / 2) % H, C = (k.x - 1 + c + H / 2) % H;
+        const float2 a = S[(size_t)C * H + R];
+        const float2 p = P[i];
+        const float2 v = make_float2(a.x * p.x - a.y * p.y, a.x * p.y + p.x * a.y);
+        const int rs = (r + h / 2) % h, cs = (c + h / 2) % h;
+        out[(size_t)l * plane + (size_t)cs * h + rs] = v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gen_stitch(const float2 *__restrict__ X, int h,
+                                                    const float2 *__restrict__ P,
+                                                    const int2 *__restrict__ led, int z_off,
+                                                    int nb, int H, int rlo, int rspan, int clo,
+                                                    int cspan, float inv_h2,
+                                                    float2 *__restrict__ G) {
+    extern __shared__ int2 s_led[];
+    for (int l = threadIdx.x; l < nb; l += blockDim.x) s_led[l] = led[z_off + l];
+    __syncthreads();
+    const size_t plane = (size_t)h * h;
+    const size_t n = (size_t)rspan * cspan;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int br = (int)(q % rspan), bc = (int)(q / rspan);
+        const int Rc = (rlo + br) % H, Cc = (clo + bc) % H;     // centred coordinates
+        KahanC acc;
+        bool any = false;
+        for (int l = 0; l < nb; ++l) {
+            const int r = pmod(Rc - (s_led[l].y - 1), H);
+            const int c = pmod(Cc - (s_led[l].x - 1), H);
+            if (r >= h || c >= h) continue;
+            const float2 x = X[(size_t)l * plane + (size_t)((c + h / 2) % h) * h + (r + h / 2) % h];
+            const float2 g = cmul_conj(x, P[(size_t)c * h + r]);
+            acc.add(make_float2(g.x * inv_h2, g.y * inv_h2));
+            any = true;
+        }
+        if (any) {
+            const int R = (Rc + H / 2) % H, C = (Cc + H / 2) % H;   // un-shifted position
+            G[(size_t)C * H + R] = acc.s;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gen_pupil_grad(const float2 *__restrict__ S, int H,
+                                                        const float2 *__restrict__ X, int h,
+                                                        const int2 *__restrict__ led, int z_off,
+                                                        int nb, float2 *__restrict__ dP) {
+    extern __shared__ int2 s_led[];
+    for (int l = threadIdx.x; l < nb; l += blockDim.x) s_led[l] = led[z_off + l];
+    __syncthreads();
+    const size_t plane = (size_t)h * h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < plane;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i % h), c = (int)(i / h);
+        const size_t xs = (size_t)((c + h / 2) % h) * h + (r + h / 2) % h;
+        KahanC acc;
+        for (int l = 0; l < nb; ++l) {
+            const int R = (s_led[l].y - 1 + r + H / 2) % H, C = (s_led[l].x - 1 + c + H / 2) % H;
+            acc.add(cmul_conj(X[(size_t)l * plane + xs], S[(size_t)C * H + R]));
+        }
+        dP[i] = acc.s;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_rmsprop_object(float2 *__restrict__ O, float *__restrict__ m,
+                                                        const float2 *__restrict__ g, size_t n,
+                                                        float lr, float beta, float eps) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float2 gr = g[i];
+        float2 w = O[i];
+        float mu = gr.x * gr.x + gr.y * gr.y;
+        mu = beta * m[i] + (1.0f - beta) * mu;
+        const float sq = lr / (sqrtf(mu) + eps);
+        w.x -= gr.x * sq;
+        w.y -= gr.y * sq;
+        O[i] = w;
+        m[i] = mu;
+    }
+}
+
+int pmod_host(int a, int m) {
+    const int r = a % m;
+    return r < 0 ? r + m : r;
+}
+
+unsigned grid_for(size_t n, int threads) {
+    const size_t b = (n + threads - 1) / threads;
+    return (unsigned)std::min<size_t>(b, (size_t)kB200SMs * 16);
+}
+
+}  // namespace
+
+std::vector<int> gen_fft_radices(int n) {
+    std::vector<int> r;
+    if (n < 2 || n > kMaxFftLen) return {};
+    int m = n;
+    while (m % 8 == 0) r.push_back(8), m /= 8;
+    if (m % 4 == 0) r.push_back(4), m /= 4;
+    if (m % 2 == 0) r.push_back(2), m /= 2;
+    for (int q : {3, 5, 7})
+        while (m % q == 0) r.push_back(q), m /= q;
+    if (m != 1) return {};
+    return r;
+}
+
+bool gen_fft_supported(int n) { return !gen_fft_radices(n).empty(); }
+
+GenFft::~GenFft() { release(); }
+
+void GenFft::release() {
+    for (auto &kv : tw_) cudaFree(kv.second);
+    tw_.clear();
+}
+
+cudaError_t GenFft::table(int n, const float2 **tw) {
+    auto it = tw_.find(n);
+    if (it == tw_.end()) {
+        std::vector<float2> h(n);
+        const double two_pi = 6.283185307179586476925286766559;
+        for (int m = 0; m < n; ++m) {
+            const double a = -two_pi * (double)m / n;
+            h[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        float2 *d = nullptr;
+        cudaError_t e = cudaMalloc(&d, (size_t)n * sizeof(float2));
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(d, h.data(), (size_t)n * sizeof(float2), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(d);
+            return e;
+        }
+        it = tw_.emplace(n, d).first;
+    }
+    *tw = it->second;
+    return cudaSuccess;
+}
+
+cudaError_t GenFft::lines(const float2 *in, float2 *out, int n, long long count, size_t ld,
+                          FftDir dir, cudaStream_t st) {
+    if (!gen_fft_supported(n) || count < 1 || ld < (size_t)n) return cudaErrorInvalidValue;
+    const float2 *tw = nullptr;
+    cudaError_t e = table(n, &tw);
+    if (e != cudaSuccess) return e;
+    const GenPlan pl = make_plan(n);
+    const long long blocks = (count + pl.lpc - 1) / pl.lpc;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const int threads = pl.T * pl.lpc;
+    const size_t smem = (size_t)pl.lpc * n * sizeof(float2);
+    auto go = [&](auto kernel) {
+        cudaError_t e2 = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem);
+        if (e2 != cudaSuccess) return e2;
+        kernel<<<(unsigned)blocks, threads, smem, st>>>(in, out, count, ld, pl, tw);
+        return cudaGetLastError();
+    };
+    if (dir == kForward)
+        return pl.v == 8 ? go(k_gen_lines<-1, 8>) : pl.v == 16 ? go(k_gen_lines<-1, 16>)
+                                                               : go(k_gen_lines<-1, 32>);
+    return pl.v == 8 ? go(k_gen_lines<1, 8>) : pl.v == 16 ? go(k_gen_lines<1, 16>)
+                                                          : go(k_gen_lines<1, 32>);
+}
+
+cudaError_t launch_transpose_pages(const float2 *in, float2 *out, int n, int count,
+                                   cudaStream_t st) {
+    if (n < 1 || count < 1 || count > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((n + 31) / 32, (n + 31) / 32, count);
+    k_transpose_pages<<<grid, 256, 0, st>>>(in, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t GenFft::fft2(const float2 *in, float2 *out, float2 *tmp, int n, int count, FftDir dir,
+                         cudaStream_t st) {
+    const size_t plane = (size_t)n * n;
+    // transform along r (contiguous), transpose, along c (now contiguous), transpose back;
+    // count pages at a time, at most 65535 per transpose launch
+    cudaError_t e = lines(in, out, n, (long long)count * n, n, dir, st);
+    for (int p0 = 0; e == cudaSuccess && p0 < count; p0 += 65535) {
+        const int pc = std::min(65535, count - p0);
+        e = launch_transpose_pages(out + p0 * plane, tmp + p0 * plane, n, pc, st);
+    }
+    if (e == cudaSuccess) e = lines(tmp, tmp, n, (long long)count * n, n, dir, st);
+    for (int p0 = 0; e == cudaSuccess && p0 < count; p0 += 65535) {
+        const int pc = std::min(65535, count - p0);
+        e = launch_transpose_pages(tmp + p0 * plane, out + p0 * plane, n, pc, st);
+    }
+    return e;
+}
+
+cudaError_t launch_gen_crop_pupil(const float2 *S, int H, const float2 *P, int h, const int2 *led,
+                                  int z_off, int nb, float2 *out, cudaStream_t st) {
+    if (nb < 1 || nb > 65535) return cudaErrorInvalidValue;
+    const size_t plane = (size_t)h * h;
+    const unsigned bx = (unsigned)std::min<size_t>((plane + 255) / 256, 1024);
+    k_gen_crop_pupil<<<dim3(bx, nb), 256, 0, st>>>(S, H, P, h, led, z_off, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gen_stitch(const float2 *X, int h, const float2 *P, const int2 *led, int z_off,
+                              int nb, int H, int rlo, int rspan, int clo, int cspan, float2 *G,
+                              cudaStream_t st) {
+    if (nb < 1 || nb > 1024 || rspan < 1 || cspan < 1) return cudaErrorInvalidValue;
+    const size_t n = (size_t)rspan * cspan;
+    const float inv_h2 = 1.0f / (float)((unsigned)H * (unsigned)H);
+    k_gen_stitch<<<grid_for(n, 256), 256, nb * sizeof(int2), st>>>(
+        X, h, P, led, z_off, nb, H, pmod_host(rlo, H), rspan, pmod_host(clo, H), cspan, inv_h2, G);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gen_pupil_grad(const float2 *S, int H, const float2 *X, int h, const int2 *led,
+                                  int z_off, int nb, float2 *dP, cudaStream_t st) {
+    if (nb < 1 || nb > 1024) return cudaErrorInvalidValue;
+    const size_t plane = (size_t)h * h;
+    k_gen_pupil_grad<<<grid_for(plane, 256), 256, nb * sizeof(int2), st>>>(S, H, X, h, led, z_off,
+                                                                          nb, dP);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rmsprop_object(float2 *O, float *m, const float2 *g, size_t n, float lr,
+                                  float beta, float eps, cudaStream_t st) {
+    k_rmsprop_object<<<grid_for(n, 256), 256, 0, st>>>(O, m, g, n, lr, beta, eps);
+    return cudaGetLastError();
+}
+
+}  // namespace fpm

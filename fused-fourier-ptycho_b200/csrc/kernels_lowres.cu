@@ -7,6 +7,7 @@
 // of h*h elements.
 #include "common.cuh"
 #include "engine.h"
+#include "stencil.cuh"
 
 namespace fpm {
 
@@ -36,7 +37,7 @@ __device__ __forceinline__ float load_amp(const StackView &Y, size_t idx, float 
     }
 }
 
-template <int TYPE>
+template <int TYPE, int LOSS>
 __global__ void __launch_bounds__(256) k_feature_grad(const float2 *__restrict__ Z, StackView Y,
                                                        int z_off, int h, int pratio,
                                                        float2 *__restrict__ out,
@@ -77,15 +78,11 @@ __global__ void __launch_bounds__(256) k_feature_grad(const float2 *__restrict__
         const int lc = threadIdx.y + 8 * k + 1;
         const int c = c0 + threadIdx.y + 8 * k;
         if (r < h && c < h) {
-            const float a = s_res[lc][lr];
-            const float rx = s_res[lc + 1][lr] - a;
-            const float ry = s_res[lc][lr + 1] - a;
-            const float ox = sign1(rx);
-            const float oy = sign1(ry);
-            const float ox_m = sign1(a - s_res[lc - 1][lr]);
-            const float oy_m = sign1(a - s_res[lc][lr - 1]);
-            const float d = (ox_m - ox + oy_m - oy) * gscale;
-            lsum += (double)fabsf(rx) + (double)fabsf(ry);
+            // right, left, down, up, down-left, up-right neighbours of (r, c)
+            const float d = stencil<LOSS>(s_res[lc][lr], s_res[lc + 1][lr], s_res[lc - 1][lr],
+                                          s_res[lc][lr + 1], s_res[lc][lr - 1],
+                                          s_res[lc - 1][lr + 1], s_res[lc + 1][lr - 1], lsum) *
+                            gscale;
             const size_t idx = (size_t)c * h + r;
             const float2 v = z[idx];
             const float mag = sqrtf(v.x * v.x + v.y * v.y);
@@ -116,13 +113,23 @@ long long feature_grad_blocks_per_image(int h) {
 }
 
 cudaError_t launch_feature_grad(const float2 *Z, StackView Y, int z_off, int nb, int h,
-                                int pratio, float2 *out, double *loss_part, cudaStream_t st) {
+                                int pratio, float2 *out, double *loss_part, cudaStream_t st,
+                                int loss) {
     const int t = (h + kTR - 1) / kTR;
     dim3 grid(t, t, nb), block(32, 8);
-    if (Y.type == kStackU16)
-        k_feature_grad<kStackU16><<<grid, block, 0, st>>>(Z, Y, z_off, h, pratio, out, loss_part);
+    const bool u16 = Y.type == kStackU16, iso = loss == kLossIsotropic;
+    if (u16 && !iso)
+        k_feature_grad<kStackU16, kLossAnisotropic><<<grid, block, 0, st>>>(Z, Y, z_off, h, pratio,
+                                                                          out, loss_part);
+    else if (u16)
+        k_feature_grad<kStackU16, kLossIsotropic><<<grid, block, 0, st>>>(Z, Y, z_off, h, pratio,
+                                                                        out, loss_part);
+    else if (!iso)
+        k_feature_grad<kStackF32, kLossAnisotropic><<<grid, block, 0, st>>>(Z, Y, z_off, h, pratio,
+                                                                          out, loss_part);
     else
-        k_feature_grad<kStackF32><<<grid, block, 0, st>>>(Z, Y, z_off, h, pratio, out, loss_part);
+        k_feature_grad<kStackF32, kLossIsotropic><<<grid, block, 0, st>>>(Z, Y, z_off, h, pratio,
+                                                                        out, loss_part);
     return cudaGetLastError();
 }
 

@@ -192,3 +192,41 @@ def rel_err(a, b) -> float:
     b = b.to(torch.complex128) if b.is_complex() else b.double()
     nb = float(torch.linalg.vector_norm(b))
     return float(torch.linalg.vector_norm(a - b)) / (nb if nb > 0 else 1.0)
+
+
+def page_normaliser(counts):
+    """Amplitudes of a uint16 stack (L, h, h) page by page with the whole stack's
+    (min, max), as :func:`normalise_u16`: a callable ``Y(first, n)`` for
+    :func:`cufpm_pure_v3`, so that the float stack is never formed whole."""
+    mn, mx = 1 << 30, -1
+    for a in range(0, counts.shape[0], 16):       # int32 copies of a few pages at a time
+        c = counts[a:a + 16].to(torch.int32)
+        mn, mx = min(mn, int(c.min())), max(mx, int(c.max()))
+    mx -= mn
+
+    def pages(first: int, n: int):
+        y = (counts[first:first + n].to(torch.int32) - mn).to(torch.float64)
+        if mx > 0:
+            y = (y / float(mx)).to(torch.float32).to(torch.float64)
+        return torch.sqrt(y).to(torch.float32)
+    return pages
+
+
+def imresize_bicubic(img, scale: int, rows_per_chunk: int = 2048):
+    """MATLAB ``imresize(img, scale, 'bicubic')`` up-scaling (``codes_v2/main_run_FPM.m:48``)
+    in float64 on img's device, with the taps and weights of
+    ``fpm_oracle.imresize_bicubic_weights``: rows first, then columns, output rows in
+    chunks."""
+    from oracle import fpm_oracle as orc
+    dev = img.device
+    img = img.to(torch.float64)
+    ir, wr = orc.imresize_bicubic_weights(img.shape[0], scale)
+    ic, wc = orc.imresize_bicubic_weights(img.shape[1], scale)
+    ir, wr = torch.from_numpy(ir).to(dev), torch.from_numpy(wr).to(dev)
+    ic, wc = torch.from_numpy(ic).to(dev), torch.from_numpy(wc).to(dev)
+    t = (img[ir, :] * wr[:, :, None]).sum(dim=1)                 # (n_out_r, n_c)
+    out = torch.empty((t.shape[0], ic.shape[0]), dtype=torch.float64, device=dev)
+    for r0 in range(0, t.shape[0], rows_per_chunk):
+        tc = t[r0:r0 + rows_per_chunk]
+        out[r0:r0 + rows_per_chunk] = (tc[:, ic] * wc[None, :, :]).sum(dim=2)
+    return out
