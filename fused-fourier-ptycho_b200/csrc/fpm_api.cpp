@@ -1314,11 +1314,12 @@ fpm_status fpm_simulate(fpm_context *ctx, const float *object, const float *pupi
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "output = %d", output);
     if (memory != FPM_MEM_DEVICE && memory != FPM_MEM_HOST)
         return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "memory = %d", memory);
-    if (h < 2 || pratio < 1 || (long long)h * pratio > kMaxFftLen ||
-        !pipeline_supported(h, h * pratio))
+    if (h < 2 || (h & 1) || pratio < 1 || (long long)h * pratio > kMaxFftLen ||
+        !(pipeline_supported(h, h * pratio) ||
+          (gen_fft_supported(h) && gen_fft_supported(h * pratio))))
         return fail(ctx, FPM_ERR_UNSUPPORTED,
-                    "h = %d, pratio = %d: h and h*pratio powers of two, 16..8192 and ..16384", h,
-                    pratio);
+                    "h = %d, pratio = %d: even h, h and h*pratio <= %d with no prime factor "
+                    "above 7", h, pratio, kMaxFftLen);
     FPM_CK(cudaSetDevice(ctx->device));
     const bool dev = memory == FPM_MEM_DEVICE;
     const void *ptrs[4] = {object, pupil, led_idx, out};
@@ -1365,6 +1366,31 @@ fpm_status fpm_simulate(fpm_context *ctx, const float *object, const float *pupi
         P = ctx->P.as<float2>();
         led = ctx->led.as<int2>();
     }
+    const float scale = (float)(1.0 / ((double)plane * pratio * pratio));
+    if (!pipeline_supported(h, H)) {
+        // any size: spectrum (un-shifted), crop x pupil with the inverse shift, inverse 2-D
+        // FFT of each LED's page, magnitude
+        FPM_CK(ctx->S.ensure(big * 8));
+        FPM_CK(ctx->W.ensure(std::max(big, plane * group) * 8));
+        FPM_CK(ctx->T1.ensure(plane * 8 * group));
+        if (!dev) FPM_CK(ctx->Rs.ensure(plane * 4 * group));
+        float2 *S = ctx->S.as<float2>(), *W = ctx->W.as<float2>(), *T1 = ctx->T1.as<float2>();
+        FPM_STAGE(ST_SPECTRUM, ctx->gfft.fft2(O, S, W, H, 1, kForward, st));
+        for (int l0 = 0; l0 < n_leds; l0 += group) {
+            const int nl = std::min(group, n_leds - l0);
+            FPM_STAGE(ST_LR_COLS_INV, launch_gen_crop_pupil(S, H, P, h, led, l0, nl, T1, st));
+            FPM_STAGE(ST_SIM_ROWS_INV, ctx->gfft.fft2(T1, T1, W, h, nl, kInverse, st));
+            float *dst = dev ? out + plane * l0 : ctx->Rs.as<float>();
+            FPM_STAGE(ST_SIM_MAGNITUDE, launch_sim_magnitude(T1, plane * nl, scale,
+                                                             output == FPM_SIM_AMPLITUDE, dst, st));
+            if (!dev)
+                FPM_CK(cudaMemcpyAsync(out + plane * l0, dst, plane * 4 * nl,
+                                       cudaMemcpyDeviceToHost, st));
+        }
+        FPM_CK(cudaStreamSynchronize(st));
+        ctx->prof.collect();
+        return FPM_OK;
+    }
     // centred spectrum of the object (gen_img_batch.m:184, fftshift(fft2(wavefront1)))
     FPM_CK(ctx->S.ensure(big * 8));
     float2 *Sc = ctx->S.as<float2>();
@@ -1389,7 +1415,6 @@ fpm_status fpm_simulate(fpm_context *ctx, const float *object, const float *pupi
     BatchBufs b;
     b.Sbox = Sc;
     b.T1 = ctx->T1.as<float2>();
-    const float scale = (float)(1.0 / ((double)plane * pratio * pratio));
     for (int l0 = 0; l0 < n_leds; l0 += group) {
         const int nl = std::min(group, n_leds - l0);
         // crop x pupil, ifftshift, inverse FFT along r; then along c

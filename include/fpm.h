@@ -22,8 +22,10 @@
  *     spectrum (MATLAB int32([kl; kt]), codes_v2/main_run_FPM.m:53-55).  A
  *     crop that runs past the spectrum edge wraps modulo H, as in v3
  *     (cuFPM_v3/cuda/kernels.cuh:43-47).  1 <= kl, kt <= H is required.
- *   - h and H = h * pratio must be powers of two from 16 to 16384 in this build
- *     (FPM_ERR_UNSUPPORTED otherwise).  The caller owns every buffer.
+ *   - h must be even; h and H = h * pratio may have no prime factor above 7, and
+ *     H <= 16384 (FPM_ERR_UNSUPPORTED otherwise).  Powers of two (h >= 16) run the
+ *     fused pipeline, other sizes the any-size path (mixed-radix transforms with the
+ *     reference's per-batch structure).  The caller owns every buffer.
  *   - Every function returns an fpm_status; nothing throws across the ABI.
  *   - A context is bound to one CUDA device and is not thread-safe: use one
  *     context per host thread.
@@ -194,7 +196,7 @@ fpm_status fpm_read_tiff_stack(fpm_context *ctx, const char *const *paths, int32
 
 /* The engine's own unnormalised 2-D FFT of `count` column-major n x n complex
    pages (direction -1 forward, +1 inverse), the transform behind the cuFFT calls
-   of cuFPM_pure_v3.cu:135-187.  n: power of two, 16 <= n <= 16384.  in may equal
+   of cuFPM_pure_v3.cu:135-187.  n: 2 <= n <= 16384, no prime factor above 7.  in may equal
    out.  Pointers follow `memory`. */
 fpm_status fpm_fft2(fpm_context *ctx, const float *in, float *out, int32_t n, int32_t count,
                     int32_t direction, int32_t memory);
@@ -257,7 +259,7 @@ fpm_status fpm_led_indices(fpm_context *ctx, const fpm_led_geometry *geo, int32_
    (1-based corner, wrapping modulo H as in fpm_problem), and out page l = |x_l|^2
    (FPM_SIM_INTENSITY) or |x_l| (FPM_SIM_AMPLITUDE).  object: complex H*H (H = h *
    pratio), pupil: complex h*h, led_idx: 2*n_leds int32, out: float h*h*n_leds; all
-   column-major, pointers follow `memory`.  h and H: powers of two (16..8192, ..16384).
+   column-major, pointers follow `memory`.  h even, h and H with no prime factor above 7, H <= 16384.
    The transforms are the engine's own; used to make training / test data and to
    check a reconstruction against its measurements. */
 typedef enum fpm_sim_output { FPM_SIM_INTENSITY = 0, FPM_SIM_AMPLITUDE = 1 } fpm_sim_output;

@@ -1,0 +1,174 @@
+"""Image sides that are not powers of two (the reference takes any even size, README.md:9;
+its cuFFT plans take any h and H, cuFPM_v3/cuFPM_pure_v3.cu:116-126).
+
+The engine's any-size path (mixed-radix line FFTs with radices 2, 3, 4, 5, 7, 8 and the
+generic per-batch stages) against numpy (transforms), the FP64 oracle (gradients, solves,
+forward model; small sizes) and the torch FP64 checker (config-3 sizes).  Tolerances as
+in test_gpu_parity: 2e-5 relative, or 3x the FP32 twin's own distance to FP64 where that
+is larger; the anisotropic loss's sign flips are avoided by noiseless amplitudes or the
+isotropic loss where a tight bar is wanted.
+"""
+import numpy as np
+import pytest
+
+from conftest import led_matlab, to_matlab_stack, dataset
+from oracle import fpm_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = 2e-5
+
+
+@pytest.mark.parametrize("n", [6, 12, 48, 96, 160, 192, 210, 384, 448, 640, 768, 896, 1152,
+                               1536, 2304, 3072, 4800, 6144, 12288])
+def test_any_size_fft2_matches_numpy(engine, n):
+    rng = np.random.default_rng(n)
+    count = 2 if n <= 4096 else 1
+    x = (rng.standard_normal((n, n, count)) + 1j * rng.standard_normal((n, n, count))).astype(np.complex64)
+    ref = np.fft.fft2(x.astype(np.complex128), axes=(0, 1))
+    got = engine.fft2(x, direction=-1)
+    tol = 2e-6 * max(1.0, np.log2(n) / 4)
+    for k in range(count):
+        assert orc.rel_err(got[:, :, k], ref[:, :, k]) < tol, (n, orc.rel_err(got[:, :, k], ref[:, :, k]))
+    back = engine.fft2(got, direction=1)
+    assert orc.rel_err(back / (n * n), x) < 2 * tol
+
+
+def _noiseless_ds(h, p, grid, seed):
+    from fpm_b200 import synth
+    ds = dataset(h, p, grid, seed=seed, aberration=True)
+    spec = np.fft.fftshift(np.fft.fft2(ds.object_true)).astype(np.complex64)
+    I = synth.forward_intensity(spec, ds.pupil_true, ds.led_idx, p)
+    Y = np.sqrt(I / I.max()).astype(np.float32)
+    O0 = synth.upsample_bicubic(Y[0], p).astype(np.float32).astype(np.complex64)
+    return ds, Y, O0
+
+
+@pytest.mark.parametrize("h,p", [(48, 4), (64, 3), (40, 5), (56, 6), (30, 7)])
+def test_any_size_solve_vs_oracle(engine, h, p):
+    """Two epochs (ragged last batch) on noiseless amplitudes, anisotropic loss, against
+    the FP64 oracle, with the FP32 twin's distance as the bar."""
+    ds, Y, O0 = _noiseless_ds(h, p, 5, seed=h + p)
+    opt = (1e-3, 0.999, 1e-4)
+    L, E, B = 25, 2, 8
+    r = engine.solve(O0, ds.P0c, to_matlab_stack(Y[:L]), led_matlab(ds.led_idx[:L]), ds.pupil0, p,
+                     E, B, lr=opt[0], beta=opt[1], eps=opt[2])
+    args = (O0, ds.P0c, Y[:L], ds.led_idx[:L], ds.pupil0, p, E, B)
+    o64 = orc.cufpm_pure_v3(*args, opt=opt, workers=1)
+    o32 = orc.cufpm_pure_v3(*args, opt=opt, workers=1, dtype=np.float32)
+    for k in ("object", "pupil", "spectrum"):
+        e, e32 = orc.rel_err(r[k], getattr(o64, k)), orc.rel_err(getattr(o32, k), getattr(o64, k))
+        assert e < max(TIGHT, 3 * e32), (h, p, k, e, e32)
+    np.testing.assert_allclose(r["loss"], o64.loss, rtol=1e-5)
+
+
+@pytest.mark.parametrize("h,p", [(48, 4), (80, 3)])
+def test_any_size_uint16_and_isotropic(engine, h, p):
+    """uint16 frames (normalised on the device) and both losses on the any-size path, one
+    epoch, against the FP64 oracle on the normalised amplitudes.  Poisson frames hold
+    quantised counts, so residual differences near zero are common and the anisotropic
+    loss's signs there depend on the FFT's rounding: the bar is the larger distance of two
+    FP32 twins with different FFTs (numpy's pocketfft and cuFFT through torch)."""
+    import torch
+    from oracle import torch_ref as tr
+    ds = dataset(h, p, 5, seed=3, aberration=True)
+    opt = (1e-3, 0.999, 1e-4)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    for loss in ("isotropic", "anisotropic"):
+        r = engine.solve(ds.O0, ds.P0c, to_matlab_stack(ds.raw), led_matlab(ds.led_idx), ds.pupil0,
+                         p, 1, 8, lr=opt[0], beta=opt[1], eps=opt[2], loss=loss)
+        args = (ds.O0, ds.P0c, ds.Y, ds.led_idx, ds.pupil0, p, 1, 8)
+        o64 = orc.cufpm_pure_v3(*args, opt=opt, workers=1, loss_kind=loss)
+        o32 = orc.cufpm_pure_v3(*args, opt=opt, workers=1, loss_kind=loss, dtype=np.float32)
+        c32 = tr.cufpm_pure_v3(t(ds.O0), t(ds.P0c), t(ds.Y), ds.led_idx, t(ds.pupil0), p, 1, 8,
+                               opt=opt, ctype=torch.complex64, loss_kind=loss)
+        for k in ("object", "pupil"):
+            e = orc.rel_err(r[k], getattr(o64, k))
+            e32 = max(orc.rel_err(getattr(o32, k), getattr(o64, k)),
+                      orc.rel_err(c32[k].cpu().numpy(), getattr(o64, k)))
+            print(f"{h} {p} {loss} {k}: engine {e:.3e} twins {e32:.3e}")
+            assert e < max(TIGHT, 3 * e32), (loss, k, e, e32)
+        np.testing.assert_allclose(r["loss"], o64.loss, rtol=1e-5)
+
+
+def test_any_size_batch_gradients_vs_oracle(engine):
+    """fpm_batch_gradients on the any-size path: isotropic loss within 2e-5 (or 3x the
+    twin), anisotropic loss value to 1e-5, crops inside and past the spectrum edge."""
+    from fpm_b200 import synth
+    h, p = 48, 5
+    H = h * p
+    rng = np.random.default_rng(5)
+    O = (0.5 + 0.5 * rng.random((H, H)) * np.exp(1j * rng.random((H, H)))).astype(np.complex64)
+    P = (synth.pupil_circle(h, synth.Optics(led_grid=3)) *
+         np.exp(0.3j * rng.standard_normal((h, h)))).astype(np.complex64)
+    P0 = np.abs(P).astype(np.float32)
+    led = np.array([[H // 2 - h // 2 + 1, H // 2 - h // 2 + 1], [1, 1], [H - 20, 30], [H, H],
+                    [100, 7]], np.int32)
+    Y = rng.random((len(led), h, h)).astype(np.float32)
+    S64 = np.fft.fft2(O.astype(np.complex128))
+    for loss in ("isotropic", "anisotropic"):
+        dO, dP, lv = engine.batch_gradients(O, P, to_matlab_stack(Y), led_matlab(led), P0, p,
+                                            loss=loss)
+        G, dP64, l64 = orc.batch_gradients(S64, P.astype(np.complex128), Y.astype(np.float64), led,
+                                           p, np.float64, loss_kind=loss)
+        G32, dP32, _ = orc.batch_gradients(np.fft.fft2(O), P, Y, led, p, np.float32,
+                                           loss_kind=loss)
+        dO64 = np.fft.ifft2(G) * H * H
+        e_o, t_o = orc.rel_err(dO, dO64), orc.rel_err(np.fft.ifft2(G32) * H * H, dO64)
+        e_p, t_p = orc.rel_err(dP, dP64), orc.rel_err(dP32, dP64)
+        assert abs(lv - l64) < 1e-5 * abs(l64), (loss, lv, l64)
+        if loss == "isotropic":
+            assert e_o < max(TIGHT, 3 * t_o), (e_o, t_o)
+            assert e_p < max(TIGHT, 3 * t_p), (e_p, t_p)
+        else:   # sign flips at near-ties: within a flip's reach of FP64, as the twin
+            assert e_o < max(1e-2, 3 * t_o) and e_p < max(1e-2, 3 * t_p), (e_o, t_o, e_p, t_p)
+
+
+@pytest.mark.parametrize("h,p,amplitude", [(48, 4, True), (40, 5, False), (96, 3, True)])
+def test_any_size_simulate_matches_oracle(engine, h, p, amplitude):
+    from fpm_b200 import synth
+    rng = np.random.default_rng(h)
+    H = h * p
+    O = np.exp(1j * 0.3 * rng.standard_normal((H, H))).astype(np.complex64)
+    P = (synth.pupil_circle(h, synth.Optics(led_grid=3)) *
+         np.exp(0.2j * rng.standard_normal((h, h)))).astype(np.complex64)
+    led = np.array([[H // 2 - h // 2 + 1, H // 2 - h // 2 + 1], [1, 1], [H - 10, 20], [H, H]],
+                   np.int32)
+    got = engine.simulate(O, P, led_matlab(led), p, amplitude=amplitude)
+    ref = orc.forward_model(O, P, led, p, amplitude=amplitude)
+    for l in range(len(led)):
+        assert orc.rel_err(got[:, :, l], ref[l]) < 2e-6 * max(1.0, np.log2(H) / 8), l
+
+
+@pytest.mark.parametrize("h,p", [(192, 4), (384, 6)])
+def test_config3_sizes_solve_vs_fp64_checker(engine, h, p):
+    """Sizes of the batched-instances configuration (h in {192, 384}, up-sampling 4-8):
+    one epoch of 25 LEDs (batch 8) on noiseless amplitudes against the torch FP64 checker
+    on the GPU, the FP32 twin's distance as the bar."""
+    import torch
+    from oracle import torch_ref as tr
+    ds, Y, O0 = _noiseless_ds(h, p, 5, seed=7)
+    opt = (1e-3, 0.999, 1e-4)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    r = engine.solve(dev(O0), dev(ds.P0c), dev(to_matlab_stack(Y)), dev(led_matlab(ds.led_idx)),
+                     dev(ds.pupil0), p, 1, 8, lr=opt[0], beta=opt[1], eps=opt[2])
+    args = (dev(O0), dev(ds.P0c), dev(Y), ds.led_idx, dev(ds.pupil0), p, 1, 8)
+    r64 = tr.cufpm_pure_v3(*args, opt=opt)
+    r32 = tr.cufpm_pure_v3(*args, opt=opt, ctype=torch.complex64)
+    for k in ("object", "pupil", "spectrum"):
+        e, t = tr.rel_err(r[k], r64[k]), tr.rel_err(r32[k], r64[k])
+        assert e < max(TIGHT, 3 * t), (h, p, k, e, t)
+    np.testing.assert_allclose(np.asarray(r["loss"].cpu()), r64["loss"], rtol=1e-5)
+
+
+def test_sizes_beyond_the_radices_are_refused(engine):
+    """A side with a prime factor above 7 (h = 44 = 4 x 11) is refused before any work."""
+    import fpm_b200
+    h = 44
+    with pytest.raises(fpm_b200.FpmError) as e:
+        engine.solve(np.ones((h * 4, h * 4), np.complex64), np.ones((h, h), np.complex64),
+                     np.ones((h, h, 2), np.float32), np.ones((2, 2), np.int32),
+                     np.ones((h, h), np.float32), 4, 1, 2)
+    assert e.value.status == 2
+    with pytest.raises(fpm_b200.FpmError):
+        engine.fft2(np.ones((22, 22), np.complex64))
