@@ -49,6 +49,9 @@ cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, void 
 
 // ---- reductions and ingest ------------------------------------------------
 cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cudaStream_t st);
+// a captured epoch's end: loss[*counter] = *acc, *acc = 0, ++*counter
+cudaError_t launch_epoch_end(double *acc, double *loss, int *counter, cudaStream_t st);
+cudaError_t launch_set_int(int *p, int v, cudaStream_t st);
 cudaError_t launch_stack_minmax(const uint16_t *p, size_t n, unsigned *minmax, cudaStream_t st);
 cudaError_t launch_normalise(const uint16_t *p, size_t n, const unsigned *minmax, float *out,
                              cudaStream_t st);

@@ -165,6 +165,9 @@ struct fpm_context {
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
         minmax, lut, spec, flag, pie;
     DevBuf opt[6];   // device copies of an optimiser step's host arrays
+    // fpm_solve_batch: one worker context per instance, on a pool of streams
+    std::vector<fpm_context *> workers;
+    std::vector<cudaStream_t> pool;
 };
 
 namespace {
@@ -706,7 +709,10 @@ void fpm_destroy(fpm_context *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (fpm_context *w : ctx->workers) fpm_destroy(w);
+    for (cudaStream_t sp : ctx->pool) cudaStreamDestroy(sp);
     ctx->fft.release();
+    ctx->gfft.release();
     if (ctx->entry) cudaEventDestroy(ctx->entry);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -827,106 +833,6 @@ static fpm_status gen_batch(fpm_context *ctx, const Shape &s, const Inputs &in, 
     return FPM_OK;
 }
 
-static fpm_status solve_generic(fpm_context *ctx, const fpm_problem *p, fpm_result *res,
-                                const Shape &s, const std::vector<int32_t> &led_host) {
-    const bool dev = p->memory == FPM_MEM_DEVICE;
-    fpm_status rc = gen_alloc(ctx, p, s, !dev, res->spectrum != nullptr);
-    if (rc != FPM_OK) return rc;
-    cudaStream_t st = ctx->stream;
-    ctx->prof.reset();
-    Inputs in;
-    rc = stage_inputs(ctx, p, s, in);
-    if (rc != FPM_OK) return rc;
-    float2 *O, *P;
-    if (dev && res->object) {
-        O = reinterpret_cast<float2 *>(res->object);
-    } else {
-        FPM_CK(ctx->O.ensure(s.big * 8));
-        O = ctx->O.as<float2>();
-    }
-    if (dev && res->pupil) {
-        P = reinterpret_cast<float2 *>(res->pupil);
-    } else {
-        FPM_CK(ctx->P.ensure(s.plane * 8));
-        P = ctx->P.as<float2>();
-    }
-    const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (p->object_init) {
-        if ((const void *)p->object_init != (const void *)O)
-            FPM_CK(copy_in(ctx, O, p->object_init, s.big * 8, kin));
-    } else {
-        FPM_CK(ctx->Rs.ensure(bicubic_work_bytes(s.h, s.pratio)));
-        FPM_CK(launch_bicubic_init(in.Y, s.h, s.pratio, O, ctx->Rs.p, st));
-    }
-    if ((const void *)p->pupil_init != (const void *)P)
-        FPM_CK(copy_in(ctx, P, p->pupil_init, s.plane * 8, kin));
-    const float *P0;
-    if (dev) {
-        P0 = p->pupil_amp;
-    } else {
-        FPM_CK(ctx->P0.ensure(s.plane * 4));
-        FPM_CK(copy_in(ctx, ctx->P0.p, p->pupil_amp, s.plane * 4, kin));
-        P0 = ctx->P0.as<float>();
-    }
-    FPM_CK(ctx->m1.ensure(s.big * 4));
-    FPM_CK(ctx->m2.ensure(s.plane * 4));
-    FPM_CK(cudaMemsetAsync(ctx->m1.p, 0, s.big * 4, st));
-    FPM_CK(cudaMemsetAsync(ctx->m2.p, 0, s.plane * 4, st));
-    const int E = p->epochs;
-    FPM_CK(ctx->loss.ensure(sizeof(double) * std::max(E, 1)));
-    FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double) * std::max(E, 1), st));
-    Support whole;
-    whole.r_hi = whole.c_hi = s.h;
-    float lr = p->lr;
-    for (int ep = 0; ep < E; ++ep) {
-        for (int cur = 0; cur < s.L; cur += s.B) {          // cuFPM_pure_v3.cu:131-141
-            const int nb = std::min(s.B, s.L - cur);
-            const Box box = batch_box(led_host, cur, nb, whole, s.H);
-            rc = gen_batch(ctx, s, in, O, P, cur, nb, box, ctx->loss.as<double>() + ep,
-                           p->loss_kind);
-            if (rc != FPM_OK) return rc;
-            FPM_STAGE(ST_GEN_RMS_OBJ, launch_rmsprop_object(O, ctx->m1.as<float>(),
-                                                            ctx->U.as<float2>(), s.big, lr,
-                                                            p->beta, p->eps, st));
-            FPM_STAGE(ST_RMS_PUPIL,
-                      launch_rmsprop_pupil(ctx->dP.as<float2>(), P, ctx->m2.as<float>(), P0,
-                                           (int)s.plane, lr, p->beta, p->eps, p->pupil_margin,
-                                           st));
-        }
-        if (ep > p->lr_halve_after) lr = (float)(lr * (double)p->lr_decay);
-    }
-    if (res->spectrum) {
-        float2 *dst = reinterpret_cast<float2 *>(res->spectrum);
-        if (!dev) {
-            FPM_CK(ctx->S.ensure(s.big * 8));
-            dst = ctx->S.as<float2>();
-        }
-        FPM_STAGE(ST_SPECTRUM, ctx->gfft.fft2(O, dst, ctx->W.as<float2>(), s.H, 1, kForward, st));
-        FPM_CK(launch_centre_in_place(dst, s.H, st));
-        if (!dev)
-            FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->spectrum, dst, s.big * 8,
-                                              cudaMemcpyDeviceToHost, st));
-    }
-    if (!dev && res->object)
-        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->object, O, s.big * 8, cudaMemcpyDeviceToHost, st));
-    if (!dev && res->pupil)
-        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->pupil, P, s.plane * 8, cudaMemcpyDeviceToHost, st));
-    std::vector<double> loss_h(std::max(E, 1));
-    FPM_CK(cudaMemcpyAsync(loss_h.data(), ctx->loss.p, sizeof(double) * std::max(E, 1),
-                           cudaMemcpyDeviceToHost, st));
-    if (res->loss && dev && E > 0)
-        FPM_CK(cudaMemcpyAsync(res->loss, ctx->loss.p, sizeof(double) * E,
-                               cudaMemcpyDeviceToDevice, st));
-    FPM_CK(cudaStreamSynchronize(st));
-    FPM_CK(cudaGetLastError());
-    ctx->prof.collect();
-    if (res->loss && !dev) std::memcpy(res->loss, loss_h.data(), sizeof(double) * E);
-    for (int ep = 0; ep < E; ++ep)
-        if (!std::isfinite(loss_h[ep]))
-            return fail(ctx, FPM_ERR_NONFINITE, "loss of epoch %d is not finite", ep);
-    return FPM_OK;
-}
-
 static fpm_status gradients_generic(fpm_context *ctx, const fpm_problem *p, const Shape &s,
                                     const std::vector<int32_t> &led_host, float *d_object,
                                     float *d_pupil, double *loss) {
@@ -961,18 +867,43 @@ static fpm_status gradients_generic(fpm_context *ctx, const fpm_problem *p, cons
     return FPM_OK;
 }
 
-fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
+// ---------------------------------------------------------------------------
+// One reconstruction in three phases: prepare (validation, plan, buffers, inputs, the
+// initial object), epochs (enqueued one at a time, eagerly or replayed from a captured
+// CUDA graph), finish (outputs, the one synchronisation, status).  fpm_solve runs the
+// phases back to back; fpm_solve_batch interleaves them over many instances.
+// ---------------------------------------------------------------------------
+struct SolveJob {
+    const fpm_problem *p = nullptr;
+    fpm_result res{};
+    Shape s{};
+    bool dev = false, generic = false;
+    std::vector<int32_t> led_host;
+    Plan pl;                    // power-of-two path
+    std::vector<Box> boxes;     // any-size path: the crop box of every mini-batch
+    Inputs in;
+    Twiddles tw;
+    float2 *O = nullptr, *P = nullptr;
+    const float *P0 = nullptr;
+    float lr = 0.f;
+    double *loss = nullptr;     // device: E epoch slots, then a captured epoch's accumulator
+    int *epoch_counter = nullptr;   // device: the slot a captured epoch writes its loss to
+};
+
+static fpm_status job_prepare(fpm_context *ctx, const fpm_problem *p, fpm_result *res,
+                              SolveJob &j) {
     if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
     ctx->err.clear();
     FPM_CK(cudaSetDevice(ctx->device));
-    Shape s;
-    fpm_status rc = shape_of(ctx, p, s, true);
+    fpm_status rc = shape_of(ctx, p, j.s, true);
     if (rc != FPM_OK) return rc;
-    fpm_result none{};
-    if (!res) res = &none;
-    const bool dev = p->memory == FPM_MEM_DEVICE;
+    const Shape &s = j.s;
+    j.p = p;
+    if (res) j.res = *res;
+    j.dev = p->memory == FPM_MEM_DEVICE;
+    const bool dev = j.dev;
     if (dev) {
-        void *outs[4] = {res->object, res->spectrum, res->pupil, res->loss};
+        void *outs[4] = {j.res.object, j.res.spectrum, j.res.pupil, j.res.loss};
         for (int i = 0; i < 4; ++i) {
             if (outs[i] && !is_device_ptr(outs[i], ctx->device))
                 return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "result pointer %d is not device memory",
@@ -981,136 +912,221 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
                 return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "result pointer %d is not 16-byte aligned",
                             i);
         }
-    }
-    if (dev) {
         rc = order_after_default_stream(ctx);
         if (rc != FPM_OK) return rc;
     }
-    std::vector<int32_t> led_host;
-    rc = fetch_leds(ctx, p, s, led_host);
+    rc = fetch_leds(ctx, p, s, j.led_host);
     if (rc != FPM_OK) return rc;
-    if (!pipeline_supported(s.h, s.H)) return solve_generic(ctx, p, res, s, led_host);
-    Support sup;
-    rc = pupil_support(ctx, p, s, sup);
-    if (rc != FPM_OK) return rc;
-    const Plan pl = make_plan(s, led_host, p->batch, sup, p->loss_kind, p->pie_weights);
-    rc = alloc_pipeline(ctx, p, s, pl, res->spectrum != nullptr);
-    if (rc != FPM_OK) return rc;
+    j.generic = !pipeline_supported(s.h, s.H);
+    if (j.generic) {
+        rc = gen_alloc(ctx, p, s, !dev, j.res.spectrum != nullptr);
+        if (rc != FPM_OK) return rc;
+        Support whole;
+        whole.r_hi = whole.c_hi = s.h;
+        for (int cur = 0; cur < s.L; cur += s.B)
+            j.boxes.push_back(batch_box(j.led_host, cur, std::min(s.B, s.L - cur), whole, s.H));
+    } else {
+        Support sup;
+        rc = pupil_support(ctx, p, s, sup);
+        if (rc != FPM_OK) return rc;
+        j.pl = make_plan(s, j.led_host, p->batch, sup, p->loss_kind, p->pie_weights);
+        rc = alloc_pipeline(ctx, p, s, j.pl, j.res.spectrum != nullptr);
+        if (rc != FPM_OK) return rc;
+    }
     cudaStream_t st = ctx->stream;
     ctx->prof.reset();
-    Inputs in;
-    rc = stage_inputs(ctx, p, s, in);
+    rc = stage_inputs(ctx, p, s, j.in);
     if (rc != FPM_OK) return rc;
-    Twiddles tw;
-    rc = twiddles_of(ctx, s, tw);
-    if (rc != FPM_OK) return rc;
-
+    if (!j.generic) {
+        rc = twiddles_of(ctx, s, j.tw);
+        if (rc != FPM_OK) return rc;
+    }
     // object and pupil: work in the caller's device outputs when given, else internal
-    float2 *O, *P;
-    if (dev && res->object) {
-        O = reinterpret_cast<float2 *>(res->object);
+    if (dev && j.res.object) {
+        j.O = reinterpret_cast<float2 *>(j.res.object);
     } else {
         FPM_CK(ctx->O.ensure(s.big * 8));
-        O = ctx->O.as<float2>();
+        j.O = ctx->O.as<float2>();
     }
-    if (dev && res->pupil) {
-        P = reinterpret_cast<float2 *>(res->pupil);
+    if (dev && j.res.pupil) {
+        j.P = reinterpret_cast<float2 *>(j.res.pupil);
     } else {
         FPM_CK(ctx->P.ensure(s.plane * 8));
-        P = ctx->P.as<float2>();
+        j.P = ctx->P.as<float2>();
     }
     const cudaMemcpyKind kin = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if (p->object_init) {
-        if ((const void *)p->object_init != (const void *)O)
-            FPM_CK(copy_in(ctx, O, p->object_init, s.big * 8, kin));
+        if ((const void *)p->object_init != (const void *)j.O)
+            FPM_CK(copy_in(ctx, j.O, p->object_init, s.big * 8, kin));
     } else {
-        FPM_CK(ctx->T2.ensure(bicubic_work_bytes(s.h, s.pratio)));   // scratch before the loop
-        FPM_CK(launch_bicubic_init(in.Y, s.h, s.pratio, O, ctx->T2.p, st));
+        DevBuf &scratch = j.generic ? ctx->Rs : ctx->T2;   // not in use before the loop
+        FPM_CK(scratch.ensure(bicubic_work_bytes(s.h, s.pratio)));
+        FPM_CK(launch_bicubic_init(j.in.Y, s.h, s.pratio, j.O, scratch.p, st));
     }
-    if ((const void *)p->pupil_init != (const void *)P)
-        FPM_CK(copy_in(ctx, P, p->pupil_init, s.plane * 8, kin));
-    const float *P0;
+    if ((const void *)p->pupil_init != (const void *)j.P)
+        FPM_CK(copy_in(ctx, j.P, p->pupil_init, s.plane * 8, kin));
     if (dev) {
-        P0 = p->pupil_amp;
+        j.P0 = p->pupil_amp;
     } else {
         FPM_CK(ctx->P0.ensure(s.plane * 4));
-        FPM_STAGE(ST_H2D, cudaMemcpyAsync(ctx->P0.p, p->pupil_amp, s.plane * 4, kin, st));
-        P0 = ctx->P0.as<float>();
+        FPM_CK(copy_in(ctx, ctx->P0.p, p->pupil_amp, s.plane * 4, kin));
+        j.P0 = ctx->P0.as<float>();
     }
     FPM_CK(ctx->m1.ensure(s.big * 4));
     FPM_CK(ctx->m2.ensure(s.plane * 4));
     FPM_CK(cudaMemsetAsync(ctx->m1.p, 0, s.big * 4, st));
     FPM_CK(cudaMemsetAsync(ctx->m2.p, 0, s.plane * 4, st));
     const int E = p->epochs;
-    FPM_CK(ctx->loss.ensure(sizeof(double) * std::max(E, 1)));
-    FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double) * std::max(E, 1), st));
-
-    const int nbatch = (int)pl.geoms.size();
-    if (E > 0) {
-        rc = spectrum_box(ctx, pl, tw, O, pl.geoms[0]);
+    // E epoch slots, the accumulator of a captured epoch, and (as an int) its slot index
+    FPM_CK(ctx->loss.ensure(sizeof(double) * (E + 2)));
+    FPM_CK(cudaMemsetAsync(ctx->loss.p, 0, sizeof(double) * (E + 2), st));
+    j.loss = ctx->loss.as<double>();
+    j.epoch_counter = reinterpret_cast<int *>(j.loss + E + 1);
+    if (!j.generic && E > 0) {
+        rc = spectrum_box(ctx, j.pl, j.tw, j.O, j.pl.geoms[0]);
         if (rc != FPM_OK) return rc;
     }
-    float lr = p->lr;
-    for (int ep = 0; ep < E; ++ep) {
-        for (int bi = 0; bi < nbatch; ++bi) {
-            const BatchGeom &g = pl.geoms[bi];
-            const bool last = ep == E - 1 && bi == nbatch - 1;
-            const BatchGeom &gn = pl.geoms[(bi + 1) % nbatch];
-            rc = lowres_and_stitch(ctx, pl, tw, in, P, g, ctx->loss.as<double>() + ep);
+    j.lr = p->lr;
+    return FPM_OK;
+}
+
+// Enqueues one epoch; the batches' losses are added to *loss_slot.  In the final epoch
+// (final) the last batch skips the spectrum of the next box, which nothing reads.
+static fpm_status job_epoch(fpm_context *ctx, SolveJob &j, double *loss_slot, bool final) {
+    const Shape &s = j.s;
+    const fpm_problem *p = j.p;
+    cudaStream_t st = ctx->stream;
+    fpm_status rc;
+    if (j.generic) {
+        for (int bi = 0, cur = 0; cur < s.L; ++bi, cur += s.B) {   // cuFPM_pure_v3.cu:131-141
+            const int nb = std::min(s.B, s.L - cur);
+            rc = gen_batch(ctx, s, j.in, j.O, j.P, cur, nb, j.boxes[bi], loss_slot, p->loss_kind);
             if (rc != FPM_OK) return rc;
-            ColsArgs a;
-            a.mode = kColsUpdate;
-            a.H = s.H;
-            a.U = ctx->U.as<float2>();
-            a.ldU = pl.ldU;
-            a.Ru0 = g.Ru0;
-            a.rspan = g.rspan;
-            a.O = O;
-            a.m = ctx->m1.as<float>();
-            a.lr = lr;
-            a.beta = p->beta;
-            a.eps = p->eps;
-            a.V = ctx->V.as<float2>();
-            a.ldV = pl.ldU;
-            a.Ru0n = last ? 0 : gn.Ru0;
-            a.rspan_n = last ? 0 : gn.rspan;
-            a.err = ctx->flag.as<int>();
-            FPM_STAGE(ST_COLS_UPDATE, launch_big_cols(a, tw, st));
-            if (!last) {
-                rc = rows_forward(ctx, pl, tw, gn);
-                if (rc != FPM_OK) return rc;
-            }
+            FPM_STAGE(ST_GEN_RMS_OBJ, launch_rmsprop_object(j.O, ctx->m1.as<float>(),
+                                                            ctx->U.as<float2>(), s.big, j.lr,
+                                                            p->beta, p->eps, st));
             FPM_STAGE(ST_RMS_PUPIL,
-                      launch_rmsprop_pupil(ctx->dP.as<float2>(), P, ctx->m2.as<float>(), P0,
-                                           (int)s.plane, lr, p->beta, p->eps, p->pupil_margin,
+                      launch_rmsprop_pupil(ctx->dP.as<float2>(), j.P, ctx->m2.as<float>(), j.P0,
+                                           (int)s.plane, j.lr, p->beta, p->eps, p->pupil_margin,
                                            st));
         }
-        if (ep > p->lr_halve_after) lr = (float)(lr * (double)p->lr_decay);
+        return FPM_OK;
     }
+    const Plan &pl = j.pl;
+    const int nbatch = (int)pl.geoms.size();
+    for (int bi = 0; bi < nbatch; ++bi) {
+        const BatchGeom &g = pl.geoms[bi];
+        const bool last = final && bi == nbatch - 1;
+        const BatchGeom &gn = pl.geoms[(bi + 1) % nbatch];
+        rc = lowres_and_stitch(ctx, pl, j.tw, j.in, j.P, g, loss_slot);
+        if (rc != FPM_OK) return rc;
+        ColsArgs a;
+        a.mode = kColsUpdate;
+        a.H = s.H;
+        a.U = ctx->U.as<float2>();
+        a.ldU = pl.ldU;
+        a.Ru0 = g.Ru0;
+        a.rspan = g.rspan;
+        a.O = j.O;
+        a.m = ctx->m1.as<float>();
+        a.lr = j.lr;
+        a.beta = p->beta;
+        a.eps = p->eps;
+        a.V = ctx->V.as<float2>();
+        a.ldV = pl.ldU;
+        a.Ru0n = last ? 0 : gn.Ru0;
+        a.rspan_n = last ? 0 : gn.rspan;
+        a.err = ctx->flag.as<int>();
+        FPM_STAGE(ST_COLS_UPDATE, launch_big_cols(a, j.tw, st));
+        if (!last) {
+            rc = rows_forward(ctx, pl, j.tw, gn);
+            if (rc != FPM_OK) return rc;
+        }
+        FPM_STAGE(ST_RMS_PUPIL,
+                  launch_rmsprop_pupil(ctx->dP.as<float2>(), j.P, ctx->m2.as<float>(), j.P0,
+                                       (int)s.plane, j.lr, p->beta, p->eps, p->pupil_margin, st));
+    }
+    return FPM_OK;
+}
 
-    // outputs
+// lr schedule after epoch `ep` (cuFPM_pure_v3.cu:204-206)
+static void job_lr_after(SolveJob &j, int ep) {
+    if (ep > j.p->lr_halve_after) j.lr = (float)(j.lr * (double)j.p->lr_decay);
+}
+
+// One epoch captured from the context's stream into an executable graph.  Every replay
+// adds its batches' losses to the accumulator slot, then moves the accumulator to the slot
+// the device-side epoch counter names and advances the counter, so one graph serves every
+// epoch that shares the learning rate.  *exec stays null when the capture did not succeed
+// (a call the capture refused, or any failure while recording: nothing ran, and the caller
+// runs the epochs eagerly, where a genuine error shows up again).
+static fpm_status job_capture(fpm_context *ctx, SolveJob &j, cudaGraphExec_t *exec) {
+    *exec = nullptr;
+    cudaStream_t st = ctx->stream;
+    const bool prof = ctx->prof.on;
+    ctx->prof.on = false;   // no stage events inside a graph
+    const int E = j.p->epochs;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->prof.on = prof;
+        return FPM_OK;
+    }
+    const fpm_status rc = job_epoch(ctx, j, j.loss + E, false);
+    cudaError_t le = cudaSuccess;
+    if (rc == FPM_OK) le = launch_epoch_end(j.loss + E, j.loss, j.epoch_counter, st);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(st, &graph);
+    ctx->prof.on = prof;
+    if (rc != FPM_OK || le != cudaSuccess || e != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        ctx->err.clear();
+        return FPM_OK;
+    }
+    e = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        *exec = nullptr;
+        cudaGetLastError();
+    }
+    return FPM_OK;
+}
+
+static fpm_status job_finish(fpm_context *ctx, SolveJob &j) {
+    const Shape &s = j.s;
+    const bool dev = j.dev;
+    cudaStream_t st = ctx->stream;
+    fpm_result *res = &j.res;
+    const int E = j.p->epochs;
+    fpm_status rc;
     if (res->spectrum) {
         float2 *dst = reinterpret_cast<float2 *>(res->spectrum);
         if (!dev) {  // stage through a full-size device buffer
             FPM_CK(ctx->S.ensure(s.big * 8));
             dst = ctx->S.as<float2>();
         }
-        rc = centred_spectrum(ctx, s, O, dst);
-        if (rc != FPM_OK) return rc;
+        if (j.generic) {
+            FPM_STAGE(ST_SPECTRUM,
+                      ctx->gfft.fft2(j.O, dst, ctx->W.as<float2>(), s.H, 1, kForward, st));
+            FPM_CK(launch_centre_in_place(dst, s.H, st));
+        } else {
+            rc = centred_spectrum(ctx, s, j.O, dst);
+            if (rc != FPM_OK) return rc;
+        }
         if (!dev)
             FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->spectrum, dst, s.big * 8,
                                               cudaMemcpyDeviceToHost, st));
     }
     if (!dev && res->object)
-        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->object, O, s.big * 8, cudaMemcpyDeviceToHost, st));
+        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->object, j.O, s.big * 8, cudaMemcpyDeviceToHost, st));
     if (!dev && res->pupil)
-        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->pupil, P, s.plane * 8, cudaMemcpyDeviceToHost, st));
+        FPM_STAGE(ST_D2H, cudaMemcpyAsync(res->pupil, j.P, s.plane * 8, cudaMemcpyDeviceToHost, st));
     std::vector<double> loss_h(std::max(E, 1));
-    FPM_CK(cudaMemcpyAsync(loss_h.data(), ctx->loss.p, sizeof(double) * std::max(E, 1),
+    FPM_CK(cudaMemcpyAsync(loss_h.data(), j.loss, sizeof(double) * std::max(E, 1),
                            cudaMemcpyDeviceToHost, st));
     if (res->loss && dev && E > 0)
-        FPM_CK(cudaMemcpyAsync(res->loss, ctx->loss.p, sizeof(double) * E,
-                               cudaMemcpyDeviceToDevice, st));
+        FPM_CK(cudaMemcpyAsync(res->loss, j.loss, sizeof(double) * E, cudaMemcpyDeviceToDevice, st));
     FPM_CK(cudaStreamSynchronize(st));
     FPM_CK(cudaGetLastError());
     ctx->prof.collect();
@@ -1123,6 +1139,114 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
         if (!std::isfinite(loss_h[ep]))
             return fail(ctx, FPM_ERR_NONFINITE, "loss of epoch %d is not finite", ep);
     return FPM_OK;
+}
+
+// The epochs of a prepared job: epoch 0 eagerly (it builds every table and sets every
+// kernel attribute the capture would otherwise meet), then one captured graph per learning
+// rate, replayed once per epoch.  Without graphs (FPM_GRAPHS=0, stage profiling on, or a
+// stream that cannot be captured) every epoch launches its kernels directly.
+static fpm_status job_run_epochs(fpm_context *ctx, SolveJob &j, bool graphs) {
+    const int E = j.p->epochs;
+    cudaStream_t st = ctx->stream;
+    fpm_status rc;
+    if (E <= 0) return FPM_OK;
+    rc = job_epoch(ctx, j, j.loss, E == 1);
+    if (rc != FPM_OK) return rc;
+    job_lr_after(j, 0);
+    cudaGraphExec_t exec = nullptr;
+    float exec_lr = 0.f;
+    for (int ep = 1; ep < E; ++ep) {
+        if (graphs && (!exec || exec_lr != j.lr)) {
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
+            FPM_CK(launch_set_int(j.epoch_counter, ep, st));   // the slot of the next replay
+            rc = job_capture(ctx, j, &exec);
+            if (rc != FPM_OK) return rc;
+            exec_lr = j.lr;
+            if (!exec) graphs = false;
+        }
+        if (exec) {
+            const cudaError_t e = cudaGraphLaunch(exec, st);
+            if (e != cudaSuccess) {
+                cudaGraphExecDestroy(exec);
+                return fail_cuda(ctx, e, "cudaGraphLaunch", __LINE__);
+            }
+        } else {
+            rc = job_epoch(ctx, j, j.loss + ep, ep == E - 1);
+            if (rc != FPM_OK) return rc;
+        }
+        job_lr_after(j, ep);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    return FPM_OK;
+}
+
+static bool graphs_enabled(const fpm_context *ctx) {
+    if (ctx->prof.on) return false;
+    const char *env = std::getenv("FPM_GRAPHS");
+    return !(env && std::atoi(env) == 0);
+}
+
+fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
+    SolveJob j;
+    fpm_status rc = job_prepare(ctx, p, res, j);
+    if (rc != FPM_OK) return rc;
+    rc = job_run_epochs(ctx, j, graphs_enabled(ctx));
+    if (rc != FPM_OK) return rc;
+    return job_finish(ctx, j);
+}
+
+// Worker contexts of fpm_solve_batch: one per instance (its buffers stay allocated for
+// the next call), on a pool of kBatchStreams streams owned by the parent context.
+static constexpr int kBatchStreams = 8;
+
+fpm_status fpm_solve_batch(fpm_context *ctx, const fpm_problem *problems, fpm_result *results,
+                           int32_t n, int32_t flags, fpm_status *statuses) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (!problems || n < 1) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "no problems (n = %d)", n);
+    if (flags & ~FPM_BATCH_EAGER) return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "flags = %d", flags);
+    FPM_CK(cudaSetDevice(ctx->device));
+    while ((int)ctx->pool.size() < std::min(n, kBatchStreams)) {
+        cudaStream_t sp = nullptr;
+        FPM_CK(cudaStreamCreateWithFlags(&sp, cudaStreamNonBlocking));
+        ctx->pool.push_back(sp);
+    }
+    while ((int)ctx->workers.size() < n) {
+        const int i = (int)ctx->workers.size();
+        fpm_device_opts o{};
+        o.device = ctx->device;
+        o.mem_limit_bytes = ctx->mem_limit;
+        o.stream = ctx->pool[i % ctx->pool.size()];
+        fpm_context *w = nullptr;
+        const fpm_status cs = fpm_create(&w, &o);
+        if (cs != FPM_OK) return fail(ctx, cs, "worker context %d: %s", i, fpm_status_string(cs));
+        ctx->workers.push_back(w);
+    }
+    const bool graphs = !(flags & FPM_BATCH_EAGER) && graphs_enabled(ctx);
+    std::vector<SolveJob> jobs(n);
+    std::vector<fpm_status> st(n, FPM_OK);
+    // prepare every instance, then enqueue every instance's epochs (no host waits between
+    // them: the instances run concurrently on the pool's streams), then finish each
+    for (int i = 0; i < n; ++i)
+        st[i] = job_prepare(ctx->workers[i], &problems[i], results ? &results[i] : nullptr, jobs[i]);
+    for (int i = 0; i < n; ++i)
+        if (st[i] == FPM_OK) st[i] = job_run_epochs(ctx->workers[i], jobs[i], graphs);
+    fpm_status first = FPM_OK;
+    for (int i = 0; i < n; ++i) {
+        if (st[i] == FPM_OK) {
+            st[i] = job_finish(ctx->workers[i], jobs[i]);
+        } else {
+            cudaStreamSynchronize(ctx->workers[i]->stream);   // nothing left in flight
+            cudaGetLastError();
+        }
+        if (st[i] != FPM_OK && first == FPM_OK) {
+            first = st[i];
+            fail(ctx, st[i], "instance %d: %s", i, ctx->workers[i]->err.c_str());
+        }
+        if (statuses) statuses[i] = st[i];
+    }
+    return first;
 }
 
 fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_object,

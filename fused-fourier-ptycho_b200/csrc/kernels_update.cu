@@ -219,6 +219,27 @@ cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cud
     return cudaGetLastError();
 }
 
+// End of a captured epoch: its accumulated loss goes to the slot the counter names, the
+// accumulator restarts at zero and the counter moves to the next epoch.
+__global__ void k_epoch_end(double *acc, double *loss, int *counter) {
+    const int ep = *counter;
+    loss[ep] = *acc;
+    *acc = 0.0;
+    *counter = ep + 1;
+}
+
+cudaError_t launch_epoch_end(double *acc, double *loss, int *counter, cudaStream_t st) {
+    k_epoch_end<<<1, 1, 0, st>>>(acc, loss, counter);
+    return cudaGetLastError();
+}
+
+__global__ void k_set_int(int *p, int v) { *p = v; }
+
+cudaError_t launch_set_int(int *p, int v, cudaStream_t st) {
+    k_set_int<<<1, 1, 0, st>>>(p, v);
+    return cudaGetLastError();
+}
+
 // Global min / max of a uint16 stack (integer atomics: order-independent).
 __global__ void __launch_bounds__(256) k_stack_minmax(const uint16_t *__restrict__ p, size_t n,
                                                        unsigned *__restrict__ mm) {

@@ -42,7 +42,7 @@ EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_sta
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
             "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
             "fpm_led_indices", "fpm_simulate", "fpm_normalise_stack_f32", "fpm_read_tiff_stack",
-            "fpm_optimizer_step"]
+            "fpm_optimizer_step", "fpm_solve_batch"]
 
 
 SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
@@ -117,6 +117,9 @@ def load_library(path: str | Path | None = None):
     lib.fpm_create.restype = C.c_int
     lib.fpm_solve.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.fpm_solve.restype = C.c_int
+    lib.fpm_solve_batch.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result), C.c_int32,
+                                    C.c_int32, C.c_void_p]
+    lib.fpm_solve_batch.restype = C.c_int
     lib.fpm_batch_gradients.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_void_p, C.c_void_p,
                                         C.c_void_p]
     lib.fpm_batch_gradients.restype = C.c_int
@@ -305,6 +308,46 @@ class Engine:
         self._check(self.solve_raw(prob, res))
         del keep
         return {"object": o, "pupil": p, "spectrum": s, "loss": loss[: int(epochs)]}
+
+    def solve_batch(self, instances, eager=False, spectrum=False):
+        """Many independent reconstructions in one fpm_solve_batch call.  instances: a list
+        of dicts with the arguments of solve (O0, P0c, Y, led_idx, P0, pratio, epochs, batch
+        and optionally lr, beta, eps, am, lr_halve_after, lr_decay, loss, pie); returns
+        (results, statuses) with one solve-style dict per instance."""
+        n = len(instances)
+        probs = (Problem * n)()
+        ress = (Result * n)()
+        keep, outs = [], []
+        for i, a in enumerate(instances):
+            kw = dict(lr=5e-4, beta=0.999, eps=1e-4, am=0.2, lr_halve_after=12, lr_decay=0.5,
+                      loss="anisotropic", pie="none")
+            kw.update({k: a[k] for k in kw if k in a})
+            prob, kp, mem = self._problem(a["O0"], a["P0c"], a["Y"], a["led_idx"], a["P0"],
+                                          a["pratio"], a["epochs"], a["batch"], kw["lr"],
+                                          kw["beta"], kw["eps"], kw["am"], kw["lr_halve_after"],
+                                          kw["lr_decay"], kw["loss"], kw["pie"])
+            keep.append(kp)
+            h = prob.h
+            H = h * prob.pratio
+            like = a["Y"] if mem == MEM_DEVICE else None
+            op, o = _empty_like_layout((H, H), np.complex64, like)
+            pp, pu = _empty_like_layout((h, h), np.complex64, like)
+            sp, sv = (None, None)
+            if spectrum:
+                sp, sv = _empty_like_layout((H, H), np.complex64, like)
+            lp, lo = _empty_like_layout((max(int(a["epochs"]), 1),), np.float64, like)
+            probs[i] = prob
+            ress[i] = Result(object=op, spectrum=sp, pupil=pp, loss=lp)
+            outs.append({"object": o, "pupil": pu, "spectrum": sv,
+                         "loss": lo[: int(a["epochs"])]})
+        st = (C.c_int * n)()
+        _inputs_ready(*[x for kp in keep for x in kp])
+        rc = self.lib.fpm_solve_batch(self._ctx, probs, ress, n, 1 if eager else 0, st)
+        statuses = [int(x) for x in st]
+        if rc != FPM_OK and all(x != FPM_OK for x in statuses):
+            self._check(rc)
+        del keep
+        return outs, statuses
 
     def batch_gradients(self, O, P, Y, led_idx, P0, pratio, loss="anisotropic", pie="none"):
         """v3 gradients of one LED batch (the fullyfusedFPM contract): (dO, dP, loss)."""

@@ -146,8 +146,27 @@ typedef struct fpm_context fpm_context;
 /* Replaces mxInitGPU + the per-call set-up of cuFPM_pure_v3.cu:49-126. */
 fpm_status fpm_create(fpm_context **ctx, const fpm_device_opts *opts);
 
-/* Replaces the body of mexFunction, cuFPM_pure_v3.cu:44-228. */
+/* Replaces the body of mexFunction, cuFPM_pure_v3.cu:44-228.  Every epoch after the
+   first is replayed from a CUDA graph captured once per learning rate (the reference
+   launches every kernel and synchronises after every mini-batch,
+   cuFPM_pure_v3.cu:202); with stage profiling on (fpm_set_profiling) the epochs run
+   eagerly. */
 fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *prob, fpm_result *res);
+
+/* Many independent reconstructions in one call: tiles of a large field of view, or
+   instances of different sizes (h, L, pratio, B may differ).  No counterpart in the
+   reference, which runs one reconstruction per mex call (cuFPM_pure_v3.cu:44).
+   problems[i] / results[i] follow fpm_solve's rules one by one.  The instances run
+   concurrently: each on a worker context of its own (its buffers stay allocated for
+   the next call; the parent's mem_limit_bytes caps each instance) over a pool of up to
+   8 streams, every instance's epochs after the first replayed from one captured CUDA
+   graph per learning rate.  flags: FPM_BATCH_EAGER launches every epoch's kernels
+   directly instead.  statuses (optional, n entries) receives each instance's status;
+   the return value is the first failing instance's (FPM_OK when all succeed), with its
+   detail in fpm_last_error(ctx).  Results equal those of n separate fpm_solve calls. */
+#define FPM_BATCH_EAGER 1
+fpm_status fpm_solve_batch(fpm_context *ctx, const fpm_problem *problems, fpm_result *results,
+                           int32_t n, int32_t flags, fpm_status *statuses);
 
 /* Gradients of one LED batch at (object, pupil), v3 loss: replaces
    fullyfusedFPM (codes/fusedfpm/fullyfusedFPM.cu:24-169).  prob->n_leds LEDs

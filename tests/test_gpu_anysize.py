@@ -65,10 +65,13 @@ def test_any_size_solve_vs_oracle(engine, h, p):
 @pytest.mark.parametrize("h,p", [(48, 4), (80, 3)])
 def test_any_size_uint16_and_isotropic(engine, h, p):
     """uint16 frames (normalised on the device) and both losses on the any-size path, one
-    epoch, against the FP64 oracle on the normalised amplitudes.  Poisson frames hold
-    quantised counts, so residual differences near zero are common and the anisotropic
-    loss's signs there depend on the FFT's rounding: the bar is the larger distance of two
-    FP32 twins with different FFTs (numpy's pocketfft and cuFFT through torch)."""
+    epoch, against the FP64 oracle on the normalised amplitudes.  The isotropic loss must
+    sit within 2e-5 (or 3x the FP32 twins' distance).  Poisson frames hold quantised
+    counts: equal neighbouring counts make the FP32 residual difference exactly zero when
+    the two |z| round together, so the anisotropic loss's sign there follows the rounding
+    of the transforms, a single LED's gradient then moves by ~1e-2 (measured: LED 5 of the
+    80 x 3 case flips in the engine and in the twin alike, LED 8 in the engine only), and
+    the object after one epoch by ~1e-4: the anisotropic bar is max(1e-3, 3x the twins)."""
     import torch
     from oracle import torch_ref as tr
     ds = dataset(h, p, 5, seed=3, aberration=True)
@@ -87,7 +90,8 @@ def test_any_size_uint16_and_isotropic(engine, h, p):
             e32 = max(orc.rel_err(getattr(o32, k), getattr(o64, k)),
                       orc.rel_err(c32[k].cpu().numpy(), getattr(o64, k)))
             print(f"{h} {p} {loss} {k}: engine {e:.3e} twins {e32:.3e}")
-            assert e < max(TIGHT, 3 * e32), (loss, k, e, e32)
+            bar = max(TIGHT if loss == "isotropic" else 1e-3, 3 * e32)
+            assert e < bar, (loss, k, e, e32)
         np.testing.assert_allclose(r["loss"], o64.loss, rtol=1e-5)
 
 
