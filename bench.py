@@ -605,6 +605,136 @@ def accuracy_for(cfg: Cfg, wl, s_per_epoch: float, epochs: int = JOB_EPOCHS):
     return out
 
 
+def make_instances_gpu(n: int, seed: int, dev):
+    """Seeded uneven instances of the batched configuration: low-res side uniform in
+    {128, 192, 256, 384, 512}, LED grid in {11, 13, 15, 17, 19} (121-361 LEDs), up-sampling
+    uniform in 4..8, each a smooth random object, the circular pupil of the optics, and
+    uint16 frames (Poisson at 3e4 peak counts) of its forward model; generated with torch
+    on the GPU, arrays in column-major memory as the C ABI takes them."""
+    import torch
+    from fpm_b200 import synth
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    out = []
+    for i in range(n):
+        h = int(rng.choice([128, 192, 256, 384, 512]))
+        grid = int(rng.choice([11, 13, 15, 17, 19]))
+        p = int(rng.integers(4, 9))
+        H = h * p
+        f0 = torch.fft.fftfreq(H, device=dev)
+        f1 = torch.fft.rfftfreq(H, device=dev)
+
+        def smooth(x, sigma):
+            X = torch.fft.rfft2(x)
+            X *= torch.exp(-2 * (math.pi * sigma) ** 2 * f0 * f0)[:, None]
+            X *= torch.exp(-2 * (math.pi * sigma) ** 2 * f1 * f1)[None, :]
+            y = torch.fft.irfft2(X, s=(H, H))
+            return (y - y.min()) / (y.max() - y.min())
+        amp = 0.5 + 0.5 * smooth(torch.rand((H, H), generator=g, device=dev), 3.0)
+        ph = (smooth(torch.randn((H, H), generator=g, device=dev), 4.0) - 0.5) * math.pi
+        spec = torch.fft.fftshift(torch.fft.fft2(torch.polar(amp, ph)))
+        del amp, ph
+        optics = synth.Optics(led_grid=grid)
+        circ = synth.pupil_circle(h, optics)
+        P = torch.from_numpy(circ.astype(np.complex64)).to(dev)
+        led = synth.led_indices(h, p, optics)
+        ar = torch.arange(h, device=dev)
+        frames = []
+        for kl, kt in led:
+            sub = spec.index_select(0, (int(kt) - 1 + ar) % H).index_select(1, (int(kl) - 1 + ar) % H)
+            x = torch.fft.ifft2(torch.fft.ifftshift(sub * P)) / (p * p)
+            frames.append(x.real ** 2 + x.imag ** 2)
+        del spec
+        I = torch.stack(frames)
+        counts = torch.poisson(I * (3e4 / float(I.max())), generator=g).clamp_(max=65535)
+        stack = counts.to(torch.int32).transpose(1, 2).contiguous().to(torch.uint16)   # [l][c][r]
+        del I, counts, frames
+        P0 = torch.from_numpy(np.ascontiguousarray(circ.T)).to(dev)
+        out.append({"h": h, "pratio": p, "L": len(led), "stack": stack, "P0": P0,
+                    "P0c": P0.to(torch.complex64),
+                    "led": torch.from_numpy(np.ascontiguousarray(led, np.int32)).to(dev)})
+    torch.cuda.synchronize(dev)
+    return out
+
+
+def run_instances(args, cfg: Cfg):
+    """The batched-instances configuration: 48 independent reconstructions of uneven size
+    (low-res side 128-512, 121-361 LEDs, up-sampling 4-8, LED batch 26, 10 epochs), run by
+    one fpm_solve_batch call (concurrent instances on a pool of streams, epochs replayed
+    from captured graphs) against the same instances solved one by one with fpm_solve;
+    aggregate LED-updates/s.  One GPU."""
+    import ctypes as C
+    import torch
+    import fpm_b200
+    from fpm_b200 import api
+    dev = torch.device("cuda", 0)
+    n, E = args.instances, JOB_EPOCHS
+    inst = make_instances_gpu(n, 1000 + cfg.seed, dev)
+    eng = fpm_b200.Engine(0)
+    probs = (api.Problem * n)()
+    ress = (api.Result * n)()
+    outs = []
+    for i, a in enumerate(inst):
+        H, h = a["h"] * a["pratio"], a["h"]
+        O = torch.empty((H, H), dtype=torch.complex64, device=dev)
+        P = torch.empty((h, h), dtype=torch.complex64, device=dev)
+        probs[i] = api.Problem(h=h, n_leds=a["L"], pratio=a["pratio"], batch=cfg.batch, epochs=E,
+                               lr=cfg.lr, beta=cfg.beta, eps=cfg.eps, pupil_margin=0.2,
+                               lr_halve_after=12, lr_decay=0.5, loss_kind=0, memory=api.MEM_DEVICE,
+                               stack_type=api.STACK_U16, stack=a["stack"].data_ptr(),
+                               led_idx=a["led"].data_ptr(), pupil_init=a["P0c"].data_ptr(),
+                               pupil_amp=a["P0"].data_ptr(), object_init=None)
+        ress[i] = api.Result(object=O.data_ptr(), spectrum=None, pupil=P.data_ptr(), loss=None)
+        outs.append((O, P))
+    st = (C.c_int * n)()
+
+    def batch_call(eager=False):
+        rc = eng.lib.fpm_solve_batch(eng._ctx, probs, ress, n, 1 if eager else 0, st)
+        eng._check(rc)
+
+    def one_by_one():
+        for i in range(n):
+            eng._check(eng.solve_raw(probs[i], ress[i]))
+
+    led_updates = sum(a["L"] for a in inst) * E
+    timings = {}
+    for name, fn in (("one_by_one", one_by_one), ("batch_eager", lambda: batch_call(True)),
+                     ("batch", batch_call)):
+        fn()                                   # warm-up: buffers, tables, kernel attributes
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            fn()                               # each call returns after its results are ready
+            ts.append(time.perf_counter() - t0)
+        timings[name] = float(np.median(ts))
+        if name == "one_by_one":
+            ref = [(O.clone(), P.clone()) for O, P in outs]
+    same = all(torch.equal(O, r[0]) and torch.equal(P, r[1]) for (O, P), r in zip(outs, ref))
+    value = led_updates / timings["batch"]
+    line = {"metric": "aggregate LED-updates/s, 48 uneven FPM instances (fpm_solve_batch)",
+            "value": round(value, 1), "unit": "LED-updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": round(timings["batch"] * 1e3, 2),
+            "higher_is_better": True, "dtype": "f32 (complex64)",
+            "data": "synthetic (seeded, generated on GPU)",
+            "config": {"workload": f"{n} independent reconstructions, low-res side in "
+                                   "{128,192,256,384,512}, 121-361 LEDs, up-sampling 4-8, "
+                                   f"LED batch {cfg.batch}, {E} epochs, uint16 frames",
+                       "instances": [(a["h"], a["L"], a["pratio"]) for a in inst],
+                       "led_updates_per_job": led_updates,
+                       "step": "one call solving every instance (10 epochs each)"},
+            "one_by_one_led_updates_per_s": round(led_updates / timings["one_by_one"], 1),
+            "batch_eager_led_updates_per_s": round(led_updates / timings["batch_eager"], 1),
+            "speedup_vs_one_by_one": round(timings["one_by_one"] / timings["batch"], 3),
+            "seconds": {k: round(v, 4) for k, v in timings.items()},
+            "batch_equals_one_by_one_bitwise": bool(same),
+            "timing": "host wall clock around each call (each returns after its final "
+                      "synchronisation), median of the steps"}
+    eng.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_simulate(args, cfg: Cfg):
     """Forward model (fpm_simulate): all LED images of a 16384^2 object, device-resident.
     Not the headline metric: a separate line for the simulator row."""
@@ -922,10 +1052,12 @@ def main():
     ap.add_argument("--grid", type=int, default=19)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--instances", type=int, default=48,
+                    help="instances of the batched workload (--workload instances)")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the per-epoch error against the FP64 run (one GPU only)")
     ap.add_argument("--workload", default="solve",
-                    choices=["solve", "simulate", "ingest", "optimizer"],
+                    choices=["solve", "simulate", "ingest", "optimizer", "instances"],
                     help="solve: the reconstruction (headline); simulate: the forward model; "
                          "ingest: TIFF frames to normalised amplitude; optimizer: the MATLAB "
                          "optimiser classes' step on the object")
@@ -939,7 +1071,8 @@ def main():
         run_reference(args, cfg)
         return
     if args.workload != "solve":
-        {"simulate": run_simulate, "ingest": run_ingest, "optimizer": run_optimizer}[args.workload](args, cfg)
+        {"simulate": run_simulate, "ingest": run_ingest, "optimizer": run_optimizer,
+         "instances": run_instances}[args.workload](args, cfg)
         return
     out, wl, rank, world = run_ours(args, cfg)
     if rank == 0:

