@@ -5,6 +5,7 @@
 
 #include "fft.h"
 #include "fft_core.cuh"
+#include "tuning.h"
 
 namespace fpm {
 
@@ -114,8 +115,8 @@ template <int N, int DIR>
 cudaError_t run_n(const float2 *in, float2 *out, int count, int axes, const float2 *hi,
                   const float2 *lo, cudaStream_t st) {
     if constexpr (N == 16384) {
-        const char *env = std::getenv("FPM_COLS_E16");
-        if (!(env && std::atoi(env) != 0)) return run_ne<N, DIR, 32>(in, out, count, axes, hi, lo, st);
+        if (knob("FPM_COLS_E16", tuning().cols_e16, -1, 0) == 0)
+            return run_ne<N, DIR, 32>(in, out, count, axes, hi, lo, st);
     }
     return run_ne<N, DIR, 16>(in, out, count, axes, hi, lo, st);
 }

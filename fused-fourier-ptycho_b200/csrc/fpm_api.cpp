@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -28,6 +29,7 @@
 #include "generic.h"
 #include "pipeline.h"
 #include "tiff.h"
+#include "tuning.h"
 
 using namespace fpm;
 
@@ -168,6 +170,9 @@ struct fpm_context {
     // fpm_solve_batch: one worker context per instance, on a pool of streams
     std::vector<fpm_context *> workers;
     std::vector<cudaStream_t> pool;
+    // autotuner: the chosen launch choices per problem shape
+    int flags = 0;
+    std::map<std::vector<int>, Tuning> tuned;
 };
 
 namespace {
@@ -455,13 +460,13 @@ Plan make_plan(const Shape &s, const std::vector<int32_t> &led, int batch, const
     // at 4 GiB of field + residual; FPM_LR_GROUP overrides it (tuning).
     const size_t per = s.plane * 16;
     pl.group = (int)std::max<size_t>(1, std::min<size_t>(s.B, (4ull << 30) / per));
-    if (const char *env = std::getenv("FPM_LR_GROUP")) {
-        const int v = std::atoi(env);
-        if (v > 0) pl.group = std::min(v, s.B);
+    {
+        const int v = knob("FPM_LR_GROUP", tuning().lr_group, 0, 0);
+        if (v > 0) pl.group = std::min(v, pl.group);
     }
     // fused L2 + L3 where its CTA shape exists; FPM_LR_FUSED=0 keeps the separate passes
-    pl.fused_rows = lr_rows_fused_supported(s.h);
-    if (const char *env = std::getenv("FPM_LR_FUSED")) pl.fused_rows = pl.fused_rows && std::atoi(env) != 0;
+    pl.fused_rows = lr_rows_fused_supported(s.h) &&
+                    knob("FPM_LR_FUSED", tuning().lr_fused, -1, 1) != 0;
     // with the fused row pass the field buffer is written by L1 alone: its unsupported
     // columns, cleared once per solve, stay zero and L1 skips them
     const bool pruned_cols = sup.c_lo > 0 || sup.c_hi < s.h;
@@ -685,6 +690,7 @@ fpm_status fpm_create(fpm_context **out, const fpm_device_opts *opts) {
     fpm_context *ctx = new fpm_context();
     ctx->device = dev;
     ctx->mem_limit = opts ? opts->mem_limit_bytes : 0;
+    ctx->flags = opts ? opts->flags : 0;
     if (opts && opts->stream) {
         ctx->stream = static_cast<cudaStream_t>(opts->stream);
     } else {
@@ -1187,9 +1193,134 @@ static bool graphs_enabled(const fpm_context *ctx) {
     return !(env && std::atoi(env) == 0);
 }
 
-fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
+// ---------------------------------------------------------------------------
+// Autotuner: one epoch per candidate launch choice on the caller's own problem,
+// coordinate search from the defaults, the fastest kept per problem shape.
+// ---------------------------------------------------------------------------
+static std::vector<int> tune_key(const fpm_problem *p) {
+    return {p->h, p->pratio, p->n_leds, std::min(p->batch, p->n_leds), p->stack_type,
+            p->loss_kind, p->pie_weights};
+}
+
+// Device time of one eager epoch of p under tuning t (set-up excluded), outputs internal.
+static fpm_status time_epoch(fpm_context *ctx, const fpm_problem *p, const Tuning &t, float *ms) {
+    fpm_problem q = *p;
+    q.epochs = 1;
+    TuningScope scope(&t);
     SolveJob j;
-    fpm_status rc = job_prepare(ctx, p, res, j);
+    fpm_status rc = job_prepare(ctx, &q, nullptr, j);
+    if (rc != FPM_OK) return rc;
+    cudaEvent_t a = nullptr, b = nullptr;
+    FPM_CK(cudaEventCreate(&a));
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return fail(ctx, FPM_ERR_CUDA, "cudaEventCreate");
+    }
+    cudaEventRecord(a, ctx->stream);
+    rc = job_run_epochs(ctx, j, false);
+    cudaEventRecord(b, ctx->stream);
+    if (rc == FPM_OK) rc = job_finish(ctx, j);
+    if (rc == FPM_OK && cudaEventElapsedTime(ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(ctx, FPM_ERR_CUDA, "cudaEventElapsedTime");
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+}
+
+static std::string tuning_text(const Tuning &t) {
+    char buf[256];
+    snprintf(buf, sizeof buf, "lr_group=%d lr_fused=%d l23_cluster=%d cols_async=%d cols_e16=%d "
+             "gen_lpc=%d", t.lr_group, t.lr_fused, t.l23_cluster, t.cols_async, t.cols_e16,
+             t.gen_lpc);
+    return buf;
+}
+
+fpm_status fpm_autotune(fpm_context *ctx, const fpm_problem *p, char *report, size_t report_cap) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    Shape s;
+    fpm_status rc = shape_of(ctx, p, s, true);
+    if (rc != FPM_OK) return rc;
+    const std::vector<int> key = tune_key(p);
+    auto it = ctx->tuned.find(key);
+    std::string text;
+    if (it == ctx->tuned.end()) {
+        // candidate values of each knob, tried one knob at a time from the best so far
+        std::vector<std::pair<int Tuning::*, std::vector<int>>> knobs;
+        const bool generic = !pipeline_supported(s.h, s.H);
+        if (generic) {
+            knobs.push_back({&Tuning::gen_lpc, {1, 2, 4, 8, 16}});
+        } else {
+            std::vector<int> groups;
+            for (int g : {s.B / 2, 8, 4})
+                if (g >= 1 && g < s.B) groups.push_back(g);
+            knobs.push_back({&Tuning::lr_group, groups});
+            if (lr_rows_fused_supported(s.h)) {
+                knobs.push_back({&Tuning::lr_fused, {0}});
+                knobs.push_back({&Tuning::l23_cluster, {4}});
+            }
+            if (s.H == 16384) {
+                knobs.push_back({&Tuning::cols_async, {0}});
+                knobs.push_back({&Tuning::cols_e16, {1}});
+            }
+        }
+        Tuning best;
+        float best_ms = 0.f, first_ms = 0.f;
+        rc = time_epoch(ctx, p, best, &best_ms);        // warm-up: tables, attributes, buffers
+        if (rc == FPM_OK) rc = time_epoch(ctx, p, best, &best_ms);
+        if (rc != FPM_OK) return rc;
+        first_ms = best_ms;
+        int trials = 2;
+        for (const auto &kv : knobs) {
+            const Tuning base = best;
+            for (int v : kv.second) {
+                Tuning t = base;
+                t.*(kv.first) = v;
+                float ms = 0.f;
+                rc = time_epoch(ctx, p, t, &ms);
+                if (rc != FPM_OK) return rc;
+                ++trials;
+                if (ms < 0.98f * best_ms) best_ms = ms, best = t;   // 2%: beyond the noise
+            }
+        }
+        it = ctx->tuned.emplace(key, best).first;
+        char buf[512];
+        snprintf(buf, sizeof buf, "%s: %.3f ms/epoch (defaults %.3f ms, %d timed epochs)",
+                 tuning_text(best).c_str(), best_ms, first_ms, trials);
+        text = buf;
+    } else {
+        text = tuning_text(it->second) + " (cached)";
+    }
+    if (report && report_cap) {
+        std::strncpy(report, text.c_str(), report_cap - 1);
+        report[report_cap - 1] = '\0';
+    }
+    return FPM_OK;
+}
+
+// The tuning of p's shape: tuned now when the context asks for it, else the cached one.
+static const Tuning *tuning_for(fpm_context *ctx, const fpm_problem *p, fpm_status *rc) {
+    *rc = FPM_OK;
+    if (!p) return nullptr;
+    auto it = ctx->tuned.find(tune_key(p));
+    if (it == ctx->tuned.end() && (ctx->flags & FPM_CTX_AUTOTUNE)) {
+        *rc = fpm_autotune(ctx, p, nullptr, 0);
+        if (*rc != FPM_OK) return nullptr;
+        it = ctx->tuned.find(tune_key(p));
+    }
+    return it == ctx->tuned.end() ? nullptr : &it->second;
+}
+
+fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *p, fpm_result *res) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    fpm_status rc;
+    const Tuning *t = tuning_for(ctx, p, &rc);
+    if (rc != FPM_OK) return rc;
+    TuningScope scope(t);
+    SolveJob j;
+    rc = job_prepare(ctx, p, res, j);
     if (rc != FPM_OK) return rc;
     rc = job_run_epochs(ctx, j, graphs_enabled(ctx));
     if (rc != FPM_OK) return rc;
@@ -1228,10 +1359,18 @@ fpm_status fpm_solve_batch(fpm_context *ctx, const fpm_problem *problems, fpm_re
     std::vector<fpm_status> st(n, FPM_OK);
     // prepare every instance, then enqueue every instance's epochs (no host waits between
     // them: the instances run concurrently on the pool's streams), then finish each
-    for (int i = 0; i < n; ++i)
+    std::vector<const Tuning *> tun(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+        tun[i] = tuning_for(ctx, &problems[i], &st[i]);
+        if (st[i] != FPM_OK) continue;
+        TuningScope scope(tun[i]);
         st[i] = job_prepare(ctx->workers[i], &problems[i], results ? &results[i] : nullptr, jobs[i]);
-    for (int i = 0; i < n; ++i)
-        if (st[i] == FPM_OK) st[i] = job_run_epochs(ctx->workers[i], jobs[i], graphs);
+    }
+    for (int i = 0; i < n; ++i) {
+        if (st[i] != FPM_OK) continue;
+        TuningScope scope(tun[i]);
+        st[i] = job_run_epochs(ctx->workers[i], jobs[i], graphs);
+    }
     fpm_status first = FPM_OK;
     for (int i = 0; i < n; ++i) {
         if (st[i] == FPM_OK) {

@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "fft_core.cuh"
 #include "generic.h"
+#include "tuning.h"
 
 namespace fpm {
 
@@ -195,7 +196,10 @@ GenPlan make_plan(int n) {
     // lines per CTA: up to 16, within 512 threads and 96 KiB of shared memory
     int lpc = 1;
     while (lpc < 16 && (lpc * 2) * pl.T <= 512 && (size_t)(lpc * 2) * n * 8 <= 96 * 1024) lpc *= 2;
-    pl.lpc = lpc;
+    // a tuned (or forced) count within the same limits
+    const int want = knob("FPM_GEN_LPC", tuning().gen_lpc, 0, lpc);
+    while (pl.lpc * 2 <= want && pl.lpc * 2 * pl.T <= 512 && (size_t)(pl.lpc * 2) * n * 8 <= 96 * 1024)
+        pl.lpc *= 2;
     return pl;
 }
 

@@ -29,6 +29,7 @@
 #include "fft_core.cuh"
 #include "pipeline.h"
 #include "stencil.cuh"
+#include "tuning.h"
 
 #include <algorithm>
 #include "tma.cuh"
@@ -1341,8 +1342,7 @@ static cudaError_t launch_fused_cl(int nl, StackView Y, const BatchGeom &g, int 
 
 // cluster size of the fused row pass: 2 (FPM_L23_CLUSTER=4 for measurements)
 static int fused_cluster() {
-    const char *e = std::getenv("FPM_L23_CLUSTER");
-    return e && std::atoi(e) == 4 ? 4 : 2;
+    return knob("FPM_L23_CLUSTER", tuning().l23_cluster, 0, 2) == 4 ? 4 : 2;
 }
 
 template <int N, int TYPE, int LOSS>
@@ -1553,16 +1553,10 @@ static cudaError_t launch_cols_e(const ColsArgs &a, const Twiddles &tw, cudaStre
 
 // 16384-point lines (passes A, B, C) run with 32 values per thread; FPM_COLS_E16=1
 // keeps 16 (measurements).
-static bool cols_e16() {
-    const char *e = std::getenv("FPM_COLS_E16");
-    return e && std::atoi(e) != 0;
-}
+static bool cols_e16() { return knob("FPM_COLS_E16", tuning().cols_e16, -1, 0) != 0; }
 
 // FPM_COLS_ASYNC=0 runs the update with plain loads (measurements)
-static bool cols_async() {
-    const char *e = std::getenv("FPM_COLS_ASYNC");
-    return !(e && std::atoi(e) == 0);
-}
+static bool cols_async() { return knob("FPM_COLS_ASYNC", tuning().cols_async, -1, 1) != 0; }
 
 static cudaError_t launch_cols_async(const ColsArgs &a, const Twiddles &tw, cudaStream_t st) {
     constexpr int N = 16384, E = 32;

@@ -31,6 +31,7 @@ STATUS_NAMES = {0: "FPM_OK", 1: "FPM_ERR_INVALID_ARGUMENT", 2: "FPM_ERR_UNSUPPOR
                 3: "FPM_ERR_OUT_OF_MEMORY", 4: "FPM_ERR_CUDA", 5: "FPM_ERR_NONFINITE",
                 6: "FPM_ERR_NO_DEVICE", 7: "FPM_ERR_INTERNAL"}
 MEM_HOST, MEM_DEVICE = 0, 1
+FPM_CTX_AUTOTUNE = 1
 STACK_F32, STACK_U16 = 0, 1
 LOSS_ANISOTROPIC, LOSS_ISOTROPIC = 0, 1
 _LOSS = {"anisotropic": LOSS_ANISOTROPIC, "isotropic": LOSS_ISOTROPIC}
@@ -42,7 +43,7 @@ EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_sta
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
             "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
             "fpm_led_indices", "fpm_simulate", "fpm_normalise_stack_f32", "fpm_read_tiff_stack",
-            "fpm_optimizer_step", "fpm_solve_batch"]
+            "fpm_optimizer_step", "fpm_solve_batch", "fpm_autotune"]
 
 
 SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
@@ -58,7 +59,7 @@ class FpmError(RuntimeError):
 
 
 class DeviceOpts(C.Structure):
-    _fields_ = [("device", C.c_int32), ("reserved0", C.c_int32),
+    _fields_ = [("device", C.c_int32), ("flags", C.c_int32),
                 ("mem_limit_bytes", C.c_size_t), ("stream", C.c_void_p)]
 
 
@@ -120,6 +121,8 @@ def load_library(path: str | Path | None = None):
     lib.fpm_solve_batch.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result), C.c_int32,
                                     C.c_int32, C.c_void_p]
     lib.fpm_solve_batch.restype = C.c_int
+    lib.fpm_autotune.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_char_p, C.c_size_t]
+    lib.fpm_autotune.restype = C.c_int
     lib.fpm_batch_gradients.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_void_p, C.c_void_p,
                                         C.c_void_p]
     lib.fpm_batch_gradients.restype = C.c_int
@@ -207,10 +210,12 @@ def _empty_like_layout(shape, dtype, device_tensor_like):
 class Engine:
     """One libfpm context (one CUDA device, one stream; not thread-safe)."""
 
-    def __init__(self, device: int = 0, mem_limit_bytes: int = 0, stream: int | None = None):
+    def __init__(self, device: int = 0, mem_limit_bytes: int = 0, stream: int | None = None,
+                 autotune: bool = False):
         self.lib = load_library()
         self._ctx = C.c_void_p()
-        opts = DeviceOpts(device, 0, mem_limit_bytes, stream or None)
+        opts = DeviceOpts(device, FPM_CTX_AUTOTUNE if autotune else 0, mem_limit_bytes,
+                          stream or None)
         st = self.lib.fpm_create(C.byref(self._ctx), C.byref(opts))
         if st != FPM_OK:
             raise FpmError(st, self.lib.fpm_status_string(st).decode())
@@ -348,6 +353,21 @@ class Engine:
             self._check(rc)
         del keep
         return outs, statuses
+
+    def autotune(self, O0, P0c, Y, led_idx, P0, pratio, batch, loss="anisotropic", pie="none"):
+        """fpm_autotune for the shape of this problem; returns the tuner's one-line report."""
+        prob, keep, mem = self._problem(O0, P0c, Y, led_idx, P0, pratio, 1, batch, 5e-4, 0.999,
+                                        1e-4, 0.2, 12, 0.5, loss, pie)
+        buf = C.create_string_buffer(512)
+        _inputs_ready(*keep)
+        self._check(self.lib.fpm_autotune(self._ctx, C.byref(prob), buf, len(buf)))
+        del keep
+        return buf.value.decode()
+
+    def autotune_raw(self, prob: Problem) -> str:
+        buf = C.create_string_buffer(512)
+        self._check(self.lib.fpm_autotune(self._ctx, C.byref(prob), buf, len(buf)))
+        return buf.value.decode()
 
     def batch_gradients(self, O, P, Y, led_idx, P0, pratio, loss="anisotropic", pie="none"):
         """v3 gradients of one LED batch (the fullyfusedFPM contract): (dO, dP, loss)."""

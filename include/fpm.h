@@ -94,9 +94,12 @@ typedef enum fpm_pie_weights {
                           / (|sub_l|^2 + 1e-5), per pixel */
 } fpm_pie_weights;
 
+/* fpm_device_opts.flags */
+#define FPM_CTX_AUTOTUNE 1   /* the first solve of every new problem shape runs fpm_autotune */
+
 typedef struct fpm_device_opts {
     int32_t device;          /* CUDA device ordinal */
-    int32_t reserved0;
+    int32_t flags;           /* FPM_CTX_* bits */
     size_t mem_limit_bytes;  /* 0 = no cap; otherwise solves needing more fail with
                                 FPM_ERR_OUT_OF_MEMORY before allocating anything */
     void *stream;            /* cudaStream_t to run on, or NULL for a context-owned stream */
@@ -167,6 +170,22 @@ fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *prob, fpm_result *res)
 #define FPM_BATCH_EAGER 1
 fpm_status fpm_solve_batch(fpm_context *ctx, const fpm_problem *problems, fpm_result *results,
                            int32_t n, int32_t flags, fpm_status *statuses);
+
+/* Autotuner (no counterpart in the reference, whose launch shapes are fixed 16 x 16
+   blocks, cuFPM_v3/cuda/addon.h:4-5, and whose README reports the LED batch moving the
+   time by 1.5x, README.md:47-49).  Times one epoch of `prob` on the caller's own data
+   for each candidate launch choice, searching one choice at a time: LEDs per
+   low-resolution launch group, the fused or two-pass row transform and its cluster
+   size, the 16384-point passes' prefetch and values per thread, the any-size line
+   FFT's lines per block.  None of these changes the result beyond the rounding of an
+   alternative radix split.  The fastest choice is kept in the context for the
+   problem's shape (h, H, LED count, batch, stack type, loss, weights) and used by every
+   later fpm_solve / fpm_solve_batch of that shape.  The LED batch B stays the caller's:
+   it changes the reconstruction itself.  Outputs nothing but `report` (optional, a
+   one-line summary, truncated to report_cap bytes); the inputs are only read.  Costs
+   about (number of candidates + 1) epochs. */
+fpm_status fpm_autotune(fpm_context *ctx, const fpm_problem *prob, char *report,
+                        size_t report_cap);
 
 /* Gradients of one LED batch at (object, pupil), v3 loss: replaces
    fullyfusedFPM (codes/fusedfpm/fullyfusedFPM.cu:24-169).  prob->n_leds LEDs
