@@ -580,6 +580,12 @@ def accuracy_for(cfg: Cfg, wl, s_per_epoch: float, epochs: int = JOB_EPOCHS):
     tr.cufpm_pure_v3(*args, opt=opt, ctype=torch.complex64,
                      on_epoch=lambda ep, Ok, Pk, l: twin.append(
                          (tr.rel_err(Ok, ref[ep][0]), tr.rel_err(Pk, ref[ep][1]))))
+    # the storage question: the same FP64 run on amplitudes rounded to FP16 (what an FP16
+    # stack would hold), against the FP64 run on the exact single-precision amplitudes
+    half = []
+    tr.cufpm_pure_v3(O0.T, wl["P0c"].T, lambda a, n: pages(a, n).half().float(), wl["led_np"],
+                     wl["P0"].T, cfg.pratio, epochs, cfg.batch, opt=opt,
+                     on_epoch=lambda ep, Ok, Pk, l: half.append(tr.rel_err(Ok, ref[ep][0])))
     ours = []
     for k in range(1, epochs + 1):
         solve(k, O0.data_ptr())
@@ -599,6 +605,10 @@ def accuracy_for(cfg: Cfg, wl, s_per_epoch: float, epochs: int = JOB_EPOCHS):
            "fp32_twin_object_rel_err": [float(f"{e:.3e}") for e, _ in twin],
            "fp32_twin_pupil_rel_err": [float(f"{p:.3e}") for _, p in twin],
            "fp64_loss": [r[2] for r in ref],
+           "fp16_stack_object_rel_err": [float(f"{e:.3e}") for e in half],
+           "fp16_stack_note": "FP64 run on amplitudes rounded to FP16 against the FP64 run "
+                              "on the exact amplitudes: the cost of holding the stack in "
+                              "FP16 instead of the exact uint16 counts (same 2 B/px)",
            "epochs_within_1e-3": within, "fp32_twin_epochs_within_1e-3": twin_within,
            "s_within_1e-3": round(within * s_per_epoch, 4),
            "note": "every FP32 run (this engine, the FP32 twin) sits at the same distance "

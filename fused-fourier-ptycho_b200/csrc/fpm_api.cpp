@@ -1237,6 +1237,22 @@ static std::string tuning_text(const Tuning &t) {
     return buf;
 }
 
+fpm_status fpm_selftest_bounded_wait(fpm_context *ctx, int64_t limit_cycles) {
+    if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
+    ctx->err.clear();
+    if (limit_cycles < 1 || limit_cycles > (1ll << 32))
+        return fail(ctx, FPM_ERR_INVALID_ARGUMENT, "limit_cycles = %lld", (long long)limit_cycles);
+    FPM_CK(cudaSetDevice(ctx->device));
+    FPM_CK(ctx->flag.ensure(sizeof(int) * 4));
+    FPM_CK(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), ctx->stream));
+    FPM_CK(launch_wait_selftest(ctx->flag.as<int>(), (long long)limit_cycles, ctx->stream));
+    FPM_CK(cudaStreamSynchronize(ctx->stream));
+    const fpm_status rc = check_device_flag(ctx);   // the path every solve takes
+    FPM_CK(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), ctx->stream));
+    FPM_CK(cudaStreamSynchronize(ctx->stream));
+    return rc;
+}
+
 fpm_status fpm_autotune(fpm_context *ctx, const fpm_problem *p, char *report, size_t report_cap) {
     if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
     ctx->err.clear();

@@ -1158,6 +1158,21 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Self-check of the bounded waits: one thread arms an mbarrier for 16 bytes that no copy
+// delivers and waits with the given limit; the wait gives up, the kernel sets the flag
+// every pass uses for a wait that ran out, and returns.  No copy is in flight at any time.
+// ---------------------------------------------------------------------------
+__global__ void k_wait_selftest(int *flag, long long limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&bar, 1);
+        tma::fence_barrier_init();
+        tma::arrive_expect_tx(&bar, 16);
+        if (!tma::mbar_wait(&bar, 0, limit)) atomicExch(flag, 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 bool pipeline_supported(int h, int H) {
@@ -1623,6 +1638,11 @@ cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, 
     FPM_DISPATCH_BIG(H, F)
 #undef F
     return e;
+}
+
+cudaError_t launch_wait_selftest(int *flag, long long limit, cudaStream_t st) {
+    k_wait_selftest<<<1, 32, 0, st>>>(flag, limit);
+    return cudaGetLastError();
 }
 
 }  // namespace fpm

@@ -112,4 +112,8 @@ cudaError_t launch_big_rows_fwd(int H, const float2 *Vr, int rspan_n, int Cu0n, 
                                 float2 *Sboxr, const Twiddles &tw, cudaStream_t st,
                                 int *err = nullptr);
 
+// A bounded wait that runs out on purpose (no copy delivers the bytes it waits for): sets
+// *flag after `limit` SM clocks and returns.
+cudaError_t launch_wait_selftest(int *flag, long long limit, cudaStream_t st);
+
 }  // namespace fpm

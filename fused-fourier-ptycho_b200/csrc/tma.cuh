@@ -77,11 +77,12 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for the phase of the given parity to complete; false after kWaitCycles.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Waits for the phase of the given parity to complete; false after `limit` SM clocks.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          long long limit = kWaitCycles) {
     const long long t0 = clock64();
     while (!mbar_test(bar, parity)) {
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     }
     return true;
 }

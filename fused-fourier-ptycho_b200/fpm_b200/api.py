@@ -43,7 +43,8 @@ EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_sta
             "fpm_destroy", "fpm_set_profiling", "fpm_stage_times", "fpm_status_string",
             "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
             "fpm_led_indices", "fpm_simulate", "fpm_normalise_stack_f32", "fpm_read_tiff_stack",
-            "fpm_optimizer_step", "fpm_solve_batch", "fpm_autotune"]
+            "fpm_optimizer_step", "fpm_solve_batch", "fpm_autotune",
+            "fpm_selftest_bounded_wait"]
 
 
 SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
@@ -123,6 +124,8 @@ def load_library(path: str | Path | None = None):
     lib.fpm_solve_batch.restype = C.c_int
     lib.fpm_autotune.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_char_p, C.c_size_t]
     lib.fpm_autotune.restype = C.c_int
+    lib.fpm_selftest_bounded_wait.argtypes = [C.c_void_p, C.c_int64]
+    lib.fpm_selftest_bounded_wait.restype = C.c_int
     lib.fpm_batch_gradients.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_void_p, C.c_void_p,
                                         C.c_void_p]
     lib.fpm_batch_gradients.restype = C.c_int

@@ -187,6 +187,15 @@ fpm_status fpm_solve_batch(fpm_context *ctx, const fpm_problem *problems, fpm_re
 fpm_status fpm_autotune(fpm_context *ctx, const fpm_problem *prob, char *report,
                         size_t report_cap);
 
+/* Self-check of the failure path of the device-side waits (no counterpart in the
+   reference, which has no waits).  The engine's passes wait for their tile copies with a
+   bound (about two seconds); a wait that runs out sets a device flag, the pass stops, and
+   the call returns FPM_ERR_INTERNAL instead of results built from incomplete data.  This
+   runs one such wait on purpose, with the given bound in SM clocks (1 .. 2^32), on an
+   mbarrier armed for bytes that no copy delivers, and returns what a solve would return
+   (FPM_ERR_INTERNAL, detail in fpm_last_error); the context stays usable. */
+fpm_status fpm_selftest_bounded_wait(fpm_context *ctx, int64_t limit_cycles);
+
 /* Gradients of one LED batch at (object, pupil), v3 loss: replaces
    fullyfusedFPM (codes/fusedfpm/fullyfusedFPM.cu:24-169).  prob->n_leds LEDs
    form one batch (prob->batch, epochs and optimiser fields are ignored);

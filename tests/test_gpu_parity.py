@@ -675,3 +675,17 @@ def test_full_size_forward_model_and_zero_residual(engine):
     _, _, loss_pert = engine.batch_gradients((O * noise).contiguous(), P, Y, ledt, P0, p)
     assert scalar(loss_pert) > 0
     assert scalar(loss_true) < 1e-3 * scalar(loss_pert), (scalar(loss_true), scalar(loss_pert))
+
+
+def test_bounded_wait_failure_reaches_the_host(engine, ds_small):
+    """A device-side wait that runs out (an mbarrier armed for bytes that no copy delivers,
+    a bound of 2^20 SM clocks) must come back as FPM_ERR_INTERNAL with its detail, through
+    the same device flag the passes use, and leave the context usable for the next solve."""
+    st = engine.lib.fpm_selftest_bounded_wait(engine._ctx, 1 << 20)
+    assert st == 7, st
+    assert "timed out" in engine.lib.fpm_last_error(engine._ctx).decode()
+    ds = ds_small
+    r = engine.solve(ds.O0, ds.P0c, to_matlab_stack(ds.Y[:8]), led_matlab(ds.led_idx[:8]),
+                     ds.pupil0, ds.pratio, 1, 8, lr=1e-3)
+    assert np.all(np.isfinite(r["loss"]))
+    assert engine.lib.fpm_selftest_bounded_wait(engine._ctx, 0) == 1      # bound out of range
