@@ -752,6 +752,72 @@ def run_instances(args, cfg: Cfg):
     print(json.dumps(line), flush=True)
 
 
+def run_warmstart(args, cfg: Cfg):
+    """The learned warm start (config 5, scaled to one GPU-minute of training data): seeded
+    problems of 64^2 frames from 11 x 11 LEDs, pratio 4; training pairs from the plain
+    reconstruction (20 epochs, LED batch 8) of `--train-pairs` seeded objects; the
+    network (25 bright-field frames in, 32 base channels) trained with Adam in libfpm's
+    own kernels; on 16 held-out seeds, the per-epoch error against the true object of the
+    plain start imresize(Y_1, pratio) and of the learned start (with the fallback to the
+    plain start where it raises the first-epoch loss), and the epochs each needs to reach
+    the plain start's 20-epoch error."""
+    import torch
+    import fpm_b200
+    from fpm_b200 import warmstart as ws
+    h, p, grid, E, B, lr = 64, 4, 11, 20, 8, 2e-3
+    dev = torch.device("cuda", 0)
+    eng = fpm_b200.Engine(0)
+    t0 = time.perf_counter()
+    x, t = ws.training_pairs(eng, args.train_pairs, h, p, grid, E, B, lr, seed0=10_000)
+    t_pairs = time.perf_counter() - t0
+    net = ws.Network(eng, 25, 32, seed=1)
+    t0 = time.perf_counter()
+    hist = ws.train(net, x, t, args.train_epochs, 32, 1e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    pbs = [ws.make_problem_gpu(h, p, grid, 90_000 + i, dev) for i in range(16)]
+    stacks = [ws.simulate_stack(eng, pb, 31 + i) for i, pb in enumerate(pbs)]
+    plain, learned, fallback = ws.evaluate(eng, net, pbs, stacks, E, B, lr)
+    # seconds per epoch of one such solve
+    prob = ws.problem_struct(pbs[0], stacks[0], E, B, lr)
+    O = torch.empty((h * p, h * p), dtype=torch.complex64, device=dev)
+    res = fpm_b200.Result(object=O.data_ptr(), spectrum=None, pupil=None, loss=None)
+    eng._check(eng.solve_raw(prob, res))
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    eng._check(eng.solve_raw(prob, res))
+    s_epoch = (time.perf_counter() - w0) / E
+    q = plain[:, E]                                   # the plain start's 20-epoch error
+
+    def epochs_to(curve, target):
+        hit = np.nonzero(curve <= target * (1 + 1e-9))[0]
+        return int(hit[0]) if len(hit) else None
+    ep_plain = [epochs_to(plain[i], q[i]) for i in range(len(pbs))]
+    ep_learn = [epochs_to(learned[i], q[i]) for i in range(len(pbs))]
+    reached = [e for e in ep_learn if e is not None]
+    line = {"metric": "epochs to the plain start's 20-epoch error, learned vs plain start",
+            "value": round(float(np.mean(ep_plain)) / max(float(np.mean(reached)), 1e-9), 3)
+                     if len(reached) == len(pbs) else None,
+            "unit": "x fewer epochs", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32 (complex64) solves; BF16 x BF16 -> FP32 convolutions",
+            "data": "synthetic (seeded objects, simulated frames)",
+            "config": {"workload": "learned warm start, 64^2 frames x 121 LEDs -> 256^2, "
+                                   "pratio 4, LED batch 8, lr 2e-3",
+                       "train_pairs": args.train_pairs, "train_epochs": args.train_epochs,
+                       "network": "4-level encoder-decoder, 25 inputs, base 32, "
+                                  f"{net.n_params} parameters", "held_out": len(pbs)},
+            "plain_error_per_epoch": [round(float(v), 5) for v in plain.mean(0)],
+            "learned_error_per_epoch": [round(float(v), 5) for v in learned.mean(0)],
+            "epochs_plain": ep_plain, "epochs_learned": ep_learn,
+            "fallbacks": int(sum(fallback)),
+            "s_per_epoch": round(s_epoch, 5),
+            "train_loss_first_last": [round(hist[0], 6), round(hist[-1], 6)],
+            "seconds": {"pairs": round(t_pairs, 1), "training": round(t_train, 1)}}
+    net.close()
+    eng.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_simulate(args, cfg: Cfg):
     """Forward model (fpm_simulate): all LED images of a 16384^2 object, device-resident.
     Not the headline metric: a separate line for the simulator row."""
@@ -1069,12 +1135,17 @@ def main():
     ap.add_argument("--grid", type=int, default=19)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--train-pairs", type=int, default=2000,
+                    help="training pairs of the warm-start workload")
+    ap.add_argument("--train-epochs", type=int, default=30,
+                    help="passes over the training pairs (--workload warmstart)")
     ap.add_argument("--instances", type=int, default=48,
                     help="instances of the batched workload (--workload instances)")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the per-epoch error against the FP64 run (one GPU only)")
     ap.add_argument("--workload", default="solve",
-                    choices=["solve", "simulate", "ingest", "optimizer", "instances"],
+                    choices=["solve", "simulate", "ingest", "optimizer", "instances",
+                             "warmstart"],
                     help="solve: the reconstruction (headline); simulate: the forward model; "
                          "ingest: TIFF frames to normalised amplitude; optimizer: the MATLAB "
                          "optimiser classes' step on the object")
@@ -1089,7 +1160,7 @@ def main():
         return
     if args.workload != "solve":
         {"simulate": run_simulate, "ingest": run_ingest, "optimizer": run_optimizer,
-         "instances": run_instances}[args.workload](args, cfg)
+         "instances": run_instances, "warmstart": run_warmstart}[args.workload](args, cfg)
         return
     out, wl, rank, world = run_ours(args, cfg)
     if rank == 0:

@@ -8,6 +8,8 @@
 #include <cstdint>
 #include <vector>
 
+struct fpm_context;   // the C ABI's context (include/fpm.h)
+
 namespace fpm {
 
 enum StackType : int { kStackF32 = 0, kStackU16 = 1 };
@@ -46,6 +48,12 @@ cudaError_t launch_transpose(const float2 *in, size_t ldi, float2 *out, size_t l
 size_t bicubic_work_bytes(int h, int pratio);
 cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, void *work,
                                 cudaStream_t st);
+// O = bicubic resize (as above) of re + i im, both h x h column-major; work as above
+cudaError_t launch_bicubic_complex(const float *re, const float *im, int h, int pratio, float2 *O,
+                                   void *work, cudaStream_t st);
+// normalised amplitudes of stack pages [first, first + count) into out (count * h*h floats)
+cudaError_t launch_stack_pages(StackView Y, int h, int first, int count, float *out,
+                               cudaStream_t st);
 
 // ---- reductions and ingest ------------------------------------------------
 cudaError_t launch_loss_accumulate(const double *parts, int n, double *slot, cudaStream_t st);
@@ -100,5 +108,9 @@ void spiral_grid_order(int n, std::vector<int2> &order);
 // led_idx[2l], led_idx[2l+1] = (kl, kt) of the LED at grid cell pos[l]
 cudaError_t launch_led_nearest(const int2 *pos, int n_leds, const LedGeom &p, int32_t *led_idx,
                                cudaStream_t st);
+
+// the stream and device of a C-ABI context (fpm_api.cpp), for the other ABI units
+void *context_stream(::fpm_context *ctx);
+int context_device(::fpm_context *ctx);
 
 }  // namespace fpm

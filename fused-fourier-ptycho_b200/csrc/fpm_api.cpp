@@ -1237,6 +1237,13 @@ static std::string tuning_text(const Tuning &t) {
     return buf;
 }
 
+}  // extern "C"
+
+void *fpm::context_stream(fpm_context *ctx) { return ctx ? ctx->stream : nullptr; }
+int fpm::context_device(fpm_context *ctx) { return ctx ? ctx->device : 0; }
+
+extern "C" {
+
 fpm_status fpm_selftest_bounded_wait(fpm_context *ctx, int64_t limit_cycles) {
     if (!ctx) return FPM_ERR_INVALID_ARGUMENT;
     ctx->err.clear();

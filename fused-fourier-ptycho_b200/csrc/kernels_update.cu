@@ -196,6 +196,82 @@ cudaError_t launch_bicubic_init(StackView Y, int h, int pratio, float2 *O, void 
     return cudaGetLastError();
 }
 
+// Complex up-sampling: the same bicubic resize of the real and the imaginary part of an
+// h x h column-major image (re, im planes), for the learned warm start.
+__global__ void __launch_bounds__(256) k_bicubic_complex(const float *__restrict__ re,
+                                                          const float *__restrict__ im,
+                                                          const Taps *__restrict__ taps, int h,
+                                                          int H, float2 *__restrict__ O) {
+    const size_t total = (size_t)H * H;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int R = (int)(q % H);
+        const int C = (int)(q / H);
+        const Taps tr = taps[R], tc = taps[C];
+        const int ir[4] = {tr.idx.x, tr.idx.y, tr.idx.z, tr.idx.w};
+        const int ic[4] = {tc.idx.x, tc.idx.y, tc.idx.z, tc.idx.w};
+        double ar = 0.0, ai = 0.0;
+        for (int kc = 0; kc < 4; ++kc) {
+            double tr_ = 0.0, ti = 0.0;
+            for (int kr = 0; kr < 4; ++kr) {
+                const size_t i = (size_t)ic[kc] * h + ir[kr];
+                tr_ += tr.w[kr] * (double)re[i];
+                ti += tr.w[kr] * (double)im[i];
+            }
+            ar += tc.w[kc] * tr_;
+            ai += tc.w[kc] * ti;
+        }
+        O[q] = make_float2((float)ar, (float)ai);
+    }
+}
+
+cudaError_t launch_bicubic_complex(const float *re, const float *im, int h, int pratio, float2 *O,
+                                   void *work, cudaStream_t st) {
+    const int H = h * pratio;
+    Taps *taps = static_cast<Taps *>(work);
+    k_bicubic_taps<<<(H + 255) / 256, 256, 0, st>>>(h, pratio, taps);
+    const size_t total = (size_t)H * H;
+    size_t gx = (total + 255) / 256;
+    const size_t cap = (size_t)kB200SMs * 8 * 8;
+    if (gx > cap) gx = cap;
+    k_bicubic_complex<<<(unsigned)gx, 256, 0, st>>>(re, im, taps, h, H, O);
+    return cudaGetLastError();
+}
+
+// Amplitudes of stack pages [first, first + count) (h*h each), as the solve normalises them.
+template <int TYPE>
+__global__ void __launch_bounds__(256) k_stack_pages(StackView Y, size_t first, size_t n,
+                                                     float *__restrict__ out) {
+    float mn = 0.f, range = 0.f;
+    if (TYPE == kStackU16) {
+        mn = (float)Y.minmax[0];
+        range = (float)(Y.minmax[1] - Y.minmax[0]);
+    }
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        float a;
+        if (TYPE == kStackF32) {
+            a = static_cast<const float *>(Y.ptr)[first + i];
+        } else {
+            const float x = (float)static_cast<const uint16_t *>(Y.ptr)[first + i] - mn;
+            a = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+        }
+        out[i] = a;
+    }
+}
+
+cudaError_t launch_stack_pages(StackView Y, int h, int first, int count, float *out,
+                               cudaStream_t st) {
+    const size_t plane = (size_t)h * h, n = plane * count;
+    size_t gx = (n + 255) / 256;
+    if (gx > (size_t)kB200SMs * 16) gx = (size_t)kB200SMs * 16;
+    if (Y.type == kStackU16)
+        k_stack_pages<kStackU16><<<(unsigned)gx, 256, 0, st>>>(Y, plane * first, n, out);
+    else
+        k_stack_pages<kStackF32><<<(unsigned)gx, 256, 0, st>>>(Y, plane * first, n, out);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Deterministic FP64 loss reduction: one block sums the per-tile partials in a
 // fixed order (Kahan per thread, then a fixed tree) and adds them to *slot.

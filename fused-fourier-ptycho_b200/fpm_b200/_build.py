@@ -25,7 +25,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I",
                   "--expt-relaxed-constexpr"]
 LIBS_SOURCES = ["kernels_lowres.cu", "kernels_update.cu", "fft_own.cu", "fpm_api.cpp",
                 "noalloc.cu", "pipeline.cu", "geometry.cu", "tiff.cpp",
-                "optimizers.cu", "generic.cu", "tuning.cpp"]
+                "optimizers.cu", "generic.cu", "tuning.cpp", "cnn.cu", "cnn_api.cpp"]
 LINK_LIBS = ["-lcudart", "-lpthread"]
 
 

@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -44,7 +45,10 @@ EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_sta
             "fpm_last_error", "fpm_abi_version", "fpm_feature_gradient_noalloc", "fpm_fft2",
             "fpm_led_indices", "fpm_simulate", "fpm_normalise_stack_f32", "fpm_read_tiff_stack",
             "fpm_optimizer_step", "fpm_solve_batch", "fpm_autotune",
-            "fpm_selftest_bounded_wait"]
+            "fpm_selftest_bounded_wait", "fpm_cnn_create", "fpm_cnn_destroy",
+            "fpm_cnn_parameter_count", "fpm_cnn_last_error", "fpm_cnn_set_parameters",
+            "fpm_cnn_get_parameters", "fpm_cnn_forward", "fpm_cnn_gradients",
+            "fpm_cnn_train_step", "fpm_cnn_initial_object"]
 
 
 SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
@@ -126,6 +130,28 @@ def load_library(path: str | Path | None = None):
     lib.fpm_autotune.restype = C.c_int
     lib.fpm_selftest_bounded_wait.argtypes = [C.c_void_p, C.c_int64]
     lib.fpm_selftest_bounded_wait.restype = C.c_int
+    vp = C.c_void_p
+    lib.fpm_cnn_create.argtypes = [vp, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(vp)]
+    lib.fpm_cnn_create.restype = C.c_int
+    lib.fpm_cnn_destroy.argtypes = [vp]
+    lib.fpm_cnn_destroy.restype = None
+    lib.fpm_cnn_parameter_count.argtypes = [vp]
+    lib.fpm_cnn_parameter_count.restype = C.c_int64
+    lib.fpm_cnn_last_error.argtypes = [vp]
+    lib.fpm_cnn_last_error.restype = C.c_char_p
+    lib.fpm_cnn_set_parameters.argtypes = [vp, vp, C.c_int64]
+    lib.fpm_cnn_set_parameters.restype = C.c_int
+    lib.fpm_cnn_get_parameters.argtypes = [vp, vp, C.c_int64]
+    lib.fpm_cnn_get_parameters.restype = C.c_int
+    lib.fpm_cnn_forward.argtypes = [vp, vp, C.c_int32, C.c_int32, vp]
+    lib.fpm_cnn_forward.restype = C.c_int
+    lib.fpm_cnn_gradients.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.POINTER(C.c_double), vp]
+    lib.fpm_cnn_gradients.restype = C.c_int
+    lib.fpm_cnn_train_step.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, C.c_float,
+                                       C.POINTER(C.c_double)]
+    lib.fpm_cnn_train_step.restype = C.c_int
+    lib.fpm_cnn_initial_object.argtypes = [vp, C.POINTER(Problem), vp]
+    lib.fpm_cnn_initial_object.restype = C.c_int
     lib.fpm_batch_gradients.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_void_p, C.c_void_p,
                                         C.c_void_p]
     lib.fpm_batch_gradients.restype = C.c_int
@@ -219,11 +245,16 @@ class Engine:
         self._ctx = C.c_void_p()
         opts = DeviceOpts(device, FPM_CTX_AUTOTUNE if autotune else 0, mem_limit_bytes,
                           stream or None)
+        # objects that hold library state on this context (warm-start networks), closed
+        # before the context is
+        self._children = weakref.WeakSet()
         st = self.lib.fpm_create(C.byref(self._ctx), C.byref(opts))
         if st != FPM_OK:
             raise FpmError(st, self.lib.fpm_status_string(st).decode())
 
     def close(self):
+        for ch in list(getattr(self, "_children", ())):
+            ch.close()
         if self._ctx:
             self.lib.fpm_destroy(self._ctx)
             self._ctx = C.c_void_p()

@@ -363,6 +363,41 @@ typedef struct fpm_optimizer {
 fpm_status fpm_optimizer_step(fpm_context *ctx, const fpm_optimizer *opt, float *param,
                               const float *grad, size_t n, int32_t memory);
 
+/* Learned warm start (config 5 of the north star; no counterpart in the reference, whose
+   initial object is imresize(Y_1, pratio) with zero phase, codes_v2/main_run_FPM.m:48).
+   A 4-level convolutional encoder-decoder (channels base, 2 base, 4 base, 8 base; 3x3
+   convolutions on the tensor cores with BF16 operands and FP32 accumulation; FP32 master
+   weights) maps the first in_channels frames of a stack (the central bright-field block
+   of the spiral order: 25 frames = the central 5 x 5 LEDs) to the real and imaginary parts
+   of a low-resolution object, which fpm_cnn_initial_object up-samples bicubically to the
+   H x H starting object.  Trained by fpm_cnn_train_step on pairs the plain
+   reconstruction produces.  All arrays: device memory of the context's device, FP32,
+   planes of h x h (h a multiple of 8), [n][channels][h*h]; the network keeps the
+   context's stream and device.  Parameter order: for each of the 14 layers, weights
+   [Cout][Cin][3][3] then biases [Cout]. */
+typedef struct fpm_cnn fpm_cnn;
+/* a network must be destroyed before its context */
+fpm_status fpm_cnn_create(fpm_context *ctx, int32_t in_channels, int32_t base_channels,
+                          uint64_t seed, fpm_cnn **net);
+void fpm_cnn_destroy(fpm_cnn *net);
+int64_t fpm_cnn_parameter_count(const fpm_cnn *net);
+const char *fpm_cnn_last_error(const fpm_cnn *net);
+/* host arrays of fpm_cnn_parameter_count floats; setting also resets the Adam state */
+fpm_status fpm_cnn_set_parameters(fpm_cnn *net, const float *params, int64_t n);
+fpm_status fpm_cnn_get_parameters(fpm_cnn *net, float *params, int64_t n);
+/* y [n][2][h*h] = network(x [n][in_channels][h*h]) */
+fpm_status fpm_cnn_forward(fpm_cnn *net, const float *x, int32_t n, int32_t h, float *y);
+/* loss = mean over all n*2*h*h outputs of (y - t)^2, and (host array or NULL) its
+   gradient with respect to every parameter; the parameters are not changed */
+fpm_status fpm_cnn_gradients(fpm_cnn *net, const float *x, const float *t, int32_t n,
+                             int32_t h, double *loss, float *grads);
+/* fpm_cnn_gradients, then one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) of rate lr */
+fpm_status fpm_cnn_train_step(fpm_cnn *net, const float *x, const float *t, int32_t n,
+                              int32_t h, float lr, double *loss);
+/* the starting object of a device-memory problem (complex H*H, column-major): the network
+   on the problem's first in_channels frames, normalised as fpm_solve normalises them */
+fpm_status fpm_cnn_initial_object(fpm_cnn *net, const fpm_problem *prob, float *object);
+
 void fpm_destroy(fpm_context *ctx);
 
 /* Per-stage device timing (no counterpart in the reference, which only times

@@ -1,0 +1,101 @@
+"""The warm-start network on the GPU (fpm_cnn_* of libfpm) against its CPU oracle
+(oracle/cnn_oracle.py), its training, and what the trained network gains.
+
+The tensor-core convolutions round their operands to BF16 as the oracle does; the rest
+is FP32 on the device and FP64 in the oracle, so an activation within an FP32 rounding
+of a BF16 halfway point may round to the neighbouring BF16 value (2^-8 relative), and
+such a flip moves the outputs downstream of it by up to ~1e-2 (measured on the oracle:
+three flips in the 14 layers of the 25-channel case moved 13 of 2048 outputs by more than
+1e-3).  The bar is therefore set by a twin of the oracle whose convolution outputs carry
+1e-6 relative noise (about the FP32 rounding of the device's sums): the device may differ
+from the oracle by at most 3x what the twin does, in the median and the relative L2 of
+the output, per layer in the gradients and in the loss (floors: a median of 1e-5 of the
+largest output, 1e-3 relative L2, 1e-4 on the loss).  An indexing or layout error is
+O(1) on most outputs."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _net(engine, in_ch=3, base=8, seed=5):
+    from fpm_b200 import warmstart
+    return warmstart.Network(engine, in_ch, base, seed)
+
+
+def _data(in_ch, n, h, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, in_ch, h, h)).astype(np.float32)
+    t = (0.1 * rng.standard_normal((n, 2, h, h))).astype(np.float32)
+    return x, t
+
+
+@pytest.mark.parametrize("in_ch,base,n,h", [(3, 8, 2, 16), (25, 16, 1, 32)])
+def test_forward_and_gradients_match_oracle(engine, in_ch, base, n, h):
+    import torch
+    from oracle import cnn_oracle as co
+    net = _net(engine, in_ch, base)
+    p = net.get_parameters()
+    rng = np.random.default_rng(3)
+    p = (p + 0.01 * rng.standard_normal(p.size)).astype(np.float32)   # non-zero biases too
+    net.set_parameters(p)
+    x, t = _data(in_ch, n, h, 7)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    y = net.forward(xd).cpu().numpy()
+    y64, _, _ = co.forward(p.astype(np.float64), x.astype(np.float64), in_ch, base)
+    p64, x64, t64 = p.astype(np.float64), x.astype(np.float64), t.astype(np.float64)
+    y_tw, _, _ = co.forward(p64, x64, in_ch, base, noise=1e-6, seed=11)
+    med = lambda a: float(np.median(np.abs(a - y64)))
+    rel = lambda a, b: float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30))
+    print(f"output: median {med(y):.2e} (twin {med(y_tw):.2e}), rel {rel(y, y64):.2e} "
+          f"(twin {rel(y_tw, y64):.2e})")
+    assert med(y) <= max(1e-5 * np.abs(y64).max(), 3 * med(y_tw))
+    assert rel(y, y64) <= max(1e-3, 3 * rel(y_tw, y64))
+    loss, g = net.gradients(xd, td)
+    l64, g64 = co.loss_and_gradients(p64, x64, t64, in_ch, base)
+    l_tw, g_tw = co.loss_and_gradients(p64, x64, t64, in_ch, base, noise=1e-6, seed=11)
+    assert abs(loss - l64) <= max(1e-4, 3 * abs(l_tw - l64) / abs(l64)) * abs(l64)
+    off = 0
+    for ci, cout in co.layers(in_ch, base):
+        for size in (ci * cout * 9, cout):
+            sl = slice(off, off + size)
+            e, e_tw = rel(g[sl], g64[sl]), rel(g_tw[sl], g64[sl])
+            assert e <= max(1e-3, 3 * e_tw), (ci, cout, size, e, e_tw)
+            off += size
+    net.close()
+
+
+def test_training_fits_a_small_set(engine):
+    """Adam steps on four fixed pairs bring the loss down by 10x (the optimiser, the
+    gradients and the BF16 weight copies working together)."""
+    import torch
+    net = _net(engine, 3, 8, seed=1)
+    x, t = _data(3, 4, 16, 11)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    first = net.train_step(xd, td, 3e-3)
+    for _ in range(150):
+        last = net.train_step(xd, td, 3e-3)
+    assert last < 0.1 * first, (first, last)
+    net.close()
+
+
+def test_learned_start_beats_the_plain_start(engine):
+    """Trained on 96 pairs the plain reconstruction made (32^2 frames of 5 x 5 LEDs,
+    pratio 4, 8 epochs), the network's starting object is closer to the true object than
+    the plain start imresize(Y_1, pratio) on held-out seeds, and the solve that starts
+    from it is at least as close after 2 epochs."""
+    from fpm_b200 import warmstart as ws
+    h, p, grid, E, B, lr = 32, 4, 5, 8, 5, 2e-3
+    x, t = ws.training_pairs(engine, 96, h, p, grid, E, B, lr, seed0=100, in_channels=9, chunk=32)
+    net = _net(engine, 9, 16, seed=2)
+    hist = ws.train(net, x, t, 40, 16, 2e-3)
+    assert hist[-1] < 0.5 * hist[0], hist
+    import torch
+    dev = torch.device("cuda", 0)
+    pbs = [ws.make_problem_gpu(h, p, grid, 5000 + i, dev) for i in range(6)]
+    stacks = [ws.simulate_stack(engine, pb, 17 + i) for i, pb in enumerate(pbs)]
+    plain, learned, fallback = ws.evaluate(engine, net, pbs, stacks, 2, B, lr)
+    print("plain", plain.mean(0), "learned", learned.mean(0), "fallback", fallback)
+    assert learned[:, 0].mean() < plain[:, 0].mean()
+    assert learned[:, 2].mean() <= plain[:, 2].mean() * 1.02
+    net.close()
