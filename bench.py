@@ -204,7 +204,7 @@ def stage_bytes(cfg: Cfg, led, sup=None):
         tot["lr_cols_inverse"] += (8 * fr * fc + 8 * fc) * px   # support crop r8, support columns w8
         tot["lr_rows_inverse"] += 22 * px      # field r8 w8, residual w4, stack r2
         tot["lr_rows_forward"] += 20 * px      # residual r4, field r8 w8
-        tot["lr_rows_fused"] += (10 + 8 * fc) * px   # field r8, stack r2, support columns w8
+        tot["lr_rows_fused"] += (12 + 8 * fc) * px   # field r8, amplitude rows r4, support columns w8
         tot["lr_cols_forward"] += 16 * fc * px        # support columns r8, gradient spectrum w8
         tot["pupil_grad"] += 16 * fr * fc * px + 8 * h2
         tot["rows_inverse_stitch"] += 8 * fr * fc * px + 8 * H * rspan
@@ -221,6 +221,7 @@ def stage_bytes(cfg: Cfg, led, sup=None):
     per["cols_forward"] = 8 * H2 + 8 * H * r0
     per["spectrum_fft2"] = 32 * H2
     per["loss_reduce"] = 8 * 1024
+    per["stack_rows"] = 6 * h2 * len(led)    # once per solve: uint16 stack r2, amplitude rows w4
     return per
 
 

@@ -23,6 +23,9 @@ struct StackView {
     // device amplitude sqrt((v - min) / (max - min)) of every uint16 value v, the same
     // float the formula gives (kStackU16; null: kernels evaluate the formula)
     const float *lut = nullptr;
+    // row-major FP32 copy of those amplitudes, page p row r at rows + (p h + r) h (the
+    // fused row pass reads it; null until launch_amplitude_rows has made it)
+    const float *rows = nullptr;
 };
 
 // Half-open box of centred-spectrum rows/cols [lo, lo + span) taken modulo H.
@@ -82,6 +85,9 @@ cudaError_t launch_optimizer_step(const OptStep &o, cudaStream_t st);
 
 // amplitude of each of the 65536 uint16 values for the stack's (min, max)
 cudaError_t launch_amplitude_lut(const unsigned *minmax, float *lut, cudaStream_t st);
+// out[p][r][c] = amplitude of element (r, c) of page p of Y (pages of h x h, column-major,
+// h a multiple of 32), the float every other pass takes for it
+cudaError_t launch_amplitude_rows(StackView Y, int h, int pages, float *out, cudaStream_t st);
 // float stack: min / max and normalise in two launches; mm: 2 unsigned of scratch
 cudaError_t launch_normalise_f32(const float *p, size_t n, unsigned *mm, float *out,
                                  cudaStream_t st);

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
@@ -22,6 +23,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "engine.h"
@@ -81,7 +83,8 @@ enum Stage : int {
     ST_COLS_FORWARD, ST_ROWS_FORWARD, ST_LR_COLS_INV, ST_LR_ROWS_INV, ST_LR_ROWS_FWD,
     ST_LR_COLS_FWD, ST_LOSS, ST_PUPIL_GRAD, ST_ROWS_INV, ST_COLS_UPDATE, ST_RMS_PUPIL,
     ST_SPECTRUM, ST_TRANSPOSE, ST_LR_ROWS_FUSED, ST_SIM_ROWS_INV, ST_SIM_MAGNITUDE, ST_H2D,
-    ST_D2H, ST_GEN_LR_FFT, ST_GEN_LOSS, ST_GEN_STITCH, ST_GEN_OBJ_FFT, ST_GEN_RMS_OBJ, ST_COUNT
+    ST_D2H, ST_GEN_LR_FFT, ST_GEN_LOSS, ST_GEN_STITCH, ST_GEN_OBJ_FFT, ST_GEN_RMS_OBJ,
+    ST_STACK_ROWS, ST_COUNT
 };
 const char *const kStageName[ST_COUNT] = {
     "cols_forward", "rows_forward", "lr_cols_inverse", "lr_rows_inverse", "lr_rows_forward",
@@ -89,10 +92,10 @@ const char *const kStageName[ST_COUNT] = {
     "rmsprop_pupil", "spectrum_fft2", "transpose", "lr_rows_fused", "sim_rows_inverse",
     "sim_magnitude", "copy_inputs_h2d", "copy_outputs_d2h", "any_size_lr_fft2",
     "any_size_loss_gradient", "any_size_stitch", "any_size_object_fft2",
-    "any_size_rmsprop_object"};
+    "any_size_rmsprop_object", "stack_rows"};
 // 0: a host <-> device copy of the caller's buffers (host-memory calls), not a kernel
 const int kStageOwn[ST_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0,
-                                 1, 1, 1, 1, 1};
+                                 1, 1, 1, 1, 1, 1};
 
 struct Profiler {
     bool on = false;
@@ -165,7 +168,7 @@ struct fpm_context {
     GenFft gfft;   // line FFTs of lengths that are not powers of two
     // work buffers, kept between calls
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
-        minmax, lut, spec, flag, pie;
+        minmax, lut, spec, flag, pie, rows;
     DevBuf opt[6];   // device copies of an optimiser step's host arrays
     // fpm_solve_batch: one worker context per instance, on a pool of streams
     std::vector<fpm_context *> workers;
@@ -377,10 +380,70 @@ fpm_status stage_inputs(fpm_context *ctx, const fpm_problem *p, const Shape &s, 
     return FPM_OK;
 }
 
+// The row-major amplitude copy of the whole stack the fused row pass reads (once per
+// call: 4 bytes per pixel beside the stack).
+fpm_status stack_rows(fpm_context *ctx, const Shape &s, Inputs &in) {
+    FPM_CK(ctx->rows.ensure(s.plane * s.L * sizeof(float)));
+    FPM_STAGE(ST_STACK_ROWS,
+              launch_amplitude_rows(in.Y, s.h, s.L, ctx->rows.as<float>(), ctx->stream));
+    in.Y.rows = ctx->rows.as<float>();
+    return FPM_OK;
+}
+
 // Pupil support of a solve: the amplitude clamp (|P| <- P0 clamp(|P|, P0 -/+ am))
 // keeps the pupil at zero wherever P0 is zero, so after the initial pupil P0c the
 // pupil is non-zero only inside supp(P0c) u supp(P0).  FPM_PUPIL_SUPPORT=0 keeps whole
 // crops (measurements).
+// bit pattern of a float
+static inline uint32_t fbits(const float *x) {
+    uint32_t b;
+    std::memcpy(&b, x, 4);
+    return b;
+}
+
+// Rows / columns [box[0], box[1]] x [box[2], box[3]] holding every pixel where the host
+// pupil P (complex, column-major h x h) or the amplitude A is not +-0 (NaN counts as
+// non-zero).  A column is tested with one OR of its bit patterns (the sign bit masked
+// afterwards), and only the non-zero columns are searched from both ends for their
+// first and last non-zero rows.
+static void host_support_cols(const float *P, const float *A, int h, int c0, int c1, int box[4]) {
+    const auto nz = [&](size_t i) {
+        return ((fbits(P + 2 * i) | fbits(P + 2 * i + 1) | fbits(A + i)) & 0x7fffffffu) != 0;
+    };
+    for (int c = c0; c < c1; ++c) {
+        const float *pc = P + 2 * (size_t)c * h, *ac = A + (size_t)c * h;
+        uint32_t any = 0;
+        for (int i = 0; i < 2 * h; ++i) any |= fbits(pc + i) & 0x7fffffffu;
+        for (int i = 0; i < h; ++i) any |= fbits(ac + i) & 0x7fffffffu;
+        if (any == 0) continue;
+        int lo = 0, hi = h - 1;
+        while (!nz((size_t)c * h + lo)) ++lo;
+        while (!nz((size_t)c * h + hi)) --hi;
+        box[0] = std::min(box[0], lo);
+        box[1] = std::max(box[1], hi);
+        box[2] = std::min(box[2], c);
+        box[3] = std::max(box[3], c);
+    }
+}
+
+// the columns split over up to 8 host threads (the arrays are 12 h^2 bytes)
+static void host_support_box(const float *P, const float *A, int h, int box[4]) {
+    const int nt = std::max(1, std::min({8, (int)std::thread::hardware_concurrency(), h / 64}));
+    std::vector<std::array<int, 4>> part(nt, std::array<int, 4>{h, -1, h, -1});
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nt; ++i)
+        pool.emplace_back(host_support_cols, P, A, h, (int)((long long)h * i / nt),
+                          (int)((long long)h * (i + 1) / nt), part[i].data());
+    host_support_cols(P, A, h, 0, h / nt, part[0].data());
+    for (std::thread &t : pool) t.join();
+    for (const auto &b : part) {
+        box[0] = std::min(box[0], b[0]);
+        box[1] = std::max(box[1], b[1]);
+        box[2] = std::min(box[2], b[2]);
+        box[3] = std::max(box[3], b[3]);
+    }
+}
+
 fpm_status pupil_support(fpm_context *ctx, const fpm_problem *p, const Shape &s, Support &sup) {
     sup.r_lo = sup.c_lo = 0;
     sup.r_hi = sup.c_hi = s.h;
@@ -390,17 +453,7 @@ fpm_status pupil_support(fpm_context *ctx, const fpm_problem *p, const Shape &s,
     if (p->pie_weights == FPM_PIE_EPIE) return FPM_OK;
     int box[4] = {s.h, -1, s.h, -1};
     if (p->memory == FPM_MEM_HOST) {
-        const float *P = p->pupil_init, *A = p->pupil_amp;
-        for (int c = 0; c < s.h; ++c)
-            for (int r = 0; r < s.h; ++r) {
-                const size_t i = (size_t)c * s.h + r;
-                if (!(P[2 * i] == 0.f && P[2 * i + 1] == 0.f) || !(A[i] == 0.f)) {
-                    box[0] = std::min(box[0], r);
-                    box[1] = std::max(box[1], r);
-                    box[2] = std::min(box[2], c);
-                    box[3] = std::max(box[3], c);
-                }
-            }
+        host_support_box(p->pupil_init, p->pupil_amp, s.h, box);
     } else {
         FPM_CK(ctx->flag.ensure(sizeof(int) * 4));
         FPM_CK(launch_support_box(reinterpret_cast<const float2 *>(p->pupil_init), p->pupil_amp,
@@ -583,7 +636,7 @@ fpm_status lowres_and_stitch(fpm_context *ctx, const Plan &pl, const Twiddles &t
         FPM_STAGE(ST_LR_COLS_INV, launch_lr_cols_inv(g, in.led, P, b, l0, nl, tw, st));
         if (pl.fused_rows) {
             FPM_STAGE(ST_LR_ROWS_FUSED,
-                      launch_lr_rows_fused(g, in.Y, in.stack_pages, b, l0, nl, part_off, tw, st));
+                      launch_lr_rows_fused(g, in.Y, b, l0, nl, part_off, tw, st));
             FPM_STAGE(ST_LR_COLS_FWD, launch_lr_cols_fwd(g, b.T2, b, l0, nl, tw, st));
             part_off += lr_rows_fused_blocks(g.h, nl);
         } else {
@@ -946,6 +999,10 @@ static fpm_status job_prepare(fpm_context *ctx, const fpm_problem *p, fpm_result
     if (!j.generic) {
         rc = twiddles_of(ctx, s, j.tw);
         if (rc != FPM_OK) return rc;
+        if (j.pl.fused_rows) {
+            rc = stack_rows(ctx, s, j.in);
+            if (rc != FPM_OK) return rc;
+        }
     }
     // object and pupil: work in the caller's device outputs when given, else internal
     if (dev && j.res.object) {
@@ -1282,7 +1339,10 @@ fpm_status fpm_autotune(fpm_context *ctx, const fpm_problem *p, char *report, si
             knobs.push_back({&Tuning::lr_group, groups});
             if (lr_rows_fused_supported(s.h)) {
                 knobs.push_back({&Tuning::lr_fused, {0}});
-                knobs.push_back({&Tuning::l23_cluster, {4}});
+                if (s.h == 2048)
+                    knobs.push_back({&Tuning::l23_cluster, {2, 8}});
+                else
+                    knobs.push_back({&Tuning::l23_cluster, {4}});
             }
             if (s.H == 16384) {
                 knobs.push_back({&Tuning::cols_async, {0}});
@@ -1452,6 +1512,10 @@ fpm_status fpm_batch_gradients(fpm_context *ctx, const fpm_problem *p, float *d_
     Inputs in;
     rc = stage_inputs(ctx, p, s, in);
     if (rc != FPM_OK) return rc;
+    if (pl.fused_rows) {
+        rc = stack_rows(ctx, s, in);
+        if (rc != FPM_OK) return rc;
+    }
     Twiddles tw;
     rc = twiddles_of(ctx, s, tw);
     if (rc != FPM_OK) return rc;

@@ -4,6 +4,8 @@
 #include "common.cuh"
 #include "engine.h"
 
+#include <algorithm>
+
 namespace fpm {
 
 // One RMSprop step (constrained_RMSprop_both, cuFPM_v3/cuda/kernels.cuh:364-382 for
@@ -412,6 +414,57 @@ __global__ void __launch_bounds__(256) k_amplitude_lut(const unsigned *__restric
 
 cudaError_t launch_amplitude_lut(const unsigned *mm, float *lut, cudaStream_t st) {
     k_amplitude_lut<<<65536 / 256, 256, 0, st>>>(mm, lut);
+    return cudaGetLastError();
+}
+
+// Row-major amplitude copy: 32 x 32 tiles through shared memory, read along the stored
+// rows of a page (r), written along c; block (x, y, z) takes tile (x, y) of pages z,
+// z + gridDim.z, ...
+template <int TYPE>
+__global__ void __launch_bounds__(256) k_amplitude_rows(StackView Y, int h, int pages,
+                                                        float *__restrict__ out) {
+    __shared__ float tile[32][33];
+    float mn = 0.f, range = 0.f;
+    if (TYPE == kStackU16 && !Y.lut) {
+        mn = (float)Y.minmax[0];
+        range = (float)(Y.minmax[1] - Y.minmax[0]);
+    }
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    for (int p = blockIdx.z; p < pages; p += gridDim.z) {
+        const size_t page = (size_t)p * h * h;
+        for (int i = threadIdx.y; i < 32; i += 8) {   // column c0 + i, row r0 + threadIdx.x
+            const size_t idx = page + (size_t)(c0 + i) * h + r0 + threadIdx.x;
+            float a;
+            if (TYPE == kStackF32) {
+                a = static_cast<const float *>(Y.ptr)[idx];
+            } else {
+                const uint16_t raw = static_cast<const uint16_t *>(Y.ptr)[idx];
+                if (Y.lut) {
+                    a = Y.lut[raw];
+                } else {
+                    const float x = (float)raw - mn;
+                    a = range > 0.f ? sqrtf(x / range) : sqrtf(x);
+                }
+            }
+            tile[i][threadIdx.x] = a;
+        }
+        __syncthreads();
+        for (int i = threadIdx.y; i < 32; i += 8)     // row r0 + i, column c0 + threadIdx.x
+            out[page + (size_t)(r0 + i) * h + c0 + threadIdx.x] = tile[threadIdx.x][i];
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_amplitude_rows(StackView Y, int h, int pages, float *out, cudaStream_t st) {
+    if (h % 32 != 0 || pages < 1) return cudaErrorInvalidValue;
+    // about 32 blocks per SM for the whole stack (each walks its tile through many pages)
+    const int tiles = (h / 32) * (h / 32);
+    const int zc = std::max(1, std::min(pages, (kB200SMs * 32 + tiles - 1) / tiles));
+    const dim3 grid((unsigned)(h / 32), (unsigned)(h / 32), (unsigned)std::min(zc, 65535));
+    if (Y.type == kStackU16)
+        k_amplitude_rows<kStackU16><<<grid, dim3(32, 8), 0, st>>>(Y, h, pages, out);
+    else
+        k_amplitude_rows<kStackF32><<<grid, dim3(32, 8), 0, st>>>(Y, h, pages, out);
     return cudaGetLastError();
 }
 

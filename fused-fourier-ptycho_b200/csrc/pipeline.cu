@@ -252,47 +252,54 @@ __global__ void __launch_bounds__(fft::LG<N>::THREADS, fft::LG<N>::MINB)
 }
 
 // ---------------------------------------------------------------------------
-// L2 + L3 fused.  A 2-CTA cluster takes 2 LIN consecutive row lines r0-1 .. of one
-// LED (LIN per CTA, 1024 threads each): every line gets its inverse FFT and its
-// residual |z|/(h^2 p^2) - Y in shared memory; the CTAs then swap their boundary
-// residual rows through distributed shared memory, and the 2 LIN - 2 central lines
-// get the loss stencil, the phase and the forward FFT.  The pair's two outer lines
-// are halo: their inverse FFTs are recomputed by the neighbouring pairs.  The output
-// goes to a second buffer because neighbours still read the halo rows of the input.
+// L2 + L3 fused.  A cluster of CL CTAs takes CL LIN consecutive row lines of one LED
+// (LIN per CTA): every line gets its inverse FFT and its residual |z|/(h^2 p^2) - Y in
+// shared memory; the CTAs read their neighbours' boundary residual rows through
+// distributed shared memory, and the CL LIN - 2 central lines get the loss stencil, the
+// phase and the forward FFT.  The two outer lines are halo: their inverse FFTs are
+// recomputed by the neighbouring clusters.  The output goes to a second buffer because
+// neighbours still read the halo rows of the input.
 //
-// The row lines are strided in memory (element c of row r at c*h + r): instead of
-// 16 scattered 8-byte loads per thread, the TMA unit copies the CTA's tile of
-// rows [r0-2, r0-2+XR) x all columns into shared memory (boxes of XR x 256) and
-// the threads pick their values there; the stack tile of the same rows (uint16)
-// follows by TMA while the inverse FFTs run.  Lines whose row wraps past the
-// image edge (first and last pair of an LED) read global memory directly.
+// Cluster p holds rows p POUT + q (q < CL LIN, taken modulo h); its central lines are
+// q in [1, POUT] with p POUT + q <= h, so row 0 is central once (as row h, in the last
+// cluster of the LED) and the first row of every CTA, p POUT + j LIN, is even (the
+// 16-byte rule of the TMA row coordinate).
+//
+// The row lines are strided in memory (element c of row r at c h + r): the TMA unit
+// copies the CTA's LIN rows x all columns into shared memory (boxes of LIN x 256) and
+// the LIN amplitude rows (FP32, a row-major copy of the stack made once per solve) come
+// by bulk copy.  Lines past row h - 1 (the last cluster of an LED) read their field
+// from global memory.  The residual rows take the exchange area once the inverse FFTs
+// are done, so a CTA holds one field tile, the amplitude rows and the twiddles: about
+// 100 KB at 512 threads from h = 1024 (two CTAs per SM), 200 KB at 1024 threads below.
 // ---------------------------------------------------------------------------
-template <int N, int CL = 2>
+template <int N, int CL>
 struct L23 {
+    static constexpr int THREADS = N >= 1024 ? 512 : 1024;
+    static constexpr int MINB = THREADS == 512 ? 2 : 1;
     static constexpr int T = N / 16;
-    static constexpr int LIN = 1024 / T;              // lines per CTA
-    static constexpr int POUT = CL * LIN - 2;         // central lines per CL-CTA cluster
+    static constexpr int LIN = THREADS / T;           // lines per CTA
+    static constexpr int POUT = CL * LIN - 2;         // central lines per cluster
     static constexpr int PAD = 16 / LIN > 0 ? 16 / LIN : 1;
     static constexpr int STRIDE = N + PAD;            // FFT exchange line stride (float2)
-    // residual line stride (float): the 32 (line, t) pairs of a warp on 32 banks
+    // residual and amplitude row strides (float): the (line, t) pairs of a warp on
+    // distinct banks where the 16-byte bulk-copy rule allows (LIN <= 8)
     static constexpr int RSTRIDE = N + (LIN >= 32 ? 1 : 32 / LIN);
+    static constexpr int ASTRIDE = N + (LIN <= 8 ? 32 / LIN : 4);
     static constexpr int LINE_BYTES = LIN * STRIDE * 8;
-    // residual rows: the LIN lines plus a ghost row above and below (the partner's)
-    static constexpr int RES_BYTES = (LIN + 2) * RSTRIDE * 4;
+    static constexpr int AMP_BYTES = LIN * ASTRIDE * 4;
     static constexpr int CB = N < 256 ? N : 256;      // TMA box width along c
-    static constexpr int XR = LIN == 8 ? 12 : LIN + 2;   // field tile rows (even; 12: no bank conflicts)
-    static constexpr int YR = LIN + 8;                // stack tile rows (uint16, 16-byte aligned start)
-    static constexpr int SMEM = LINE_BYTES + RES_BYTES + 2 * 128 * 8 + 16;
+    static constexpr int SMEM = LINE_BYTES + AMP_BYTES + 2 * 128 * 8 + 16;
     static constexpr int PAIRS_PER_LED = (N + POUT - 1) / POUT;   // clusters per LED
     static constexpr int CTAS_PER_LED = CL * PAIRS_PER_LED;
     static constexpr int NHI = N >= 128 ? N / 128 : 1;
     static constexpr int NLO = N >= 128 ? 128 : N;
-    static_assert(LIN >= 8 && LIN % 8 == 0, "fused row pass needs T <= 128");
-    static_assert(POUT % 2 == 0, "even pair stride keeps the TMA row start even");
-    static_assert(XR * N * 8 <= LINE_BYTES + RES_BYTES, "field tile fits the line + residual areas");
-    static_assert(YR * N * 2 <= RES_BYTES, "stack tile fits the residual area");
-    static_assert(LINE_BYTES % 128 == 0, "residual area 128-byte aligned for TMA");
-    static_assert(SMEM + 256 <= 227 * 1024, "shared memory per CTA");
+    static_assert(LIN >= 4 && LIN % 2 == 0 && LIN <= 256, "TMA box rows");
+    static_assert(POUT % 2 == 0, "even cluster stride keeps the TMA row start even");
+    static_assert(LIN * N * 8 <= LINE_BYTES, "field tile fits the exchange area");
+    static_assert((LIN + 2) * RSTRIDE * 4 <= LINE_BYTES, "residual rows fit the exchange area");
+    static_assert(LINE_BYTES % 16 == 0 && (ASTRIDE * 4) % 16 == 0, "bulk-copy alignment");
+    static_assert(MINB * (SMEM + 1024) <= 228 * 1024, "shared memory per SM");
 };
 
 __device__ __forceinline__ void cluster_arrive() {
@@ -312,145 +319,128 @@ __device__ __forceinline__ float cluster_load(const float *p, unsigned rank) {
     return v;
 }
 
-template <int N, int TYPE, int LOSS, int CL>
-__global__ void __launch_bounds__(1024, 1)
-    k_lr_rows_fused(StackView Y, BatchGeom g, int l0, const float2 *__restrict__ T1,
-                    float2 *__restrict__ T2, double *__restrict__ parts, int *__restrict__ flag,
-                    const __grid_constant__ CUtensorMap tm_field,
-                    const __grid_constant__ CUtensorMap tm_stack, const float2 *__restrict__ thi,
+template <int N, int LOSS, int CL>
+__global__ void __launch_bounds__(L23<N, CL>::THREADS, L23<N, CL>::MINB)
+    k_lr_rows_fused(const float *__restrict__ amp, BatchGeom g, int l0,
+                    const float2 *__restrict__ T1, float2 *__restrict__ T2,
+                    double *__restrict__ parts, int *__restrict__ flag,
+                    const __grid_constant__ CUtensorMap tm_field, const float2 *__restrict__ thi,
                     const float2 *__restrict__ tlo) {
     using F = L23<N, CL>;
-    constexpr int T = F::T;
+    constexpr int T = F::T, LIN = F::LIN;
     extern __shared__ __align__(128) float2 smem[];
     __shared__ double s_red[32];
-    float *res = reinterpret_cast<float *>(smem + F::LIN * F::STRIDE);   // row 0: ghost above
-    float2 *s_hi = reinterpret_cast<float2 *>(res + (F::LIN + 2) * F::RSTRIDE);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(s_hi + 256);          // [0] field, [1] stack
-    const float2 *tile = smem;                                          // [c][XR] field tile
-    const uint16_t *ytile = reinterpret_cast<const uint16_t *>(res);    // [c][YR] stack tile
-    const int k = threadIdx.x % F::LIN, t = threadIdx.x / F::LIN;
+    float *ampt = reinterpret_cast<float *>(smem + LIN * F::STRIDE);     // [k][ASTRIDE]
+    float2 *s_hi = reinterpret_cast<float2 *>(ampt + LIN * F::ASTRIDE);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(s_hi + 256);          // [0] field, [1] rows
+    const float2 *tile = smem;                                          // [c][LIN] field tile
+    float *res = reinterpret_cast<float *>(smem);   // after the inverse FFTs: row 0 ghost above
+    const int k = threadIdx.x % LIN, t = threadIdx.x / LIN;
     const unsigned j = blockIdx.x % CL;                 // rank in the cluster
     const int pair = blockIdx.x / CL;
     const int lloc = pair / F::PAIRS_PER_LED;
-    const int r0 = (pair % F::PAIRS_PER_LED) * F::POUT + (int)j * F::LIN;   // rows r0-1+k
-    const int x0 = r0 - 2;                      // first tile row (even: 16-byte TMA rule)
-    const int y0 = (r0 - 1) & ~7;               // first stack tile row (8 x 2 bytes)
+    const int x0 = (pair % F::PAIRS_PER_LED) * F::POUT + (int)j * LIN;   // first row (even)
     const int zpage = g.z_off + l0 + lloc;
     // boxes of CB stored columns holding a supported crop column; with a field buffer
     // whose other columns are known zeros (t1_clean) only those are copied
     unsigned boxes = 0;
+    if (x0 < N) {
 #pragma unroll
-    for (int q = 0; q < N / F::CB; ++q) {
-        const int lo = (q * F::CB + N / 2) % N, hi = lo + F::CB;   // crop columns of box q
-        const bool sup = hi <= N ? (lo < g.pc_hi && hi > g.pc_lo)
-                                 : (lo < g.pc_hi || hi - N > g.pc_lo);
-        if (sup || !g.t1_clean) boxes |= 1u << q;
+        for (int q = 0; q < N / F::CB; ++q) {
+            const int lo = (q * F::CB + N / 2) % N, hi = lo + F::CB;   // crop columns of box q
+            const bool sup = hi <= N ? (lo < g.pc_hi && hi > g.pc_lo)
+                                     : (lo < g.pc_hi || hi - N > g.pc_lo);
+            if (sup || !g.t1_clean) boxes |= 1u << q;
+        }
     }
     if (threadIdx.x == 0) {
         tma::mbar_init(&bar[0], 1);
         tma::mbar_init(&bar[1], 1);
         tma::fence_barrier_init();
-        tma::arrive_expect_tx(&bar[0], (uint32_t)__popc(boxes) * F::XR * F::CB * 8);
+        tma::arrive_expect_tx(&bar[0], (uint32_t)__popc(boxes) * LIN * F::CB * 8);
 #pragma unroll 1
         for (int q = 0; q < N / F::CB; ++q)
             if (boxes >> q & 1u)
-                tma::load_3d(smem + q * F::CB * F::XR, &tm_field, x0, q * F::CB, lloc, &bar[0]);
+                tma::load_3d(smem + q * F::CB * LIN, &tm_field, x0, q * F::CB, lloc, &bar[0]);
+        tma::arrive_expect_tx(&bar[1], (uint32_t)LIN * N * 4);
     }
     fft::load_twiddles(s_hi, s_hi + 128, thi, tlo, F::NHI, F::NLO);
-    __syncthreads();                                    // barriers initialised before any wait
-    const int rraw = r0 - 1 + k;                        // row before the wrap
-    const bool wrapped = rraw < 0 || rraw >= N;
-    const int r = rraw < 0 ? rraw + N : (rraw >= N ? rraw - N : rraw);
-    const int q = (int)j * F::LIN + k;                  // line within the pair
-    const bool central = q >= 1 && q <= F::POUT && rraw < N;
+    __syncthreads();                                    // barriers initialised before any use
+    if (threadIdx.x >> 5 == 1) {                        // warp 1: the amplitude rows
+        for (int kk = threadIdx.x & 31; kk < LIN; kk += 32) {
+            const int rr = (x0 + kk) & (N - 1);
+            tma::load_1d(ampt + kk * F::ASTRIDE, amp + ((size_t)zpage * N + rr) * N, N * 4,
+                         &bar[1]);
+        }
+    }
+    const int rraw = x0 + k;                            // row before the wrap
+    const bool wrapped = rraw >= N;
+    const int r = rraw & (N - 1);
+    const int q = (int)j * LIN + k;                     // line within the cluster
+    const bool central = q >= 1 && q <= F::POUT && rraw <= N;
     float *rk = res + (k + 1) * F::RSTRIDE;
     float2 v[16];
-    if (wrapped) {   // first / last pair of an LED: the wrapped halo row from global memory
+    if (wrapped) {   // past the last row: the field from global memory
         const float2 *page = T1 + (size_t)lloc * N * N + r;
 #pragma unroll
         for (int m = 0; m < 16; ++m) v[m] = page[(size_t)(t + m * T) * N];
     }
-    // A tile load that never completes is flagged for the host; the CTA then skips its
-    // work but still passes both cluster barriers, so its partner never waits for ever.
+    // A copy that never completes is flagged for the host; the CTA then skips its work
+    // but still passes every cluster barrier, so its partners never wait for ever.
     bool failed = __syncthreads_or(!tma::mbar_wait(&bar[0], 0));
     if (failed && threadIdx.x == 0) {
         atomicExch(flag, 1);
         tma::mbar_wait(&bar[0], 0);
     }
-    double lsum = 0.0;
     if (!failed) {
         if (!wrapped) {
 #pragma unroll
             for (int m = 0; m < 16; ++m)
-                v[m] = boxes >> ((t + m * T) / F::CB) & 1u ? tile[(t + m * T) * F::XR + (rraw - x0)]
+                v[m] = boxes >> ((t + m * T) / F::CB) & 1u ? tile[(t + m * T) * LIN + k]
                                                           : make_float2(0.f, 0.f);
         }
         __syncthreads();                                // the tile area becomes FFT scratch
-        if (TYPE == kStackU16 && threadIdx.x == 0) {
-            tma::fence_proxy_async();
-            tma::arrive_expect_tx(&bar[1], F::YR * N * 2);
-#pragma unroll 1
-            for (int qb = 0; qb < N / F::CB; ++qb)
-                tma::load_3d(const_cast<uint16_t *>(ytile) + qb * F::CB * F::YR, &tm_stack, y0,
-                             qb * F::CB, zpage, &bar[1]);
-        }
         fft::line_fft_regs<N, +1>(v, smem + k * F::STRIDE, s_hi, s_hi + 128, t);
-        float mn = 0.f, range = 0.f;
-        if (TYPE == kStackU16) {
-            mn = (float)Y.minmax[0];
-            range = (float)(Y.minmax[1] - Y.minmax[0]);
-        }
-        // 1 / (h^2 p^2): a power of two, so the product equals the quotient exactly
-    const float inv_ratio = (float)(1.0 / ((double)N * N * g.pratio * g.pratio));
-        const size_t ypage = (size_t)zpage * N * N + r;
-        float y[16];
-        if (TYPE == kStackU16) {
-            failed = __syncthreads_or(!tma::mbar_wait(&bar[1], 0));
-            if (failed && threadIdx.x == 0) {
-                atomicExch(flag, 1);
-                tma::mbar_wait(&bar[1], 0);
-            }
-            if (!failed) {
-#pragma unroll
-                for (int m = 0; m < 16; ++m) {
-                    const int c = t + m * T;
-                    const uint16_t raw = wrapped ? static_cast<const uint16_t *>(Y.ptr)[ypage + (size_t)c * N]
-                                                 : ytile[c * F::YR + (rraw - y0)];
-                    if (Y.lut) {
-                        y[m] = Y.lut[raw];
-                    } else {
-                        const float x = (float)raw - mn;
-                        y[m] = range > 0.f ? sqrtf(x / range) : sqrtf(x);
-                    }
-                }
-            }
-            __syncthreads();                            // the stack tile area becomes residuals
-        } else {
-#pragma unroll
-            for (int m = 0; m < 16; ++m)
-                y[m] = amplitude<TYPE>(Y, ypage + (size_t)(t + m * T) * N, mn, range);
-        }
-        if (!failed) {
-#pragma unroll
-            for (int m = 0; m < 16; ++m) {
-                const float2 z = v[m];
-                rk[t + m * T] = sqrtf(z.x * z.x + z.y * z.y) * inv_ratio - y[m];
-            }
-        }
-        __syncthreads();
     }
-    // residual rows of both CTAs written: take the partner's boundary row as a ghost row
+    // every read of the exchange area done (the residuals take it) and the rows in
+    const bool failed_rows = __syncthreads_or(!tma::mbar_wait(&bar[1], 0));
+    if (failed_rows && threadIdx.x == 0) {
+        atomicExch(flag, 1);
+        tma::mbar_wait(&bar[1], 0);
+    }
+    failed = failed || failed_rows;
+    if (!failed) {
+        // 1 / (h^2 p^2): a power of two, so the product equals the quotient exactly
+        const float inv_ratio = (float)(1.0 / ((double)N * N * g.pratio * g.pratio));
+        const float *ak = ampt + k * F::ASTRIDE;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const float2 z = v[m];
+            const float mag = sqrtf(z.x * z.x + z.y * z.y);
+            rk[t + m * T] = mag * inv_ratio - ak[t + m * T];
+            // z / |z| for the phase of the gradient (zero where |z| is): the stencil step
+            // multiplies it by d, in the order (z.x / |z|) d
+            if (mag > 0.f) {
+                const float inv = 1.0f / mag;
+                v[m] = make_float2(z.x * inv, z.y * inv);
+            } else {
+                v[m] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+    // residual rows of every CTA written: take the neighbours' boundary rows as ghosts
     cluster_arrive();
     cluster_wait();
     if (!failed) {
         // ghost above: the last line of rank j-1; ghost below: the first line of rank j+1
-        for (int c = threadIdx.x; c < N; c += 1024) {
-            if (j > 0) res[c] = cluster_load(res + F::LIN * F::RSTRIDE + c, j - 1);
-            if (j + 1 < CL) res[(F::LIN + 1) * F::RSTRIDE + c] = cluster_load(res + F::RSTRIDE + c, j + 1);
+        for (int c = threadIdx.x; c < N; c += F::THREADS) {
+            if (j > 0) res[c] = cluster_load(res + LIN * F::RSTRIDE + c, j - 1);
+            if (j + 1 < CL) res[(LIN + 1) * F::RSTRIDE + c] = cluster_load(res + F::RSTRIDE + c, j + 1);
         }
         __syncthreads();
     }
-    cluster_arrive();   // done with the partner's memory; waited for before leaving
+    cluster_arrive();   // done with the neighbours' memory; waited for before the area is reused
+    double lsum = 0.0;
     if (!failed) {
         const float gscale = (float)(g.pratio * g.pratio);
 #pragma unroll
@@ -464,25 +454,26 @@ __global__ void __launch_bounds__(1024, 1)
                                   LOSS == kLossAnisotropic ? 0.f : rk[F::RSTRIDE + cm],
                                   LOSS == kLossAnisotropic ? 0.f : rk[cp - F::RSTRIDE], lsum) *
                     gscale;
-                const float2 z = v[m];
-                const float mag = sqrtf(z.x * z.x + z.y * z.y);
-                if (mag > 0.f) {
-                    const float inv = 1.0f / mag;
-                    o.x = z.x * inv * d;
-                    o.y = z.y * inv * d;
+                const float2 u = v[m];   // z / |z|, or zero
+                if (u.x != 0.f || u.y != 0.f) {
+                    o.x = u.x * d;
+                    o.y = u.y * d;
                 }
             }
             v[m] = o;
         }
+    }
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
-        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = lsum;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (int w = 0; w < 32; ++w) tot += s_red[w];
-            parts[blockIdx.x] = tot;
-        }
+    for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = lsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < F::THREADS / 32; ++w) tot += s_red[w];
+        parts[blockIdx.x] = failed ? 0.0 : tot;
+    }
+    cluster_wait();     // the neighbours are done with this CTA's residual rows
+    if (!failed) {
         fft::line_fft_regs<N, -1>(v, smem + k * F::STRIDE, s_hi, s_hi + 128, t);
         if (central) {   // only the columns the next pass transforms (pupil support, fftshifted)
             float2 *dst = T2 + (size_t)lloc * N * N + r;
@@ -493,10 +484,7 @@ __global__ void __launch_bounds__(1024, 1)
                 if (c >= g.pc_lo && c < g.pc_hi) dst[(size_t)cf * N] = v[m];
             }
         }
-    } else if (threadIdx.x == 0) {
-        parts[blockIdx.x] = 0.0;
     }
-    cluster_wait();
 }
 
 // ---------------------------------------------------------------------------
@@ -1280,11 +1268,11 @@ cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, 
 
 bool lr_rows_fused_supported(int h) { return h >= 128 && h <= 2048 && (h & (h - 1)) == 0; }
 
-static int fused_cluster();
+static int fused_cluster(int h);
 
 static int ctas_per_led_fused(int h) {   // L23<h, CL>::CTAS_PER_LED
-    const int cl = fused_cluster();
-    const int pout = cl * (1024 / (h / 16)) - 2;
+    const int cl = fused_cluster(h);
+    const int pout = cl * ((h >= 1024 ? 512 : 1024) / (h / 16)) - 2;
     return cl * ((h + pout - 1) / pout);
 }
 
@@ -1332,17 +1320,18 @@ static cudaError_t page_tile_map(CUtensorMap *map, CUtensorMapDataType type, siz
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-template <int N, int TYPE, int LOSS, int CL>
-static cudaError_t launch_fused_cl(int nl, StackView Y, const BatchGeom &g, int l0,
+template <int N, int LOSS, int CL>
+static cudaError_t launch_fused_cl(int nl, const float *amp, const BatchGeom &g, int l0,
                                    const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
-                                   const CUtensorMap &tm_stack, const Twiddles &tw, cudaStream_t st) {
-    auto kern = k_lr_rows_fused<N, TYPE, LOSS, CL>;
-    cudaError_t e = set_smem(kern, L23<N, CL>::SMEM);
+                                   const Twiddles &tw, cudaStream_t st) {
+    using F = L23<N, CL>;
+    auto kern = k_lr_rows_fused<N, LOSS, CL>;
+    cudaError_t e = set_smem(kern, F::SMEM);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(nl * L23<N, CL>::CTAS_PER_LED));
-    cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = L23<N, CL>::SMEM;
+    cfg.gridDim = dim3((unsigned)(nl * F::CTAS_PER_LED));
+    cfg.blockDim = dim3(F::THREADS);
+    cfg.dynamicSmemBytes = F::SMEM;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1351,52 +1340,41 @@ static cudaError_t launch_fused_cl(int nl, StackView Y, const BatchGeom &g, int 
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, Y, g, l0, (const float2 *)b.T1, b.T2, b.parts + part_off,
-                              b.flag, tm_field, tm_stack, tw.lo_hi, tw.lo_lo);
+    return cudaLaunchKernelEx(&cfg, kern, amp, g, l0, (const float2 *)b.T1, b.T2,
+                              b.parts + part_off, b.flag, tm_field, tw.lo_hi, tw.lo_lo);
 }
 
-// cluster size of the fused row pass: 2 (FPM_L23_CLUSTER=4 for measurements)
-static int fused_cluster() {
-    return knob("FPM_L23_CLUSTER", tuning().l23_cluster, 0, 2) == 4 ? 4 : 2;
+// cluster size of the fused row pass: 16 lines per cluster by default (4 CTAs of 4 lines
+// at h = 2048, 2 CTAs below); FPM_L23_CLUSTER (or the tuner) picks 2, 4 or 8
+static int fused_cluster(int h) {
+    const int v = knob("FPM_L23_CLUSTER", tuning().l23_cluster, 0, h == 2048 ? 4 : 2);
+    return v == 8 ? 8 : (v == 4 ? 4 : 2);
 }
 
-template <int N, int TYPE, int LOSS>
-static cudaError_t launch_fused_k(int nl, StackView Y, const BatchGeom &g, int l0,
+template <int N, int LOSS>
+static cudaError_t launch_fused_k(int nl, const float *amp, const BatchGeom &g, int l0,
                                   const BatchBufs &b, int part_off, const CUtensorMap &tm_field,
-                                  const CUtensorMap &tm_stack, const Twiddles &tw, cudaStream_t st) {
-    return fused_cluster() == 4
-               ? launch_fused_cl<N, TYPE, LOSS, 4>(nl, Y, g, l0, b, part_off, tm_field, tm_stack, tw, st)
-               : launch_fused_cl<N, TYPE, LOSS, 2>(nl, Y, g, l0, b, part_off, tm_field, tm_stack, tw, st);
+                                  const Twiddles &tw, cudaStream_t st) {
+    switch (fused_cluster(N)) {
+        case 8: return launch_fused_cl<N, LOSS, 8>(nl, amp, g, l0, b, part_off, tm_field, tw, st);
+        case 4: return launch_fused_cl<N, LOSS, 4>(nl, amp, g, l0, b, part_off, tm_field, tw, st);
+        default: return launch_fused_cl<N, LOSS, 2>(nl, amp, g, l0, b, part_off, tm_field, tw, st);
+    }
 }
 
-cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_pages, BatchBufs b,
-                                 int l0, int nl, int part_off, const Twiddles &tw,
-                                 cudaStream_t st) {
+cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, BatchBufs b, int l0, int nl,
+                                 int part_off, const Twiddles &tw, cudaStream_t st) {
+    if (!Y.rows) return cudaErrorInvalidValue;   // the amplitude rows are made per solve
     cudaError_t e = cudaSuccess;
-    CUtensorMap tm_field{}, tm_stack{};
+    CUtensorMap tm_field{};
 #define F(N)                                                                              \
-    static_assert(L23<N, 2>::CTAS_PER_LED ==                                              \
-                      2 * ((N + 2 * (1024 / (N / 16)) - 3) / (2 * (1024 / (N / 16)) - 2)),     \
-                  "host CTA count");                                                      \
+    static_assert(L23<N, 2>::LIN == (N >= 1024 ? 512 : 1024) / (N / 16), "host CTA count");  \
     e = page_tile_map(&tm_field, CU_TENSOR_MAP_DATA_TYPE_UINT64, 8, b.T1, N, nl,          \
-                      L23<N, 2>::XR, L23<N, 2>::CB);                                            \
+                      L23<N, 2>::LIN, L23<N, 2>::CB);                                     \
     if (e != cudaSuccess) return e;                                                       \
-    if (Y.type == kStackU16) {                                                            \
-        e = page_tile_map(&tm_stack, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, Y.ptr, N,         \
-                          stack_pages, L23<N, 2>::YR, L23<N, 2>::CB);                           \
-        if (e != cudaSuccess) return e;                                                   \
-        e = g.loss == kLossIsotropic                                                      \
-                ? launch_fused_k<N, kStackU16, kLossIsotropic>(nl, Y, g, l0, b, part_off, \
-                                                               tm_field, tm_stack, tw, st)    \
-                : launch_fused_k<N, kStackU16, kLossAnisotropic>(nl, Y, g, l0, b, part_off, \
-                                                                 tm_field, tm_stack, tw, st); \
-    } else {                                                                              \
-        e = g.loss == kLossIsotropic                                                      \
-                ? launch_fused_k<N, kStackF32, kLossIsotropic>(nl, Y, g, l0, b, part_off, \
-                                                               tm_field, tm_stack, tw, st)    \
-                : launch_fused_k<N, kStackF32, kLossAnisotropic>(nl, Y, g, l0, b, part_off, \
-                                                                 tm_field, tm_stack, tw, st); \
-    }                                                                                     \
+    e = g.loss == kLossIsotropic                                                          \
+            ? launch_fused_k<N, kLossIsotropic>(nl, Y.rows, g, l0, b, part_off, tm_field, tw, st) \
+            : launch_fused_k<N, kLossAnisotropic>(nl, Y.rows, g, l0, b, part_off, tm_field, tw, st); \
     if (e != cudaSuccess) return e;
     FPM_DISPATCH_FUSED(g.h, F)
 #undef F

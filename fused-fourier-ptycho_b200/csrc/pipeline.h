@@ -57,12 +57,12 @@ cudaError_t launch_lr_rows_inv(const BatchGeom &g, StackView Y, BatchBufs b, int
 cudaError_t launch_lr_rows_fwd(const BatchGeom &g, BatchBufs b, int l0, int nl, int part_off,
                                const Twiddles &tw, cudaStream_t st);
 // L2 + L3 in one pass (h in [128, 2048]): T1 -> T2, loss partials at parts + part_off,
-// lr_rows_fused_blocks(h, nl) of them.
+// lr_rows_fused_blocks(h, nl) of them; reads the amplitude rows Y.rows
+// (launch_amplitude_rows), not the stack itself.
 bool lr_rows_fused_supported(int h);
 int lr_rows_fused_blocks(int h, int nl);
-cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, int stack_pages, BatchBufs b,
-                                 int l0, int nl, int part_off, const Twiddles &tw,
-                                 cudaStream_t st);
+cudaError_t launch_lr_rows_fused(const BatchGeom &g, StackView Y, BatchBufs b, int l0, int nl,
+                                 int part_off, const Twiddles &tw, cudaStream_t st);
 // L4 over src (T1 after separate L2, L3; T2 after the fused pass) -> Xs
 cudaError_t launch_lr_cols_fwd(const BatchGeom &g, const float2 *src, BatchBufs b, int l0,
                                int nl, const Twiddles &tw, cudaStream_t st);

@@ -11,7 +11,7 @@ namespace fpm {
 struct Tuning {
     int lr_group = 0;       // LEDs per low-resolution launch group; 0 = the whole batch
     int lr_fused = -1;      // fused row pass (h in [128, 2048]): -1 default (on), 0, 1
-    int l23_cluster = 0;    // CTAs per cluster of the fused row pass: 0 default (2), 2, 4
+    int l23_cluster = 0;    // CTAs per cluster of the fused row pass: 0 default (16 lines), 2, 4, 8
     int cols_async = -1;    // bulk-copy prefetch in the 16384-point passes: -1 (on), 0, 1
     int cols_e16 = -1;      // 16 values per thread in the 16384-point passes: -1 (off), 0, 1
     int gen_lpc = 0;        // lines per CTA of the any-size line FFT; 0 = planned
