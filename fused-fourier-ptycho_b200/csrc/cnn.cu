@@ -1,145 +1,292 @@
 // Kernels of the learned warm start (cnn.h).
 //
-// Convolutions are implicit GEMMs on the tensor cores: a CTA of four warps computes a
-// 64 x 64 tile of C = A B, staging 64 x 32 and 32 x 64 BF16 tiles of A and B in shared
-// memory (rounded from the FP32 activations as they are gathered), each warp a 32 x 32
-// block of 2 x 2 WMMA 16x16x16 fragments with FP32 accumulators; the tile goes back
-// through shared memory to a per-GEMM epilogue.  Gathers and stores run with consecutive
-// threads on consecutive pixels.
-//   forward      M = N*H*W pixels, N = Cout, K = Cin*9: A = im2col(in), B = W^T
+// Convolutions are implicit GEMMs on the fifth-generation tensor cores (tcgen05, umma.cuh):
+// a CTA of 128 threads computes a 128-row tile of D = A B^T with all of B's rows (at most
+// 256) as the MMA's N, the FP32 accumulator in tensor memory.  The threads stage the
+// operands as BF16 (rounded from the FP32 activations as they are gathered, the weights
+// already BF16) into two shared-memory stages of 64 K columns in the 128-byte swizzled
+// K-major layout while one thread issues the MMAs of the other stage; the epilogue reads
+// the accumulator back with tcgen05.ld, one TMEM lane per tile row.
+//   forward      rows = N*H*W pixels, K = Cin*9, B = W (rows co): D = im2col(in) W^T
 //   data grad    the forward GEMM on the output gradient with the flipped weights
-//   weight grad  M = Cout, N = Cin*9, K = N*H*W: A = dout, B = im2col(in)^T, split over K
-//                into partials that one more pass sums in split order (deterministic)
-#include <mma.h>
+//   weight grad  rows = Cin*9 taps, K = N*H*W pixels, B = dout (rows co): D = dW^T, split
+//                over the pixels into partials that one more pass sums in split order
+//                (deterministic)
+// Gathers run with consecutive threads on consecutive pixels where the layout allows.
+#include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdint>
 
 #include "cnn.h"
 #include "common.cuh"
+#include "tma.cuh"
+#include "umma.cuh"
 
 namespace fpm {
 namespace cnn {
 
 namespace {
 
-using namespace nvcuda;
-
-constexpr int BM = 64, BN = 64, BK = 32, GT = 128;
-constexpr int LDA = BK + 8, LDB = BN + 8, LDC = BN + 4;
+constexpr int kTM = 128;              // MMA M: rows of a tile, one thread per row
+constexpr int kTK = 64;               // K per stage: one 128-byte row of BF16
+constexpr int kThreads = 128;
+constexpr int kATile = kTM * 128;     // bytes of one A stage
 
 unsigned grid_1d(size_t n) {
     return (unsigned)std::min<size_t>((n + 255) / 256, (size_t)kB200SMs * 16);
 }
 
-// Generic tile GEMM; Op supplies a(m, k), b(k, n) as floats, c(m, n, value, split) and
-// which index varies fastest across threads when gathering / storing.
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);   // lo at the lower address
+    return *reinterpret_cast<const uint32_t *>(&p);
+}
+
+// 16-byte chunk c of row r of a swizzled K-major operand tile (umma.cuh)
+__device__ __forceinline__ uint4 *chunk(uint8_t *tile, int r, int c) {
+    return reinterpret_cast<uint4 *>(tile + r * 128 + ((c ^ (r & 7)) << 4));
+}
+
+// One tile of D = A B^T on the tensor cores: D (kTM rows x bn columns, FP32) in TMEM;
+// A (kTM x K) and B (bn x K) staged as BF16 by the CTA's threads through two shared-
+// memory stages of kTK columns each while the MMAs of the other stage run (one thread
+// issues them, completion on one mbarrier per stage).  Op supplies
+//   kdim()                         the GEMM's K (its M is the host's `rows`)
+//   build_a(tile, m0, k0)          row threadIdx.x of A, K columns k0 .. k0 + 63
+//   build_b(tile, bn, k0)          all bn rows of B, the same K columns
+//   store(m, n0, v[16], split)     D(m, n0 .. n0 + 15) of K split `split`
+// Blocks: x = M tile, z = K split (kchunk columns, a multiple of kTK).  A wait that
+// runs out sets *flag and skips the epilogue; TMEM is always freed.
 template <class Op>
-__global__ void __launch_bounds__(GT) k_gemm(Op op, int M, int N, int K, int kchunk) {
-    __shared__ __align__(32) __nv_bfloat16 sA[BM * LDA];
-    __shared__ __align__(32) __nv_bfloat16 sB[BK * LDB];
-    __shared__ __align__(32) float sC[BM * LDC];
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int kbeg = blockIdx.z * kchunk, kend = min(K, kbeg + kchunk);
+__global__ void __launch_bounds__(kThreads) k_umma_gemm(Op op, int bn, int kchunk, int *flag) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t pad = (1024u - (umma::saddr(smem_raw) & 1023u)) & 1023u;
+    uint8_t *base = smem_raw + pad;                      // swizzle atoms need 1024-byte bases
+    uint8_t *sa[2] = {base, base + kATile};
+    uint8_t *sb[2] = {base + 2 * kATile, base + 2 * kATile + bn * 128};
+    uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * kATile + 2 * bn * 128);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 2);
     const int warp = threadIdx.x >> 5;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) wmma::fill_fragment(acc[i][j], 0.0f);
-    for (int k0 = kbeg; k0 < kend; k0 += BK) {
-        for (int i = threadIdx.x; i < BM * BK; i += GT) {
-            const int r = Op::A_ROW_FAST ? i % BM : i / BK;
-            const int c = Op::A_ROW_FAST ? i / BM : i % BK;
-            const int m = m0 + r, k = k0 + c;
-            sA[r * LDA + c] = __float2bfloat16_rn(m < M && k < kend ? op.a(m, k) : 0.f);
-        }
-        for (int i = threadIdx.x; i < BK * BN; i += GT) {
-            const int r = Op::B_ROW_FAST ? i % BK : i / BN;
-            const int c = Op::B_ROW_FAST ? i / BK : i % BN;
-            const int k = k0 + r, n = n0 + c;
-            sB[r * LDB + c] = __float2bfloat16_rn(k < kend && n < N ? op.b(k, n) : 0.f);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += 16) {
-            wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> fa[2];
-            wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> fb[2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) wmma::load_matrix_sync(fa[i], sA + (wm + 16 * i) * LDA + kk, LDA);
-#pragma unroll
-            for (int j = 0; j < 2; ++j) wmma::load_matrix_sync(fb[j], sB + kk * LDB + wn + 16 * j, LDB);
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) wmma::mma_sync(acc[i][j], fa[i], fb[j], acc[i][j]);
-        }
-        __syncthreads();
+    const int m0 = blockIdx.x * kTM;
+    const int K = op.kdim();
+    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+    const int ntiles = (ke - kb + kTK - 1) / kTK;
+    const uint32_t ncols = umma::tmem_cols(bn);
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_barrier_init();
     }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-            wmma::store_matrix_sync(sC + (wm + 16 * i) * LDC + wn + 16 * j, acc[i][j], LDC,
-                                    wmma::mem_row_major);
+    if (warp == 0) umma::alloc(slot, ncols);
+    umma::fence_before_sync();
     __syncthreads();
-    for (int i = threadIdx.x; i < BM * BN; i += GT) {
-        const int r = Op::C_ROW_FAST ? i % BM : i / BN;
-        const int c = Op::C_ROW_FAST ? i / BM : i % BN;
-        const int m = m0 + r, n = n0 + c;
-        if (m < M && n < N) op.c(m, n, sC[r * LDC + c], blockIdx.z);
+    umma::fence_after_sync();
+    const uint32_t tmem = *slot;
+    const uint32_t idesc = umma::idesc_bf16_f32(kTM, bn);
+    bool failed = false;
+    int issued = 0;
+    for (int t = 0; t < ntiles; ++t) {
+        const int s = t & 1;
+        if (t >= 2) {   // the MMAs of tile t - 2 are done with stage s
+            failed = __syncthreads_or(!tma::mbar_wait(&bar[s], ((t - 2) >> 1) & 1));
+            if (failed) break;
+        }
+        const int k0 = kb + t * kTK;
+        op.build_a(sa[s], m0, k0);
+        op.build_b(sb[s], bn, k0);
+        tma::fence_proxy_async();   // the stores above, visible to the tensor cores
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            umma::fence_after_sync();
+            const uint32_t a = umma::saddr(sa[s]), b = umma::saddr(sb[s]);
+#pragma unroll
+            for (int kk = 0; kk < kTK / 16; ++kk)
+                umma::mma_bf16(tmem, umma::sw128_desc(a + 32 * kk), umma::sw128_desc(b + 32 * kk),
+                               idesc, (t > 0 || kk > 0) ? 1u : 0u);
+            umma::commit(&bar[s]);
+        }
+        issued = t + 1;
+    }
+    if (!failed && issued > 0) {   // the last commit covers every MMA before it
+        const int tl = issued - 1;
+        failed = __syncthreads_or(!tma::mbar_wait(&bar[tl & 1], (tl >> 1) & 1));
+    }
+    if (failed) {
+        if (threadIdx.x == 0) {
+            atomicExch(flag, 1);
+            if (issued > 0) tma::mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1);
+        }
+    } else {
+        umma::fence_after_sync();
+        const int row = warp * 32 + (threadIdx.x & 31);   // TMEM lane = tile row
+        for (int c0 = 0; c0 < bn; c0 += 16) {
+            float v[16];
+            umma::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            op.store(m0 + row, c0, v, blockIdx.z);
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::dealloc(tmem, ncols);
     }
 }
 
-// in[n][ci][y+ky-1][x+kx-1] for pixel q = (n, y, x) and tap j = (ci, ky, kx), 0 outside
-__device__ __forceinline__ float im2col(const float *in, int Cin, int Hh, int Ww, int q, int j) {
-    const int HW = Hh * Ww;
-    const int n = q / HW, p = q - n * HW;
-    const int y = p / Ww, x = p - y * Ww;
-    const int ci = j / 9, t = j - ci * 9;
-    const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
-    if (yy < 0 || yy >= Hh || xx < 0 || xx >= Ww) return 0.f;
-    return in[((size_t)(n * Cin + ci) * Hh + yy) * Ww + xx];
-}
-
+// Forward convolution: rows = pixels q = (n, y, x), K = taps j = (ci, ky, kx) in the
+// order of W[co][ci][ky][kx]; B = the BF16 weights, rows co (ldw >= 9 Cin per row, zero
+// beyond 9 Cin, zero rows up to the padded bn); out[n][co][y][x] = bias[co] + D.
 struct ConvFwd {
-    static constexpr bool A_ROW_FAST = true, B_ROW_FAST = true, C_ROW_FAST = true;
     const float *in;
     const __nv_bfloat16 *W;
+    int ldw;
     const float *bias;
     float *out;
-    int Cin, Hh, Ww, Cout;
-    __device__ float a(int m, int k) const { return im2col(in, Cin, Hh, Ww, m, k); }
-    __device__ float b(int k, int co) const { return __bfloat162float(W[(size_t)co * Cin * 9 + k]); }
-    __device__ void c(int m, int co, float v, int) const {
+    int N, Cin, Hh, Ww, Cout;
+    __device__ int kdim() const { return Cin * 9; }
+    __device__ void build_a(uint8_t *tile, int m0, int k0) const {
+        const int r = threadIdx.x, q = m0 + r;
+        const int HW = Hh * Ww, K = Cin * 9;
+        const bool live = q < N * HW;
+        int n = 0, y = 0, x = 0;
+        if (live) {
+            n = q / HW;
+            const int p = q - n * HW;
+            y = p / Ww;
+            x = p - y * Ww;
+        }
+        const float *src = in + (size_t)n * Cin * HW;
+        int ci = k0 / 9, t = k0 - ci * 9;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            uint32_t w[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float v2[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = k0 + c * 8 + e * 2 + h;
+                    const int ky = t / 3, yy = y + ky - 1, xx = x + (t - 3 * ky) - 1;
+                    float a = 0.f;
+                    if (live && k < K && yy >= 0 && yy < Hh && xx >= 0 && xx < Ww)
+                        a = src[(size_t)ci * HW + yy * Ww + xx];
+                    v2[h] = a;
+                    if (++t == 9) {
+                        t = 0;
+                        ++ci;
+                    }
+                }
+                w[e] = pack_bf16(v2[0], v2[1]);
+            }
+            *chunk(tile, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+    __device__ void build_b(uint8_t *tile, int nrows, int k0) const {
+        for (int i = threadIdx.x; i < nrows * 8; i += kThreads) {
+            const int r = i >> 3, c = i & 7;
+            *chunk(tile, r, c) = *reinterpret_cast<const uint4 *>(W + (size_t)r * ldw + k0 + c * 8);
+        }
+    }
+    __device__ void store(int m, int co0, const float (&v)[16], int) const {
         const int HW = Hh * Ww;
+        if (m >= N * HW) return;
         const int n = m / HW, p = m - n * HW;
-        out[(size_t)(n * Cout + co) * HW + p] = bias ? v + bias[co] : v;
+        float *o = out + (size_t)n * Cout * HW + p;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int co = co0 + j;
+            if (co < Cout) o[(size_t)co * HW] = bias ? v[j] + bias[co] : v[j];
+        }
     }
 };
 
+// Weight gradient, transposed: rows = taps k = (ci, ky, kx), K = pixels q; A = im2col(in)^T,
+// B = dout (rows co, zero rows up to bn); D(k, co) = dW[co][k] of the split's pixels,
+// into part[split][co][k].
 struct ConvWgrad {
-    static constexpr bool A_ROW_FAST = false, B_ROW_FAST = true, C_ROW_FAST = false;
     const float *in, *dout;
     float *part;
-    int Cin, Hh, Ww, Cout;
-    __device__ float a(int co, int q) const {
-        const int HW = Hh * Ww;
-        const int n = q / HW, p = q - n * HW;
-        return dout[(size_t)(n * Cout + co) * HW + p];
+    int N, Cin, Hh, Ww, Cout;
+    __device__ int kdim() const { return N * Hh * Ww; }
+    __device__ void build_a(uint8_t *tile, int m0, int q0) const {
+        const int r = threadIdx.x, k = m0 + r;
+        const int HW = Hh * Ww, Q = N * HW;
+        const bool live = k < Cin * 9;
+        const int ci = live ? k / 9 : 0, t = k - ci * 9;
+        const int ky = t / 3, dy = ky - 1, dx = t - 3 * ky - 1;
+        int n = q0 / HW, p = q0 - n * HW;
+        int y = p / Ww, x = p - y * Ww;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            uint32_t w[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float v2[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int q = q0 + c * 8 + e * 2 + h;
+                    const int yy = y + dy, xx = x + dx;
+                    float a = 0.f;
+                    if (live && q < Q && yy >= 0 && yy < Hh && xx >= 0 && xx < Ww)
+                        a = in[((size_t)(n * Cin + ci) * Hh + yy) * Ww + xx];
+                    v2[h] = a;
+                    if (++x == Ww) {
+                        x = 0;
+                        if (++y == Hh) {
+                            y = 0;
+                            ++n;
+                        }
+                    }
+                }
+                w[e] = pack_bf16(v2[0], v2[1]);
+            }
+            *chunk(tile, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
-    __device__ float b(int q, int j) const { return im2col(in, Cin, Hh, Ww, q, j); }
-    __device__ void c(int co, int j, float v, int z) const {
-        part[((size_t)z * Cout + co) * Cin * 9 + j] = v;
+    __device__ void build_b(uint8_t *tile, int nrows, int q0) const {
+        const int HW = Hh * Ww, Q = N * HW;
+        for (int i = threadIdx.x; i < nrows * 8; i += kThreads) {
+            const int r = i >> 3, c = i & 7;   // row co, pixels q0 + 8 c .. + 7
+            int q = q0 + c * 8;
+            int n = q / HW, p = q - n * HW;
+            uint32_t w[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float v2[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    v2[h] = r < Cout && q < Q ? dout[((size_t)n * Cout + r) * HW + p] : 0.f;
+                    ++q;
+                    if (++p == HW) {
+                        p = 0;
+                        ++n;
+                    }
+                }
+                w[e] = pack_bf16(v2[0], v2[1]);
+            }
+            *chunk(tile, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+    __device__ void store(int k, int co0, const float (&v)[16], int z) const {
+        const int K = Cin * 9;
+        if (k >= K) return;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int co = co0 + j;
+            if (co < Cout) part[((size_t)z * Cout + co) * K + k] = v[j];
+        }
     }
 };
 
-__global__ void k_flip(const __nv_bfloat16 *W, int Cout, int Cin, __nv_bfloat16 *Wt) {
+// Wt[ci][co*9 + 8 - t] = W[co][ci*9 + t] (rows of ldw and ldt values, pads untouched)
+__global__ void k_flip(const __nv_bfloat16 *W, int ldw, int Cout, int Cin, __nv_bfloat16 *Wt,
+                       int ldt) {
     const int total = Cout * Cin * 9;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const int co = i / (Cin * 9), rem = i - co * Cin * 9;
         const int ci = rem / 9, t = rem - ci * 9;
-        Wt[((size_t)ci * Cout + co) * 9 + (8 - t)] = W[i];    // (ky, kx) -> (2-ky, 2-kx)
+        Wt[(size_t)ci * ldt + co * 9 + (8 - t)] = W[(size_t)co * ldw + rem];   // (ky, kx) -> (2-ky, 2-kx)
     }
 }
 
@@ -263,8 +410,11 @@ __global__ void k_mse_final(const double *work, int nb, size_t n, double *loss) 
     }
 }
 
+// Adam on n FP32 weights; the BF16 copy (if any) of element i goes to
+// wb[(i / row) * ldb + i % row] (rows of `row` values padded to ldb)
 __global__ void k_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, size_t n,
-                       float lr, float b1, float b2, float eps, float c1, float c2) {
+                       int row, int ldb, float lr, float b1, float b2, float eps, float c1,
+                       float c2) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
         const float gi = g[i];
@@ -274,40 +424,53 @@ __global__ void k_adam(float *w, float *m, float *v, const float *g, __nv_bfloat
         v[i] = vi;
         const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
         w[i] = wi;
-        if (wb) wb[i] = __float2bfloat16_rn(wi);
+        if (wb) wb[(i / row) * ldb + i % row] = __float2bfloat16_rn(wi);
     }
 }
 
-__global__ void k_to_bf16(const float *w, __nv_bfloat16 *wb, size_t n) {
+__global__ void k_to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int row, int ldb) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)
-        wb[i] = __float2bfloat16_rn(w[i]);
+        wb[(i / row) * ldb + i % row] = __float2bfloat16_rn(w[i]);
 }
 
+constexpr int kMaxSmem = 1024 + 2 * kATile + 2 * 256 * 128 + 64;
+
 template <class Op>
-cudaError_t gemm(const Op &op, int M, int N, int K, int splits, cudaStream_t st) {
-    if (M < 1 || N < 1 || K < 1) return cudaErrorInvalidValue;
+cudaError_t umma_gemm(const Op &op, int rows, int K, int bn, int splits, int *flag,
+                      cudaStream_t st) {
+    if (rows < 1 || K < 1 || bn < 16 || bn > 256 || bn % 16 != 0 || !flag)
+        return cudaErrorInvalidValue;
     int kchunk = (K + splits - 1) / splits;
-    kchunk = (kchunk + BK - 1) / BK * BK;
+    kchunk = (kchunk + kTK - 1) / kTK * kTK;
     const int sp = (K + kchunk - 1) / kchunk;
-    const dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, sp);
-    if (grid.y > 65535u || grid.z > 65535u) return cudaErrorInvalidValue;
-    k_gemm<Op><<<grid, GT, 0, st>>>(op, M, N, K, kchunk);
+    const dim3 grid((unsigned)((rows + kTM - 1) / kTM), 1, (unsigned)sp);
+    if (grid.z > 65535u) return cudaErrorInvalidValue;
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        k_umma_gemm<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    if (attr != cudaSuccess) return attr;
+    const int smem = 1024 + 2 * kATile + 2 * bn * 128 + 64;
+    k_umma_gemm<Op><<<grid, kThreads, smem, st>>>(op, bn, kchunk, flag);
     return cudaGetLastError();
 }
 
 }  // namespace
 
+int padded_taps(int cin) { return (cin * 9 + kTK - 1) / kTK * kTK; }
+int padded_rows(int c) { return (c + 15) / 16 * 16; }
+
 cudaError_t conv3x3_forward(const float *in, int N, int Cin, int Hh, int Ww,
                             const __nv_bfloat16 *W, const float *bias, int Cout, float *out,
-                            cudaStream_t st) {
-    ConvFwd op{in, W, bias, out, Cin, Hh, Ww, Cout};
-    return gemm(op, N * Hh * Ww, Cout, Cin * 9, 1, st);
+                            int *flag, cudaStream_t st) {
+    if (Cout > 256) return cudaErrorInvalidValue;
+    ConvFwd op{in, W, padded_taps(Cin), bias, out, N, Cin, Hh, Ww, Cout};
+    return umma_gemm(op, N * Hh * Ww, Cin * 9, padded_rows(Cout), 1, flag, st);
 }
 
 cudaError_t conv3x3_flip(const __nv_bfloat16 *W, int Cout, int Cin, __nv_bfloat16 *Wt,
                          cudaStream_t st) {
-    k_flip<<<grid_1d((size_t)Cout * Cin * 9), 256, 0, st>>>(W, Cout, Cin, Wt);
+    k_flip<<<grid_1d((size_t)Cout * Cin * 9), 256, 0, st>>>(W, padded_taps(Cin), Cout, Cin, Wt,
+                                                           padded_taps(Cout));
     return cudaGetLastError();
 }
 
@@ -317,14 +480,15 @@ int conv3x3_weight_grad_splits(int N, int Hh, int Ww) {
 }
 
 cudaError_t conv3x3_weight_grad(const float *in, const float *dout, int N, int Cin, int Hh,
-                                int Ww, int Cout, float *dW, float *work, int splits,
+                                int Ww, int Cout, float *dW, float *work, int splits, int *flag,
                                 cudaStream_t st) {
+    if (Cout > 256) return cudaErrorInvalidValue;
     const int K = N * Hh * Ww;
     int kchunk = (K + splits - 1) / splits;
-    kchunk = (kchunk + BK - 1) / BK * BK;
+    kchunk = (kchunk + kTK - 1) / kTK * kTK;
     const int sp = (K + kchunk - 1) / kchunk;   // the splits the GEMM actually makes
-    ConvWgrad op{in, dout, work, Cin, Hh, Ww, Cout};
-    cudaError_t e = gemm(op, Cout, Cin * 9, K, splits, st);
+    ConvWgrad op{in, dout, work, N, Cin, Hh, Ww, Cout};
+    cudaError_t e = umma_gemm(op, Cin * 9, K, padded_rows(Cout), splits, flag, st);
     if (e != cudaSuccess) return e;
     const size_t n = (size_t)Cout * Cin * 9;
     k_sum_parts<<<grid_1d(n), 256, 0, st>>>(work, sp, n, dW);
@@ -381,15 +545,19 @@ cudaError_t mse(const float *y, const float *t, size_t n, float *dy, double *los
 }
 
 cudaError_t adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, size_t n,
-                 float lr, float b1, float b2, float eps, int t, cudaStream_t st) {
+                 int row, int ldb, float lr, float b1, float b2, float eps, int t,
+                 cudaStream_t st) {
+    if (row < 1 || ldb < row) return cudaErrorInvalidValue;
     const float c1 = (float)(1.0 - std::pow((double)b1, t));
     const float c2 = (float)(1.0 - std::pow((double)b2, t));
-    k_adam<<<grid_1d(n), 256, 0, st>>>(w, m, v, g, wb, n, lr, b1, b2, eps, c1, c2);
+    k_adam<<<grid_1d(n), 256, 0, st>>>(w, m, v, g, wb, n, row, ldb, lr, b1, b2, eps, c1, c2);
     return cudaGetLastError();
 }
 
-cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, cudaStream_t st) {
-    k_to_bf16<<<grid_1d(n), 256, 0, st>>>(w, wb, n);
+cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int row, int ldb,
+                    cudaStream_t st) {
+    if (row < 1 || ldb < row) return cudaErrorInvalidValue;
+    k_to_bf16<<<grid_1d(n), 256, 0, st>>>(w, wb, n, row, ldb);
     return cudaGetLastError();
 }
 

@@ -5,12 +5,17 @@
 // codes_v2/main_run_FPM.m:48).
 //
 // Kernels (cnn.cu): 3x3 convolutions (stride 1, zero padding 1) as implicit GEMMs on the
-// tensor cores (BF16 operands, FP32 accumulation, WMMA 16x16x16 tiles), their data and
-// weight gradients (the weight gradient split over the pixel axis into ordered partials),
-// bias gradients, ReLU, 2x2 average pooling, 2x nearest up-sampling, additions, the
-// mean-squared loss and an Adam step on FP32 master weights with BF16 copies.
-// Activations are FP32 in memory, NCHW; operands are rounded to BF16 as they are staged
-// into shared memory.
+// fifth-generation tensor cores (tcgen05: BF16 operands staged in shared memory, FP32
+// accumulators in tensor memory), their data and weight gradients (the weight gradient
+// split over the pixel axis into ordered partials), bias gradients, ReLU, 2x2 average
+// pooling, 2x nearest up-sampling, additions, the mean-squared loss and an Adam step on
+// FP32 master weights with BF16 copies.  Activations are FP32 in memory, NCHW; operands
+// are rounded to BF16 as they are staged into shared memory.
+//
+// BF16 weights are kept in padded rows: layer weights W[co][ci][ky][kx] of a convolution
+// with Cin inputs and Cout outputs as padded_rows(Cout) rows of padded_taps(Cin) values,
+// element (co, j) at co * padded_taps(Cin) + j, zero in every pad.  Every convolution takes
+// a device int *flag that a tensor-core wait which runs out sets to 1.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -21,19 +26,22 @@
 namespace fpm {
 namespace cnn {
 
+int padded_taps(int cin);   // 9 cin rounded up to 64
+int padded_rows(int c);     // c rounded up to 16
 // out[n][co][y][x] = bias[co] + sum_{ci,ky,kx} W[co][ci][ky][kx] in[n][ci][y+ky-1][x+kx-1]
-// (W as BF16 [co][ci][3][3]; bias may be null)
+// (W: BF16 padded rows; bias may be null; Cout <= 256)
 cudaError_t conv3x3_forward(const float *in, int N, int Cin, int Hh, int Ww,
                             const __nv_bfloat16 *W, const float *bias, int Cout, float *out,
-                            cudaStream_t st);
-// Wt[ci][co][2-ky][2-kx] = W[co][ci][ky][kx]: the data gradient is conv3x3_forward of the
-// output gradient with Wt
+                            int *flag, cudaStream_t st);
+// Wt[ci][co][2-ky][2-kx] = W[co][ci][ky][kx], both in padded rows (Wt: padded_rows(Cin)
+// rows of padded_taps(Cout), pads left as they are): the data gradient is
+// conv3x3_forward of the output gradient with Wt
 cudaError_t conv3x3_flip(const __nv_bfloat16 *W, int Cout, int Cin, __nv_bfloat16 *Wt,
                          cudaStream_t st);
 // dW[co][ci][ky][kx] = sum_{n,y,x} dout[n][co][y][x] in[n][ci][y+ky-1][x+kx-1], FP32;
 // work: splits * Cout * Cin * 9 floats of partials, summed in split order
 cudaError_t conv3x3_weight_grad(const float *in, const float *dout, int N, int Cin, int Hh,
-                                int Ww, int Cout, float *dW, float *work, int splits,
+                                int Ww, int Cout, float *dW, float *work, int splits, int *flag,
                                 cudaStream_t st);
 int conv3x3_weight_grad_splits(int N, int Hh, int Ww);
 // db[c] = sum_{n,p} dout[n][c][p] (ordered)
@@ -55,10 +63,13 @@ cudaError_t up_backward(const float *dout, int planes, int Hh, int Ww, float *di
 // loss = sum (y - t)^2 / n (FP64, ordered), dy = 2 (y - t) / n
 cudaError_t mse(const float *y, const float *t, size_t n, float *dy, double *loss,
                 double *work, cudaStream_t st);
-// Adam on FP32 master weights w (m, v moments), BF16 copy wb (may be null), step t >= 1
+// Adam on FP32 master weights w (m, v moments), BF16 copy wb (may be null) with element i
+// at (i / row) * ldb + i % row, step t >= 1
 cudaError_t adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, size_t n,
-                 float lr, float b1, float b2, float eps, int t, cudaStream_t st);
-cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, cudaStream_t st);
+                 int row, int ldb, float lr, float b1, float b2, float eps, int t,
+                 cudaStream_t st);
+cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int row, int ldb,
+                    cudaStream_t st);
 
 }  // namespace cnn
 }  // namespace fpm

@@ -51,6 +51,7 @@ struct Buf {
 struct Layer {
     int cin = 0, cout = 0;
     size_t w = 0, b = 0;   // offsets of the weights and biases in the parameter vector
+    size_t wb = 0, wf = 0; // offsets of the padded BF16 weights and of their flipped copy
 };
 
 #define CK(call)                                        \
@@ -66,8 +67,8 @@ struct fpm_cnn {
     cudaStream_t st = nullptr;
     int device = 0, in_ch = 0, base = 0;
     std::vector<Layer> L;
-    size_t n_params = 0, n_weights_bf16 = 0;
-    Buf w, g, m, v, wb, wflip, loss, mse_work, wg_work;
+    size_t n_params = 0, n_bf16 = 0, n_flip = 0;
+    Buf w, g, m, v, wb, wflip, loss, mse_work, wg_work, flag;
     int step = 0;
     // activations and gradients for the current (N, h)
     int cur_n = 0, cur_h = 0;
@@ -75,13 +76,10 @@ struct fpm_cnn {
     Buf ga, gb, gc, ge1, ge2, ge3, dy;
     std::string err;
 
-    size_t wb_off(int i) const {  // offset of layer i's BF16 weights
-        size_t o = 0;
-        for (int k = 0; k < i; ++k) o += (size_t)L[k].cout * L[k].cin * 9;
-        return o;
-    }
-    const __nv_bfloat16 *W(int i) const { return wb.as<__nv_bfloat16>() + wb_off(i); }
-    __nv_bfloat16 *Wf(int i) const { return wflip.as<__nv_bfloat16>() + wb_off(i); }
+    // BF16 weights of layer i in padded rows (cnn.h), and the flipped copy
+    __nv_bfloat16 *W(int i) const { return wb.as<__nv_bfloat16>() + L[i].wb; }
+    __nv_bfloat16 *Wf(int i) const { return wflip.as<__nv_bfloat16>() + L[i].wf; }
+    int *dflag() const { return flag.as<int>(); }
     const float *bias(int i) const { return w.as<float>() + L[i].b; }
     float *dW(int i) const { return g.as<float>() + L[i].w; }
     float *db(int i) const { return g.as<float>() + L[i].b; }
@@ -100,7 +98,7 @@ void build_layers(fpm_cnn *net) {
                            {2 * c, 4 * c},  {4 * c, 4 * c}, {4 * c, 8 * c}, {8 * c, 4 * c},
                            {4 * c, 4 * c},  {4 * c, 2 * c}, {2 * c, 2 * c}, {2 * c, c},
                            {c, c},          {c, 2}};
-    size_t off = 0, nb = 0;
+    size_t off = 0, nb = 0, nf = 0;
     for (auto &x : io) {
         Layer l;
         l.cin = x[0];
@@ -109,11 +107,15 @@ void build_layers(fpm_cnn *net) {
         off += (size_t)l.cout * l.cin * 9;
         l.b = off;
         off += l.cout;
-        nb += (size_t)l.cout * l.cin * 9;
+        l.wb = nb;
+        nb += (size_t)cnn::padded_rows(l.cout) * cnn::padded_taps(l.cin);
+        l.wf = nf;
+        nf += (size_t)cnn::padded_rows(l.cin) * cnn::padded_taps(l.cout);
         net->L.push_back(l);
     }
     net->n_params = off;
-    net->n_weights_bf16 = nb;
+    net->n_bf16 = nb;
+    net->n_flip = nf;
 }
 
 // the plane count and side of each activation slot for batch N at side h
@@ -157,7 +159,8 @@ float *A(fpm_cnn *net, int s) { return net->act[s].as<float>(); }
 
 cudaError_t conv(fpm_cnn *net, int i, const float *in, int N, int side, float *out, bool relu) {
     const Layer &l = net->L[i];
-    CK(cnn::conv3x3_forward(in, N, l.cin, side, side, net->W(i), net->bias(i), l.cout, out, net->st));
+    CK(cnn::conv3x3_forward(in, N, l.cin, side, side, net->W(i), net->bias(i), l.cout, out,
+                            net->dflag(), net->st));
     if (relu) CK(cnn::relu_forward(out, (size_t)N * l.cout * side * side, net->st));
     return cudaSuccess;
 }
@@ -200,11 +203,12 @@ cudaError_t conv_back(fpm_cnn *net, int i, const float *in, float *gout, int N, 
     cudaStream_t st = net->st;
     const int sp = cnn::conv3x3_weight_grad_splits(N, side, side);
     CK(cnn::conv3x3_weight_grad(in, gout, N, l.cin, side, side, l.cout, net->dW(i),
-                                net->wg_work.as<float>(), sp, st));
+                                net->wg_work.as<float>(), sp, net->dflag(), st));
     CK(cnn::bias_grad(gout, N, l.cout, side * side, net->db(i), st));
     if (gin) {
         CK(cnn::conv3x3_flip(net->W(i), l.cout, l.cin, net->Wf(i), st));
-        CK(cnn::conv3x3_forward(gout, N, l.cout, side, side, net->Wf(i), nullptr, l.cin, gin, st));
+        CK(cnn::conv3x3_forward(gout, N, l.cout, side, side, net->Wf(i), nullptr, l.cin, gin,
+                                net->dflag(), st));
     }
     return cudaSuccess;
 }
@@ -289,6 +293,21 @@ bool device_ptr(const void *p, int device) {
     return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device;
 }
 
+// waits for the network's stream and reports a tensor-core wait that ran out (the flag
+// is cleared for the next call)
+fpm_status sync_and_check(fpm_cnn *net, const char *what) {
+    int f = 0;
+    fpm_status rc = net_cuda(net, cudaMemcpyAsync(&f, net->flag.p, sizeof(int),
+                                                  cudaMemcpyDeviceToHost, net->st), what);
+    if (rc == FPM_OK) rc = net_cuda(net, cudaStreamSynchronize(net->st), what);
+    if (rc != FPM_OK) return rc;
+    if (f != 0) {
+        cudaMemsetAsync(net->flag.p, 0, sizeof(int), net->st);
+        return net_fail(net, FPM_ERR_INTERNAL, std::string(what) + ": a tensor-core wait ran out");
+    }
+    return FPM_OK;
+}
+
 fpm_status check_batch(fpm_cnn *net, int n, int h) {
     if (n < 1 || h < 8 || h % 8)
         return net_fail(net, FPM_ERR_INVALID_ARGUMENT,
@@ -304,7 +323,8 @@ fpm_status fpm_cnn_create(fpm_context *ctx, int32_t in_channels, int32_t base_ch
                           uint64_t seed, fpm_cnn **out) {
     if (!ctx || !out) return FPM_ERR_INVALID_ARGUMENT;
     *out = nullptr;
-    if (in_channels < 1 || in_channels > 1024 || base_channels < 8 || base_channels > 256 ||
+    // the bottom level's 8 base channels are one tensor-core N tile (at most 256)
+    if (in_channels < 1 || in_channels > 1024 || base_channels < 8 || base_channels > 32 ||
         base_channels % 8)
         return FPM_ERR_INVALID_ARGUMENT;
     fpm_cnn *net = new fpm_cnn();
@@ -320,8 +340,13 @@ fpm_status fpm_cnn_create(fpm_context *ctx, int32_t in_channels, int32_t base_ch
     Buf *bufs[] = {&net->w, &net->g, &net->m, &net->v};
     for (Buf *b : bufs)
         if (e == cudaSuccess) e = b->ensure(P * 4);
-    if (e == cudaSuccess) e = net->wb.ensure(net->n_weights_bf16 * 2);
-    if (e == cudaSuccess) e = net->wflip.ensure(net->n_weights_bf16 * 2);
+    if (e == cudaSuccess) e = net->wb.ensure(net->n_bf16 * 2);
+    if (e == cudaSuccess) e = net->wflip.ensure(net->n_flip * 2);
+    if (e == cudaSuccess) e = net->flag.ensure(16);
+    // the pads of the BF16 rows stay zero: only the weights themselves are written later
+    if (e == cudaSuccess) e = cudaMemsetAsync(net->wb.p, 0, net->n_bf16 * 2, net->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(net->wflip.p, 0, net->n_flip * 2, net->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(net->flag.p, 0, 16, net->st);
     if (e == cudaSuccess) e = net->loss.ensure(64);
     if (e == cudaSuccess) e = net->mse_work.ensure(256 * 8);
     if (e != cudaSuccess) {
@@ -368,9 +393,9 @@ fpm_status fpm_cnn_set_parameters(fpm_cnn *net, const float *params, int64_t n) 
     // BF16 copies of the weights, layer by layer
     for (size_t i = 0; i < net->L.size(); ++i) {
         const Layer &l = net->L[i];
-        rc = net_cuda(net, cnn::to_bf16(net->w.as<float>() + l.w,
-                                        net->wb.as<__nv_bfloat16>() + net->wb_off((int)i),
-                                        (size_t)l.cout * l.cin * 9, st),
+        rc = net_cuda(net, cnn::to_bf16(net->w.as<float>() + l.w, net->W((int)i),
+                                        (size_t)l.cout * l.cin * 9, l.cin * 9,
+                                        cnn::padded_taps(l.cin), st),
                       "weights");
         if (rc != FPM_OK) return rc;
     }
@@ -401,7 +426,7 @@ fpm_status fpm_cnn_forward(fpm_cnn *net, const float *x, int32_t n, int32_t h, f
     rc = net_cuda(net, cudaMemcpyAsync(y, A(net, Y), (size_t)n * 2 * h * h * 4,
                                        cudaMemcpyDeviceToDevice, net->st), "output");
     if (rc != FPM_OK) return rc;
-    return net_cuda(net, cudaStreamSynchronize(net->st), "forward");
+    return sync_and_check(net, "forward");
 }
 
 // loss and parameter gradients of one batch (no update); grads: host, n_params floats, or null
@@ -427,7 +452,7 @@ fpm_status fpm_cnn_gradients(fpm_cnn *net, const float *x, const float *t, int32
         rc = net_cuda(net, cudaMemcpyAsync(grads, net->g.p, net->n_params * 4,
                                            cudaMemcpyDeviceToHost, st), "gradients");
     if (rc != FPM_OK) return rc;
-    rc = net_cuda(net, cudaStreamSynchronize(st), "gradients");
+    rc = sync_and_check(net, "gradients");
     if (rc == FPM_OK && loss) *loss = l;
     return rc;
 }
@@ -444,12 +469,12 @@ fpm_status fpm_cnn_train_step(fpm_cnn *net, const float *x, const float *t, int3
         const size_t nw = (size_t)l.cout * l.cin * 9;
         float *w = net->w.as<float>(), *m = net->m.as<float>(), *v = net->v.as<float>();
         const float *g = net->g.as<float>();
-        cudaError_t e = cnn::adam(w + l.w, m + l.w, v + l.w, g + l.w,
-                                  net->wb.as<__nv_bfloat16>() + net->wb_off((int)i), nw, lr, 0.9f,
-                                  0.999f, 1e-8f, net->step, st);
+        cudaError_t e = cnn::adam(w + l.w, m + l.w, v + l.w, g + l.w, net->W((int)i), nw,
+                                  l.cin * 9, cnn::padded_taps(l.cin), lr, 0.9f, 0.999f, 1e-8f,
+                                  net->step, st);
         if (e == cudaSuccess)
-            e = cnn::adam(w + l.b, m + l.b, v + l.b, g + l.b, nullptr, (size_t)l.cout, lr, 0.9f,
-                          0.999f, 1e-8f, net->step, st);
+            e = cnn::adam(w + l.b, m + l.b, v + l.b, g + l.b, nullptr, (size_t)l.cout, l.cout,
+                          l.cout, lr, 0.9f, 0.999f, 1e-8f, net->step, st);
         rc = net_cuda(net, e, "adam");
         if (rc != FPM_OK) return rc;
     }
@@ -491,9 +516,10 @@ fpm_status fpm_cnn_initial_object(fpm_cnn *net, const fpm_problem *p, float *obj
     if (e == cudaSuccess)
         e = launch_bicubic_complex(A(net, Y), A(net, Y) + plane, h, p->pratio,
                                    reinterpret_cast<float2 *>(object), work.p, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     (void)H;
-    return net_cuda(net, e, "initial object");
+    fpm_status rc2 = net_cuda(net, e, "initial object");
+    if (rc2 != FPM_OK) return rc2;
+    return sync_and_check(net, "initial object");
 }
 
 }  // extern "C"
