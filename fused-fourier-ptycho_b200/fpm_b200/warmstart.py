@@ -111,15 +111,47 @@ class Network:
 # ---------------------------------------------------------------------------
 # problems, training pairs, evaluation
 # ---------------------------------------------------------------------------
-def make_problem_gpu(h: int, pratio: int, grid: int, seed: int, dev):
+def make_object_gpu(H: int, seed: int, dev, smooth_scale: float = 1.0):
+    """The object model of ``synth.make_object`` drawn on the GPU from a seeded torch
+    generator (other random values than numpy's for the same seed): amplitude = uniform
+    noise smoothed periodically with a Gaussian of sigma 3 smooth_scale pixels, rescaled to
+    [0.5, 1]; phase = normal noise smoothed with sigma 4 smooth_scale, rescaled to
+    [-pi/2, pi/2].  (H, H) complex64 in [c][r] order."""
+    import torch
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed))
+
+    def smooth(x, sigma):
+        f0 = torch.fft.fftfreq(H, device=dev)
+        f1 = torch.fft.rfftfreq(H, device=dev)
+        w0 = torch.exp(-2.0 * (np.pi * sigma) ** 2 * f0 * f0)
+        w1 = torch.exp(-2.0 * (np.pi * sigma) ** 2 * f1 * f1)
+        return torch.fft.irfft2(torch.fft.rfft2(x) * w0[:, None] * w1[None, :], s=(H, H))
+
+    def rescale(x, lo, hi):
+        mn, mx = x.min(), x.max()
+        return (x - mn) / torch.clamp(mx - mn, min=1e-30) * (hi - lo) + lo
+
+    amp = rescale(smooth(torch.rand((H, H), generator=g, device=dev), 3.0 * smooth_scale), 0.5, 1.0)
+    ph = rescale(smooth(torch.randn((H, H), generator=g, device=dev), 4.0 * smooth_scale),
+                 -np.pi / 2, np.pi / 2)
+    return torch.polar(amp, ph).to(torch.complex64)
+
+
+def make_problem_gpu(h: int, pratio: int, grid: int, seed: int, dev, smooth_scale=None):
     """A seeded problem on the GPU: the synthetic object model of ``synth`` (smooth random
-    amplitude in [0.5, 1] and phase in [-pi/2, pi/2]), the circular pupil with a seeded
-    aberration, frames of the forward model with Poisson noise at 3e4 peak counts (engine's
-    simulator), uint16 stack in column-major pages.  Returns tensors and the true object."""
+    amplitude in [0.5, 1] and phase in [-pi/2, pi/2]; drawn on the GPU by
+    ``make_object_gpu`` with that smoothing scale when smooth_scale is given), the circular
+    pupil with a seeded aberration, frames of the forward model with Poisson noise at 3e4
+    peak counts (engine's simulator), uint16 stack in column-major pages.  Returns tensors
+    and the true object."""
     import torch
     optics = synth.Optics(led_grid=grid)
     H = h * pratio
-    obj = torch.from_numpy(np.ascontiguousarray(synth.make_object(H, seed).T)).to(dev)   # [c][r]
+    if smooth_scale is None:
+        obj = torch.from_numpy(np.ascontiguousarray(synth.make_object(H, seed).T)).to(dev)   # [c][r]
+    else:
+        obj = make_object_gpu(H, seed, dev, smooth_scale)
     circ = synth.pupil_circle(h, optics)
     ptrue = circ * np.exp(1j * synth.pupil_aberration(h, optics, seed))
     Pt = torch.from_numpy(np.ascontiguousarray(ptrue.T.astype(np.complex64))).to(dev)
@@ -207,14 +239,16 @@ def solve_objects(eng: api.Engine, pbs, stacks, epochs: int, batch: int, lr: flo
 
 
 def training_pairs(eng: api.Engine, n: int, h: int, pratio: int, grid: int, epochs: int,
-                   batch: int, lr: float, seed0: int, in_channels: int = 25, chunk: int = 64):
+                   batch: int, lr: float, seed0: int, in_channels: int = 25, chunk: int = 64,
+                   smooth_scale=None):
     """(x, t): n inputs (the first in_channels amplitudes of each seeded problem) and targets
     (the low-pass of the plain method's object after `epochs` epochs), on the GPU."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     xs, ts = [], []
     for c0 in range(0, n, chunk):
-        pbs = [make_problem_gpu(h, pratio, grid, seed0 + i, dev) for i in range(c0, min(n, c0 + chunk))]
+        pbs = [make_problem_gpu(h, pratio, grid, seed0 + i, dev, smooth_scale)
+               for i in range(c0, min(n, c0 + chunk))]
         stacks = [simulate_stack(eng, pb, 7919 + pb["seed"]) for pb in pbs]
         objs, _ = solve_objects(eng, pbs, stacks, epochs, batch, lr)
         for pb, st, O in zip(pbs, stacks, objs):
@@ -243,17 +277,22 @@ def train(net: Network, x, t, epochs: int, batch_size: int, lr: float, seed: int
     return hist
 
 
-def evaluate(eng: api.Engine, net: Network, pbs, stacks, epochs: int, batch: int, lr: float):
+def evaluate(eng: api.Engine, net: Network, pbs, stacks, epochs: int, batch: int, lr: float,
+             refs=None):
     """Per-epoch error against the true object (global complex scale free) of the plain
     start and of the learned start (falling back to the plain start for a problem whose
     first-epoch loss the network's start raises), for every problem; k-epoch solves for
-    k = 1..epochs, each from its start."""
+    k = 1..epochs, each from its start.  With refs (one object per problem, e.g. the plain
+    method's converged result) the same distances to those are returned too:
+    (plain, learned, fallback) or (plain, learned, fallback, plain_ref, learned_ref)."""
     import torch
     dev = stacks[0].device
     inits = [net.initial_object(problem_struct(pb, st, 1, batch, lr), dev)
              for pb, st in zip(pbs, stacks)]
     plain = np.zeros((len(pbs), epochs + 1))
     learned = np.zeros((len(pbs), epochs + 1))
+    plain_r = np.zeros((len(pbs), epochs + 1))
+    learned_r = np.zeros((len(pbs), epochs + 1))
     # epoch 0: the starts themselves; first-epoch losses for the fallback rule
     plain0, lp = solve_objects(eng, pbs, stacks, 1, batch, lr)
     _, ll = solve_objects(eng, pbs, stacks, 1, batch, lr, inits)
@@ -263,6 +302,9 @@ def evaluate(eng: api.Engine, net: Network, pbs, stacks, epochs: int, batch: int
         T = pb["object_true"]
         plain[i, 0] = truth_error(starts0[i], T)
         learned[i, 0] = truth_error(starts0[i] if fallback[i] else inits[i], T)
+        if refs is not None:
+            plain_r[i, 0] = truth_error(starts0[i], refs[i])
+            learned_r[i, 0] = truth_error(starts0[i] if fallback[i] else inits[i], refs[i])
     chosen = [starts0[i] if fallback[i] else inits[i] for i in range(len(pbs))]
     for k in range(1, epochs + 1):
         op, _ = solve_objects(eng, pbs, stacks, k, batch, lr)
@@ -270,4 +312,10 @@ def evaluate(eng: api.Engine, net: Network, pbs, stacks, epochs: int, batch: int
         for i, pb in enumerate(pbs):
             plain[i, k] = truth_error(op[i], pb["object_true"])
             learned[i, k] = truth_error(ol[i], pb["object_true"])
+            if refs is not None:
+                plain_r[i, k] = truth_error(op[i], refs[i])
+                learned_r[i, k] = truth_error(ol[i], refs[i])
+        del op, ol
+    if refs is not None:
+        return plain, learned, fallback, plain_r, learned_r
     return plain, learned, fallback
