@@ -380,7 +380,8 @@ def run_ours(args, cfg: Cfg):
     # the autotuner's choice for this shape (one timed epoch per candidate), kept by the
     # context for every solve below
     t_tune = time.perf_counter()
-    tune_report = eng.autotune_raw(problem(1, api.MEM_DEVICE, *dev_args))
+    tune_report = ("skipped (--no-autotune): default launch choices" if args.no_autotune else
+                   eng.autotune_raw(problem(1, api.MEM_DEVICE, *dev_args)))
     t_tune = time.perf_counter() - t_tune
     # warm-up epochs
     eng._check(eng.solve_raw(problem(args.warmup, api.MEM_DEVICE, *dev_args), res))
@@ -1174,6 +1175,9 @@ def main():
     ap.add_argument("--grid", type=int, default=19)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch choices (profiler runs, whose timings would "
+                         "mislead the tuner)")
     ap.add_argument("--train-pairs", type=int, default=2000,
                     help="training pairs of the warm-start workload")
     ap.add_argument("--ws-small", action="store_true",

@@ -144,6 +144,7 @@ struct ConvFwd {
     const float *bias;
     float *out;
     int N, Cin, Hh, Ww, Cout;
+    int relu;   // ReLU of the output in the epilogue
     __device__ int kdim() const { return Cin * 9; }
     __device__ void build_a(uint8_t *tile, int m0, int k0) const {
         const int r = threadIdx.x, q = m0 + r;
@@ -196,7 +197,10 @@ struct ConvFwd {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int co = co0 + j;
-            if (co < Cout) o[(size_t)co * HW] = bias ? v[j] + bias[co] : v[j];
+            if (co < Cout) {
+                const float y = bias ? v[j] + bias[co] : v[j];
+                o[(size_t)co * HW] = relu ? fmaxf(y, 0.f) : y;
+            }
         }
     }
 };
@@ -300,26 +304,34 @@ __global__ void k_sum_parts(const float *part, int splits, size_t n, float *out)
 }
 
 // one block per channel, fixed order: thread-strided sums then a tree in shared memory
-__global__ void __launch_bounds__(256) k_bias_grad(const float *dout, int N, int C, int HW,
-                                                   float *db) {
+// db[c] = sum over n, p of dout[n][c][p], in a fixed order: block (c, s) sums the pixels
+// q = 256 s + t, + 256 S, ... of the N images (thread t), then a tree, into work[c S + s];
+// k_bias_grad_sum adds the S partials of a channel in order
+__global__ void __launch_bounds__(256) k_bias_grad_part(const float *dout, int N, int C, int HW,
+                                                        int S, float *work) {
     __shared__ float s[256];
-    const int c = blockIdx.x;
+    const int c = blockIdx.x, sp = blockIdx.y;
+    const size_t P = (size_t)N * HW;
     float acc = 0.f;
-    for (int n = 0; n < N; ++n)
-        for (int p = threadIdx.x; p < HW; p += 256) acc += dout[(size_t)(n * C + c) * HW + p];
+    for (size_t q = (size_t)sp * 256 + threadIdx.x; q < P; q += (size_t)S * 256) {
+        const size_t n = q / HW, p = q - n * HW;
+        acc += dout[(n * C + c) * HW + p];
+    }
     s[threadIdx.x] = acc;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
         if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) db[c] = s[0];
+    if (threadIdx.x == 0) work[(size_t)c * S + sp] = s[0];
 }
 
-__global__ void k_relu(float *x, size_t n) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (size_t)gridDim.x * blockDim.x)
-        x[i] = fmaxf(x[i], 0.f);
+__global__ void k_bias_grad_sum(const float *work, int C, int S, float *db) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    float acc = 0.f;
+    for (int i = 0; i < S; ++i) acc += work[(size_t)c * S + i];
+    db[c] = acc;
 }
 
 __global__ void k_relu_bwd(float *dy, const float *y, size_t n) {
@@ -461,9 +473,9 @@ int padded_rows(int c) { return (c + 15) / 16 * 16; }
 
 cudaError_t conv3x3_forward(const float *in, int N, int Cin, int Hh, int Ww,
                             const __nv_bfloat16 *W, const float *bias, int Cout, float *out,
-                            int *flag, cudaStream_t st) {
+                            bool relu, int *flag, cudaStream_t st) {
     if (Cout > 256) return cudaErrorInvalidValue;
-    ConvFwd op{in, W, padded_taps(Cin), bias, out, N, Cin, Hh, Ww, Cout};
+    ConvFwd op{in, W, padded_taps(Cin), bias, out, N, Cin, Hh, Ww, Cout, relu ? 1 : 0};
     return umma_gemm(op, N * Hh * Ww, Cin * 9, padded_rows(Cout), 1, flag, st);
 }
 
@@ -474,9 +486,14 @@ cudaError_t conv3x3_flip(const __nv_bfloat16 *W, int Cout, int Cin, __nv_bfloat1
     return cudaGetLastError();
 }
 
-int conv3x3_weight_grad_splits(int N, int Hh, int Ww) {
-    const int K = N * Hh * Ww;
-    return std::max(1, std::min(64, K / 2048));   // at least 2048 pixels per split
+int conv3x3_weight_grad_splits(int N, int Hh, int Ww, int Cin) {
+    // about four waves of 128-tap tiles x splits over the SMs, each split at least 8 stages
+    // of 64 pixels
+    const long long K = (long long)N * Hh * Ww;
+    const int mtiles = (Cin * 9 + kTM - 1) / kTM;
+    const long long want = (4LL * kB200SMs + mtiles - 1) / mtiles;
+    const long long most = std::max<long long>(1, K / (8 * kTK));
+    return (int)std::max<long long>(1, std::min<long long>({want, most, 1024}));
 }
 
 cudaError_t conv3x3_weight_grad(const float *in, const float *dout, int N, int Cin, int Hh,
@@ -495,13 +512,15 @@ cudaError_t conv3x3_weight_grad(const float *in, const float *dout, int N, int C
     return cudaGetLastError();
 }
 
-cudaError_t bias_grad(const float *dout, int N, int C, int HW, float *db, cudaStream_t st) {
-    k_bias_grad<<<C, 256, 0, st>>>(dout, N, C, HW, db);
-    return cudaGetLastError();
+int bias_grad_splits(int N, int HW) {
+    return (int)std::max<long long>(1, std::min<long long>(64, (long long)N * HW / 8192));
 }
 
-cudaError_t relu_forward(float *x, size_t n, cudaStream_t st) {
-    k_relu<<<grid_1d(n), 256, 0, st>>>(x, n);
+cudaError_t bias_grad(const float *dout, int N, int C, int HW, float *db, float *work,
+                      cudaStream_t st) {
+    const int S = bias_grad_splits(N, HW);
+    k_bias_grad_part<<<dim3((unsigned)C, (unsigned)S), 256, 0, st>>>(dout, N, C, HW, S, work);
+    k_bias_grad_sum<<<(C + 127) / 128, 128, 0, st>>>(work, C, S, db);
     return cudaGetLastError();
 }
 

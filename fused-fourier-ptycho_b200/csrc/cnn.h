@@ -29,10 +29,10 @@ namespace cnn {
 int padded_taps(int cin);   // 9 cin rounded up to 64
 int padded_rows(int c);     // c rounded up to 16
 // out[n][co][y][x] = bias[co] + sum_{ci,ky,kx} W[co][ci][ky][kx] in[n][ci][y+ky-1][x+kx-1]
-// (W: BF16 padded rows; bias may be null; Cout <= 256)
+// (W: BF16 padded rows; bias may be null; Cout <= 256), then max(out, 0) with relu
 cudaError_t conv3x3_forward(const float *in, int N, int Cin, int Hh, int Ww,
                             const __nv_bfloat16 *W, const float *bias, int Cout, float *out,
-                            int *flag, cudaStream_t st);
+                            bool relu, int *flag, cudaStream_t st);
 // Wt[ci][co][2-ky][2-kx] = W[co][ci][ky][kx], both in padded rows (Wt: padded_rows(Cin)
 // rows of padded_taps(Cout), pads left as they are): the data gradient is
 // conv3x3_forward of the output gradient with Wt
@@ -43,11 +43,14 @@ cudaError_t conv3x3_flip(const __nv_bfloat16 *W, int Cout, int Cin, __nv_bfloat1
 cudaError_t conv3x3_weight_grad(const float *in, const float *dout, int N, int Cin, int Hh,
                                 int Ww, int Cout, float *dW, float *work, int splits, int *flag,
                                 cudaStream_t st);
-int conv3x3_weight_grad_splits(int N, int Hh, int Ww);
-// db[c] = sum_{n,p} dout[n][c][p] (ordered)
-cudaError_t bias_grad(const float *dout, int N, int C, int HW, float *db, cudaStream_t st);
+// the split count conv3x3_weight_grad is meant to get (work holds that many partials)
+int conv3x3_weight_grad_splits(int N, int Hh, int Ww, int Cin);
+// db[c] = sum_{n,p} dout[n][c][p] (ordered: bias_grad_splits(N, HW) partials per channel in
+// work, C times that many floats)
+int bias_grad_splits(int N, int HW);
+cudaError_t bias_grad(const float *dout, int N, int C, int HW, float *db, float *work,
+                      cudaStream_t st);
 
-cudaError_t relu_forward(float *x, size_t n, cudaStream_t st);                     // in place
 // dx = dy where y > 0 else 0 (in place on dy)
 cudaError_t relu_backward(float *dy, const float *y, size_t n, cudaStream_t st);
 // out = a + b (out may alias a)

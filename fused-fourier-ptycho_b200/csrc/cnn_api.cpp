@@ -146,9 +146,10 @@ cudaError_t ensure_shape(fpm_cnn *net, int N, int h) {
     size_t wg = 0;
     for (int i = 0; i < 14; ++i) {
         const int side = i < 2 || i >= 11 ? h : (i < 4 || i >= 9 ? h / 2 : (i < 6 || i >= 7 ? h / 4 : h / 8));
-        const int sp = cnn::conv3x3_weight_grad_splits(N, side, side);
+        const int sp = cnn::conv3x3_weight_grad_splits(N, side, side, net->L[i].cin);
         wg = std::max(wg, (size_t)sp * net->L[i].cout * net->L[i].cin * 9);
     }
+    wg = std::max(wg, (size_t)8 * net->base * cnn::bias_grad_splits(N, h * h));
     CK(net->wg_work.ensure(wg * 4));
     net->cur_n = N;
     net->cur_h = h;
@@ -160,8 +161,7 @@ float *A(fpm_cnn *net, int s) { return net->act[s].as<float>(); }
 cudaError_t conv(fpm_cnn *net, int i, const float *in, int N, int side, float *out, bool relu) {
     const Layer &l = net->L[i];
     CK(cnn::conv3x3_forward(in, N, l.cin, side, side, net->W(i), net->bias(i), l.cout, out,
-                            net->dflag(), net->st));
-    if (relu) CK(cnn::relu_forward(out, (size_t)N * l.cout * side * side, net->st));
+                            relu, net->dflag(), net->st));
     return cudaSuccess;
 }
 
@@ -201,14 +201,15 @@ cudaError_t conv_back(fpm_cnn *net, int i, const float *in, float *gout, int N, 
                       float *gin) {
     const Layer &l = net->L[i];
     cudaStream_t st = net->st;
-    const int sp = cnn::conv3x3_weight_grad_splits(N, side, side);
+    const int sp = cnn::conv3x3_weight_grad_splits(N, side, side, l.cin);
     CK(cnn::conv3x3_weight_grad(in, gout, N, l.cin, side, side, l.cout, net->dW(i),
                                 net->wg_work.as<float>(), sp, net->dflag(), st));
-    CK(cnn::bias_grad(gout, N, l.cout, side * side, net->db(i), st));
+    // the weight gradient's partials are summed: its work buffer is free for these
+    CK(cnn::bias_grad(gout, N, l.cout, side * side, net->db(i), net->wg_work.as<float>(), st));
     if (gin) {
         CK(cnn::conv3x3_flip(net->W(i), l.cout, l.cin, net->Wf(i), st));
         CK(cnn::conv3x3_forward(gout, N, l.cout, side, side, net->Wf(i), nullptr, l.cin, gin,
-                                net->dflag(), st));
+                                false, net->dflag(), st));
     }
     return cudaSuccess;
 }
