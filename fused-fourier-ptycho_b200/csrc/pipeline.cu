@@ -685,142 +685,147 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, fft::LG<N, E>::MINB)
     for (int l = threadIdx.x; l < g.nb; l += G::THREADS) s_ab[l] = led_box_offset(led, l, g);
     setup<N, E>(smem, thi, tlo);
     const int ln = G::cline(), t = G::ct();
-    const int i = blockIdx.x * G::LPC + ln;     // box row of this line
-    const bool live = i < g.rspan;
     const int h = g.h;
-    float2 v[E];
-    if constexpr (OWNED) {
-        // Per covering LED, only its supported crop columns: they land on the contiguous
-        // (mod N) line positions e = pc_lo + ab.y + Cu0 + idx.  Thread t owns the positions
-        // e = t (mod T), accumulated in LED order in this line's exchange area, so no two
-        // threads touch one position and no barrier is needed until the transform.
-        float2 *acc = smem + ln * G::STRIDE;
+    // persistent: the CTA walks groups of LPC box rows (its set-up done once; a row's store
+    // drains while the next row's gathers are in flight)
+    for (int grp = blockIdx.x; grp * G::LPC < g.rspan; grp += gridDim.x) {
+        if (grp != (int)blockIdx.x) __syncthreads();   // the last transform's reads of the lines done
+        const int i = grp * G::LPC + ln;            // box row of this line
+        const bool live = i < g.rspan;
+        float2 v[E];
+        if constexpr (OWNED) {
+            // Per covering LED, only its supported crop columns: they land on the contiguous
+            // (mod N) line positions e = pc_lo + ab.y + Cu0 + idx.  Thread t owns the positions
+            // e = t (mod T), accumulated in LED order in this line's exchange area, so no two
+            // threads touch one position and no barrier is needed until the transform.
+            float2 *acc = smem + ln * G::STRIDE;
 #pragma unroll
-        for (int m = 0; m < E; ++m) acc[t + m * G::T] = make_float2(0.f, 0.f);
-        const int W = g.pc_hi - g.pc_lo;
-        // one covering LED's share of this line: its rows of Xs and Pt and the position
-        // of its first supported column; four of this thread's positions per pass
-        struct Src {
-            const float2 *x = nullptr, *p = nullptr;
-            int es = 0, base = 0x7fffffff;
-        };
-        auto src_of = [&](int l) {
-            Src q;
-            const int2 ab = s_ab[l];
-            int rr = i - ab.x;
-            if (rr < 0) rr += N;
-            if (rr < g.pr_lo || rr >= g.pr_hi) return q;   // pupil zero on that crop row
-            q.x = Xs + ((size_t)l * h + rr) * h + g.pc_lo;
-            q.p = Pt + (size_t)rr * h + g.pc_lo;
-            q.es = (int)(((long long)g.pc_lo + ab.y + g.Cu0) % N);   // position of idx 0
-            q.base = (t - q.es) & (G::T - 1);
-            return q;
-        };
-        auto load4 = [&](const Src &q, int base, float2 (&x)[4], float2 (&pp)[4]) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int idx = base + u * G::T;
-                x[u] = idx < W ? q.x[idx] : make_float2(0.f, 0.f);
-                pp[u] = idx < W ? q.p[idx] : make_float2(0.f, 0.f);
-            }
-        };
-        auto add4 = [&](const Src &q, int base, const float2 (&x)[4], const float2 (&pp)[4]) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int idx = base + u * G::T;
-                if (idx < W) {
-                    int e = q.es + idx;
-                    if (e >= N) e -= N;
-                    int j = e - g.Cu0;                  // box column
-                    if (j < 0) j += N;
-                    if (j < g.cspan) {
-                        const float2 pr = cmul(x[u], pp[u]);
-                        float2 a = acc[e];
-                        a.x += pr.x;
-                        a.y += pr.y;
-                        acc[e] = a;
-                    }
-                }
-            }
-        };
-        if (W <= 4 * G::T) {
-            // every LED in one pass: two covering LEDs' loads in flight together, each
-            // position still summed in LED order (four in flight measured no faster)
-            int l = 0;
-            while (live) {
-                Src qa, qb;
-                for (; l < g.nb && !(qa = src_of(l)).x; ++l) {}
-                if (l >= g.nb) break;
-                for (++l; l < g.nb && !(qb = src_of(l)).x; ++l) {}
-                ++l;
-                float2 xa[4], pa[4], xb[4], pb[4];
-                load4(qa, qa.base, xa, pa);
-                if (qb.x) load4(qb, qb.base, xb, pb);
-                add4(qa, qa.base, xa, pa);
-                if (qb.x) add4(qb, qb.base, xb, pb);
-                if (!qb.x) break;
-            }
-        } else {
-            for (int l = 0; live && l < g.nb; ++l) {
-                const Src q = src_of(l);
-                if (!q.x) continue;
-                for (int base = q.base; base < W; base += 4 * G::T) {
-                    float2 x[4], pp[4];
-                    load4(q, base, x, pp);
-                    add4(q, base, x, pp);
-                }
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < E; ++m) v[m] = acc[t + m * G::T];
-        __syncthreads();                        // every accumulator read before the exchanges
-    } else {
-    // four elements per LED sweep: four independent gathers in flight per thread
-#pragma unroll
-    for (int m0 = 0; m0 < E; m0 += 4) {
-        int jj[4];
-        bool any = false;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            int j = t + (m0 + k) * G::T - g.Cu0;     // box column of element e
-            if (j < 0) j += N;
-            jj[k] = (live && j < g.cspan) ? j : -1;
-            any |= jj[k] >= 0;
-        }
-        KahanC acc[4];
-        if (__any_sync(0xffffffffu, any)) {
-            for (int l = 0; l < g.nb; ++l) {
+            for (int m = 0; m < E; ++m) acc[t + m * G::T] = make_float2(0.f, 0.f);
+            const int W = g.pc_hi - g.pc_lo;
+            // one covering LED's share of this line: its rows of Xs and Pt and the position
+            // of its first supported column; four of this thread's positions per pass
+            struct Src {
+                const float2 *x = nullptr, *p = nullptr;
+                int es = 0, base = 0x7fffffff;
+            };
+            auto src_of = [&](int l) {
+                Src q;
                 const int2 ab = s_ab[l];
                 int rr = i - ab.x;
                 if (rr < 0) rr += N;
-                if (rr < g.pr_lo || rr >= g.pr_hi) continue;   // pupil zero on that crop row
-                const float2 *xrow = Xs + ((size_t)l * h + rr) * h;
-                const float2 *prow = Pt + (size_t)rr * h;
-                float2 x[4], pp[4];
-                bool in[4];
+                if (rr < g.pr_lo || rr >= g.pr_hi) return q;   // pupil zero on that crop row
+                q.x = Xs + ((size_t)l * h + rr) * h + g.pc_lo;
+                q.p = Pt + (size_t)rr * h + g.pc_lo;
+                q.es = (int)(((long long)g.pc_lo + ab.y + g.Cu0) % N);   // position of idx 0
+                q.base = (t - q.es) & (G::T - 1);
+                return q;
+            };
+            auto load4 = [&](const Src &q, int base, float2 (&x)[4], float2 (&pp)[4]) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    int c = jj[k] - ab.y;
-                    if (c < 0) c += N;
-                    in[k] = jj[k] >= 0 && c >= g.pc_lo && c < g.pc_hi;
-                    x[k] = in[k] ? xrow[c] : make_float2(0.f, 0.f);
-                    pp[k] = in[k] ? prow[c] : make_float2(0.f, 0.f);
+                for (int u = 0; u < 4; ++u) {
+                    const int idx = base + u * G::T;
+                    x[u] = idx < W ? q.x[idx] : make_float2(0.f, 0.f);
+                    pp[u] = idx < W ? q.p[idx] : make_float2(0.f, 0.f);
                 }
+            };
+            auto add4 = [&](const Src &q, int base, const float2 (&x)[4], const float2 (&pp)[4]) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if (in[k]) acc[k].add(cmul(x[k], pp[k]));
+                for (int u = 0; u < 4; ++u) {
+                    const int idx = base + u * G::T;
+                    if (idx < W) {
+                        int e = q.es + idx;
+                        if (e >= N) e -= N;
+                        int j = e - g.Cu0;                  // box column
+                        if (j < 0) j += N;
+                        if (j < g.cspan) {
+                            const float2 pr = cmul(x[u], pp[u]);
+                            float2 a = acc[e];
+                            a.x += pr.x;
+                            a.y += pr.y;
+                            acc[e] = a;
+                        }
+                    }
+                }
+            };
+            if (W <= 4 * G::T) {
+                // every LED in one pass: two covering LEDs' loads in flight together, each
+                // position still summed in LED order (four in flight measured no faster)
+                int l = 0;
+                while (live) {
+                    Src qa, qb;
+                    for (; l < g.nb && !(qa = src_of(l)).x; ++l) {}
+                    if (l >= g.nb) break;
+                    for (++l; l < g.nb && !(qb = src_of(l)).x; ++l) {}
+                    ++l;
+                    float2 xa[4], pa[4], xb[4], pb[4];
+                    load4(qa, qa.base, xa, pa);
+                    if (qb.x) load4(qb, qb.base, xb, pb);
+                    add4(qa, qa.base, xa, pa);
+                    if (qb.x) add4(qb, qb.base, xb, pb);
+                    if (!qb.x) break;
+                }
+            } else {
+                for (int l = 0; live && l < g.nb; ++l) {
+                    const Src q = src_of(l);
+                    if (!q.x) continue;
+                    for (int base = q.base; base < W; base += 4 * G::T) {
+                        float2 x[4], pp[4];
+                        load4(q, base, x, pp);
+                        add4(q, base, x, pp);
+                    }
                 }
             }
+#pragma unroll
+            for (int m = 0; m < E; ++m) v[m] = acc[t + m * G::T];
+            __syncthreads();                        // every accumulator read before the exchanges
+        } else {
+        // four elements per LED sweep: four independent gathers in flight per thread
+#pragma unroll
+        for (int m0 = 0; m0 < E; m0 += 4) {
+            int jj[4];
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                int j = t + (m0 + k) * G::T - g.Cu0;     // box column of element e
+                if (j < 0) j += N;
+                jj[k] = (live && j < g.cspan) ? j : -1;
+                any |= jj[k] >= 0;
+            }
+            KahanC acc[4];
+            if (__any_sync(0xffffffffu, any)) {
+                for (int l = 0; l < g.nb; ++l) {
+                    const int2 ab = s_ab[l];
+                    int rr = i - ab.x;
+                    if (rr < 0) rr += N;
+                    if (rr < g.pr_lo || rr >= g.pr_hi) continue;   // pupil zero on that crop row
+                    const float2 *xrow = Xs + ((size_t)l * h + rr) * h;
+                    const float2 *prow = Pt + (size_t)rr * h;
+                    float2 x[4], pp[4];
+                    bool in[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        int c = jj[k] - ab.y;
+                        if (c < 0) c += N;
+                        in[k] = jj[k] >= 0 && c >= g.pc_lo && c < g.pc_hi;
+                        x[k] = in[k] ? xrow[c] : make_float2(0.f, 0.f);
+                        pp[k] = in[k] ? prow[c] : make_float2(0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (in[k]) acc[k].add(cmul(x[k], pp[k]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[m0 + k] = acc[k].s;
         }
+        }
+        line_fft_e<N, +1, E>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
+        if (live) {
+            float2 *row = Ur + (size_t)i * N;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) v[m0 + k] = acc[k].s;
-    }
-    }
-    line_fft_e<N, +1, E>(v, smem + ln * G::STRIDE, G::tw_hi(smem), G::tw_hi(smem) + 128, t);
-    if (live) {
-        float2 *row = Ur + (size_t)i * N;
-#pragma unroll
-        for (int m = 0; m < E; ++m) row[t + m * G::T] = v[m];
+            for (int m = 0; m < E; ++m) row[t + m * G::T] = v[m];
+        }
     }
 }
 
@@ -1503,11 +1508,17 @@ static cudaError_t launch_rows_inv_e(const BatchGeom &g, const int2 *led, const 
                                      cudaStream_t st) {
     using G = fft::LG<N, E>;
     const int smem = G::SMEM + g.nb * (int)sizeof(int2);
-    const int blocks = (g.rspan + G::LPC - 1) / G::LPC;
+    const int groups = (g.rspan + G::LPC - 1) / G::LPC;
     auto kern = stitch_owned() ? k_big_rows_inv<N, E, true> : k_big_rows_inv<N, E, false>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
-    kern<<<blocks, G::THREADS, smem, st>>>(g, led, Pt, Xs, Ur, tw.hi_hi, tw.hi_lo);
+    int per_sm = 0, dev = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::THREADS, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int grid = std::max(1, std::min(groups, std::max(1, per_sm) * sms));
+    kern<<<grid, G::THREADS, smem, st>>>(g, led, Pt, Xs, Ur, tw.hi_hi, tw.hi_lo);
     return cudaGetLastError();
 }
 
