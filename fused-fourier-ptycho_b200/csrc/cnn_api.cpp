@@ -523,4 +523,49 @@ fpm_status fpm_cnn_initial_object(fpm_cnn *net, const fpm_problem *p, float *obj
     return sync_and_check(net, "initial object");
 }
 
+// The warm start with its fallback: the network's starting object and the plain one
+// (object_init, or the bicubic start when that is NULL) each get one epoch, and the solve
+// then runs from the start whose first-epoch loss is lower (the network's on a tie).
+fpm_status fpm_solve_warm(fpm_context *ctx, fpm_cnn *net, const fpm_problem *p, fpm_result *res,
+                          int32_t *used_network) {
+    if (!ctx || !net || !p || !res) return FPM_ERR_INVALID_ARGUMENT;
+    if (used_network) *used_network = 0;
+    cudaSetDevice(net->device);
+    if (p->memory != FPM_MEM_DEVICE)
+        return net_fail(net, FPM_ERR_UNSUPPORTED, "the warm start takes device-memory problems");
+    if (p->epochs < 1 || p->h < 1 || p->pratio < 1)
+        return net_fail(net, FPM_ERR_INVALID_ARGUMENT, "epochs, h and pratio must be positive");
+    const size_t H = (size_t)p->h * p->pratio, plane = (size_t)p->h * p->h;
+    Buf start, obj, pup, loss;
+    cudaError_t e = start.ensure(H * H * 8);
+    if (e == cudaSuccess) e = obj.ensure(H * H * 8);
+    if (e == cudaSuccess) e = pup.ensure(plane * 8);
+    if (e == cudaSuccess) e = loss.ensure(8);
+    fpm_status rc = net_cuda(net, e, "warm start buffers");
+    if (rc != FPM_OK) return rc;
+    rc = fpm_cnn_initial_object(net, p, start.as<float>());
+    if (rc != FPM_OK) return rc;
+    fpm_problem q = *p;
+    q.epochs = 1;
+    fpm_result t{obj.as<float>(), nullptr, pup.as<float>(), loss.as<double>()};
+    double first[2] = {0.0, 0.0};   // first-epoch loss: network start, plain start
+    const float *starts[2] = {start.as<float>(), p->object_init};
+    for (int k = 0; k < 2; ++k) {
+        q.object_init = starts[k];
+        rc = fpm_solve(ctx, &q, &t);
+        if (rc != FPM_OK) return net_fail(net, rc, "first epoch of a warm-start candidate");
+        rc = net_cuda(net, cudaMemcpyAsync(&first[k], loss.p, 8, cudaMemcpyDeviceToHost, net->st),
+                      "first-epoch loss");
+        if (rc == FPM_OK) rc = net_cuda(net, cudaStreamSynchronize(net->st), "first-epoch loss");
+        if (rc != FPM_OK) return rc;
+    }
+    const bool use = first[0] <= first[1];   // a NaN loss of the network start: plain start
+    q = *p;
+    q.object_init = use ? start.as<float>() : p->object_init;
+    rc = fpm_solve(ctx, &q, res);
+    if (rc != FPM_OK) return rc;
+    if (used_network) *used_network = use ? 1 : 0;
+    return FPM_OK;
+}
+
 }  // extern "C"

@@ -48,7 +48,7 @@ EXPORTED = ["fpm_create", "fpm_solve", "fpm_batch_gradients", "fpm_normalise_sta
             "fpm_selftest_bounded_wait", "fpm_cnn_create", "fpm_cnn_destroy",
             "fpm_cnn_parameter_count", "fpm_cnn_last_error", "fpm_cnn_set_parameters",
             "fpm_cnn_get_parameters", "fpm_cnn_forward", "fpm_cnn_gradients",
-            "fpm_cnn_train_step", "fpm_cnn_initial_object"]
+            "fpm_cnn_train_step", "fpm_cnn_initial_object", "fpm_solve_warm"]
 
 
 SIM_INTENSITY, SIM_AMPLITUDE = 0, 1
@@ -152,6 +152,9 @@ def load_library(path: str | Path | None = None):
     lib.fpm_cnn_train_step.restype = C.c_int
     lib.fpm_cnn_initial_object.argtypes = [vp, C.POINTER(Problem), vp]
     lib.fpm_cnn_initial_object.restype = C.c_int
+    lib.fpm_solve_warm.argtypes = [vp, vp, C.POINTER(Problem), C.POINTER(Result),
+                                   C.POINTER(C.c_int32)]
+    lib.fpm_solve_warm.restype = C.c_int
     lib.fpm_batch_gradients.argtypes = [C.c_void_p, C.POINTER(Problem), C.c_void_p, C.c_void_p,
                                         C.c_void_p]
     lib.fpm_batch_gradients.restype = C.c_int

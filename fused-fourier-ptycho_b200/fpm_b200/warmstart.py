@@ -108,6 +108,17 @@ class Network:
         return O
 
 
+    def solve(self, prob: api.Problem, res: api.Result) -> bool:
+        """fpm_solve_warm: the solve from the learned start, or from the plain start where
+        that one's first-epoch loss is lower; True when the network's start was used."""
+        import torch
+        used = C.c_int32(0)
+        torch.cuda.synchronize()
+        self._check(self.lib.fpm_solve_warm(self.eng._ctx, self._net, C.byref(prob),
+                                            C.byref(res), C.byref(used)))
+        return bool(used.value)
+
+
 # ---------------------------------------------------------------------------
 # problems, training pairs, evaluation
 # ---------------------------------------------------------------------------

@@ -397,6 +397,13 @@ fpm_status fpm_cnn_train_step(fpm_cnn *net, const float *x, const float *t, int3
 /* the starting object of a device-memory problem (complex H*H, column-major): the network
    on the problem's first in_channels frames, normalised as fpm_solve normalises them */
 fpm_status fpm_cnn_initial_object(fpm_cnn *net, const fpm_problem *prob, float *object);
+/* fpm_solve from the learned start with the plain start as the fallback: one epoch from
+   each of the network's object (fpm_cnn_initial_object) and the plain start (object_init,
+   or the bicubic start when NULL), then the full solve from the start whose first-epoch
+   loss is lower (the network's on a tie).  *used_network (may be NULL) tells which.
+   Device-memory problems; costs two extra epochs and one network evaluation. */
+fpm_status fpm_solve_warm(fpm_context *ctx, fpm_cnn *net, const fpm_problem *prob,
+                          fpm_result *res, int32_t *used_network);
 
 void fpm_destroy(fpm_context *ctx);
 

@@ -98,4 +98,36 @@ def test_learned_start_beats_the_plain_start(engine):
     print("plain", plain.mean(0), "learned", learned.mean(0), "fallback", fallback)
     assert learned[:, 0].mean() < plain[:, 0].mean()
     assert learned[:, 2].mean() <= plain[:, 2].mean() * 1.02
+    # the library's own fallback rule (fpm_solve_warm) picks what the first epochs chose
+    import fpm_b200
+    O = torch.empty((h * p, h * p), dtype=torch.complex64, device=dev)
+    used = net.solve(ws.problem_struct(pbs[0], stacks[0], 2, B, lr),
+                     fpm_b200.Result(object=O.data_ptr(), spectrum=None, pupil=None, loss=None))
+    assert used == (not fallback[0])
+    net.close()
+
+
+def test_warm_solve_falls_back_from_a_useless_network(engine):
+    """An all-zero network starts the reconstruction at zero, whose first epoch loses to
+    the plain start: fpm_solve_warm reports the fallback and returns the plain solve bit
+    for bit."""
+    import torch
+    import fpm_b200
+    from fpm_b200 import warmstart as ws
+    net = _net(engine, 9, 8, seed=3)
+    net.set_parameters(np.zeros(net.n_params, np.float32))
+    dev = torch.device("cuda", 0)
+    h, p = 32, 4
+    pb = ws.make_problem_gpu(h, p, 5, 6000, dev)
+    st = ws.simulate_stack(engine, pb, 9)
+    prob = ws.problem_struct(pb, st, 3, 5, 2e-3)
+    O1 = torch.empty((h * p, h * p), dtype=torch.complex64, device=dev)
+    O2 = torch.empty_like(O1)
+    used = net.solve(prob, fpm_b200.Result(object=O1.data_ptr(), spectrum=None, pupil=None,
+                                           loss=None))
+    assert not used
+    engine._check(engine.solve_raw(prob, fpm_b200.Result(object=O2.data_ptr(), spectrum=None,
+                                                         pupil=None, loss=None)))
+    torch.cuda.synchronize()
+    assert torch.equal(O1, O2)
     net.close()
