@@ -1,8 +1,8 @@
 """Parity of the kernels that run at the bench's size, against an FP64 checker.
 
 The bench reconstructs 2048² frames into a 16384² object; several kernels exist only
-in their 2048 / 16384 instantiations (the fused row pass with 2-CTA clusters and TMA
-tiles at h = 2048, the persistent low-resolution column pass, the 16384-point column
+in their 2048 / 16384 instantiations (the fused row pass with 4-CTA clusters, two CTAs
+per SM and TMA tiles at h = 2048, the persistent low-resolution column pass, the 16384-point column
 update and row passes with 32 values per thread and bulk-copy prefetch).  The numpy
 FP64 oracle takes minutes per update there, so the checker is its torch restatement
 (``oracle/torch_ref.py``, pinned on the CPU against the numpy oracle) run on the GPU in
@@ -140,6 +140,55 @@ def test_bench_size_gradients_vs_fp64(engine, full_case, loss):
     assert e_p < _bar(t_p), (e_p, t_p)
     assert abs(loss_e - r64[2]) < 1e-5 * abs(r64[2]), (loss_e, r64[2])
     del ref, dO, dP
+    torch.cuda.empty_cache()
+
+
+def test_row_pass_cluster_sizes_are_bit_identical(engine, full_case, monkeypatch):
+    """The fused row pass at h = 2048 in clusters of 2, 4 (default) and 8 CTAs: the same
+    lines get the same arithmetic whatever the cluster holds (only the halo lines and the
+    CTA count differ), so the gradients and the loss agree bit for bit."""
+    import torch
+    c = full_case
+    stack, ledt = _engine_args(c)
+    out = {}
+    for cl in ("2", "4", "8"):
+        monkeypatch.setenv("FPM_L23_CLUSTER", cl)
+        out[cl] = engine.batch_gradients(c["O0"], c["P_true"], stack, ledt, c["P0"], c["p"],
+                                         loss="anisotropic")
+    monkeypatch.delenv("FPM_L23_CLUSTER")
+    for cl in ("2", "8"):
+        assert torch.equal(out[cl][0], out["4"][0]), cl
+        assert torch.equal(out[cl][1], out["4"][1]), cl
+        assert out[cl][2] == out["4"][2], cl
+    del out
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("loss", ["isotropic", "anisotropic"])
+def test_h1024_gradients_vs_fp64(engine, loss):
+    """fpm_batch_gradients at 1024² -> 4096² (the fused row pass with 8 lines per CTA in
+    2-CTA clusters, two CTAs per SM), one batch of six LEDs with one crop past the
+    spectrum edge and an off-centre pupil support, against FP64 with the bars above."""
+    import torch
+    from oracle import torch_ref as tr
+    c = _case(1024, 4, 5, 5, seed=23, shift=(-70, 40))
+    H = c["H"]
+    stack, ledt = _engine_args(c)
+    dO, dP, loss_e = engine.batch_gradients(c["O0"], c["P_true"], stack, ledt, c["P0"], c["p"],
+                                            loss=loss)
+    ref = {}
+    for ct in (torch.complex128, torch.complex64):
+        S = torch.fft.fft2(c["O0"].to(ct))
+        G, dPr, lr_ = tr.batch_gradients(S, c["P_true"].to(ct), c["Y"], c["led"], c["p"], loss)
+        ref[ct] = (torch.fft.ifft2(G) * float(H * H), dPr, lr_)
+    r64, r32 = ref[torch.complex128], ref[torch.complex64]
+    e_o, e_p = tr.rel_err(dO, r64[0]), tr.rel_err(dP, r64[1])
+    t_o, t_p = tr.rel_err(r32[0], r64[0]), tr.rel_err(r32[1], r64[1])
+    print(f"{loss}: dO engine {e_o:.2e} twin {t_o:.2e}; dP engine {e_p:.2e} twin {t_p:.2e}")
+    assert e_o < _bar(t_o), (e_o, t_o)
+    assert e_p < _bar(t_p), (e_p, t_p)
+    assert abs(loss_e - r64[2]) < 1e-5 * abs(r64[2]), (loss_e, r64[2])
+    del ref, dO, dP, c
     torch.cuda.empty_cache()
 
 
