@@ -330,3 +330,37 @@ def evaluate(eng: api.Engine, net: Network, pbs, stacks, epochs: int, batch: int
     if refs is not None:
         return plain, learned, fallback, plain_r, learned_r
     return plain, learned, fallback
+
+
+def _time_training_steps(h: int, n: int, steps: int, in_channels: int = 25, base: int = 32):
+    """Milliseconds per Adam step of the network on seeded random (n, in_channels, h, h)
+    inputs and (n, 2, h, h) targets, after one warm-up step."""
+    import time
+    import torch
+    eng = api.Engine(0)
+    net = Network(eng, in_channels, base, seed=1)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    x = torch.rand((n, in_channels, h, h), device="cuda", generator=g)
+    t = 0.1 * torch.randn((n, 2, h, h), device="cuda", generator=g)
+    net.train_step(x, t, 1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        net.train_step(x, t, 1e-3)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / steps * 1e3
+    net.close()
+    eng.close()
+    return ms
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="time Adam steps of the warm-start network")
+    ap.add_argument("--h", type=int, default=256)
+    ap.add_argument("--n", type=int, default=32)
+    ap.add_argument("--steps", type=int, default=3)
+    a = ap.parse_args()
+    print(json.dumps({"h": a.h, "batch": a.n, "ms_per_step": round(_time_training_steps(a.h, a.n, a.steps), 3)}))
