@@ -53,7 +53,8 @@ __device__ __forceinline__ uint4 *chunk(uint8_t *tile, int r, int c) {
 // memory stages of kTK columns each while the MMAs of the other stage run (one thread
 // issues them, completion on one mbarrier per stage).  Op supplies
 //   kdim()                         the GEMM's K (its M is the host's `rows`)
-//   build_a(tile, m0, k0)          row threadIdx.x of A, K columns k0 .. k0 + 63
+//   build_a(tile, m0, k0, scratch) row threadIdx.x of A, K columns k0 .. k0 + 63 (called by
+//                                  every thread; scratch: kScratch floats of shared memory)
 //   build_b(tile, bn, k0)          all bn rows of B, the same K columns
 //   store(m, n0, v[16], split)     D(m, n0 .. n0 + 15) of K split `split`
 // Blocks: x = M tile, z = K split (kchunk columns, a multiple of kTK).  A wait that
@@ -67,6 +68,7 @@ __global__ void __launch_bounds__(kThreads) k_umma_gemm(Op op, int bn, int kchun
     uint8_t *sb[2] = {base + 2 * kATile, base + 2 * kATile + bn * 128};
     uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * kATile + 2 * bn * 128);
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 2);
+    float *scratch = reinterpret_cast<float *>(bar + 4);   // Op::kScratch floats (16-byte aligned)
     const int warp = threadIdx.x >> 5;
     const int m0 = blockIdx.x * kTM;
     const int K = op.kdim();
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(kThreads) k_umma_gemm(Op op, int bn, int kchun
             if (failed) break;
         }
         const int k0 = kb + t * kTK;
-        op.build_a(sa[s], m0, k0);
+        op.build_a(sa[s], m0, k0, scratch);
         op.build_b(sb[s], bn, k0);
         tma::fence_proxy_async();   // the stores above, visible to the tensor cores
         __syncthreads();
@@ -134,9 +136,9 @@ __global__ void __launch_bounds__(kThreads) k_umma_gemm(Op op, int bn, int kchun
     }
 }
 
-// Forward convolution: rows = pixels q = (n, y, x), K = taps j = (ci, ky, kx) in the
-// order of W[co][ci][ky][kx]; B = the BF16 weights, rows co (ldw >= 9 Cin per row, zero
-// beyond 9 Cin, zero rows up to the padded bn); out[n][co][y][x] = bias[co] + D.
+// Forward convolution: rows = pixels q = (n, y, x), K = taps k = tap Cin + ci (tap = 3 ky +
+// kx); B = the BF16 weights in that order, rows co (ldw >= 9 Cin per row, zero beyond
+// 9 Cin, zero rows up to the padded bn); out[n][co][y][x] = bias[co] + D.
 struct ConvFwd {
     const float *in;
     const __nv_bfloat16 *W;
@@ -145,10 +147,11 @@ struct ConvFwd {
     float *out;
     int N, Cin, Hh, Ww, Cout;
     int relu;   // ReLU of the output in the epilogue
+    static constexpr int kScratch = 0;
     __device__ int kdim() const { return Cin * 9; }
-    __device__ void build_a(uint8_t *tile, int m0, int k0) const {
+    __device__ void build_a(uint8_t *tile, int m0, int k0, float *) const {
         const int r = threadIdx.x, q = m0 + r;
-        const int HW = Hh * Ww, K = Cin * 9;
+        const int HW = Hh * Ww;
         const bool live = q < N * HW;
         int n = 0, y = 0, x = 0;
         if (live) {
@@ -158,29 +161,42 @@ struct ConvFwd {
             x = p - y * Ww;
         }
         const float *src = in + (size_t)n * Cin * HW;
-        int ci = k0 / 9, t = k0 - ci * 9;
+        // K = tap Cin + ci: the tap's offset and bounds hold over a run of channels.  Per
+        // group of 16 values the offsets and a validity mask come first (the bookkeeping's
+        // branches depend on no load), then the 16 loads go out together.
+        int tap = k0 / Cin, ci = k0 - tap * Cin;
+        int off = 0;
+        bool ok = false;
+        auto enter_tap = [&]() {
+            const int ky = tap / 3, yy = y + ky - 1, xx = x + (tap - 3 * ky) - 1;
+            ok = live && tap < 9 && yy >= 0 && yy < Hh && xx >= 0 && xx < Ww;
+            off = ci * HW + yy * Ww + xx;
+        };
+        enter_tap();
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            uint32_t w[4];
+        for (int g = 0; g < 4; ++g) {
+            int o[16];
+            unsigned mask = 0;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                float v2[2];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int k = k0 + c * 8 + e * 2 + h;
-                    const int ky = t / 3, yy = y + ky - 1, xx = x + (t - 3 * ky) - 1;
-                    float a = 0.f;
-                    if (live && k < K && yy >= 0 && yy < Hh && xx >= 0 && xx < Ww)
-                        a = src[(size_t)ci * HW + yy * Ww + xx];
-                    v2[h] = a;
-                    if (++t == 9) {
-                        t = 0;
-                        ++ci;
-                    }
+            for (int j = 0; j < 16; ++j) {
+                o[j] = off;
+                mask |= ok ? 1u << j : 0u;
+                off += HW;
+                if (++ci == Cin) {
+                    ci = 0;
+                    ++tap;
+                    enter_tap();
                 }
-                w[e] = pack_bf16(v2[0], v2[1]);
             }
-            *chunk(tile, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = mask >> j & 1u ? src[o[j]] : 0.f;
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc)
+                *chunk(tile, r, 2 * g + cc) =
+                    make_uint4(pack_bf16(v[8 * cc], v[8 * cc + 1]), pack_bf16(v[8 * cc + 2], v[8 * cc + 3]),
+                               pack_bf16(v[8 * cc + 4], v[8 * cc + 5]),
+                               pack_bf16(v[8 * cc + 6], v[8 * cc + 7]));
         }
     }
     __device__ void build_b(uint8_t *tile, int nrows, int k0) const {
@@ -205,69 +221,101 @@ struct ConvFwd {
     }
 };
 
-// Weight gradient, transposed: rows = taps k = (ci, ky, kx), K = pixels q; A = im2col(in)^T,
-// B = dout (rows co, zero rows up to bn); D(k, co) = dW[co][k] of the split's pixels,
-// into part[split][co][k].
+// Weight gradient, transposed: rows = taps k = ci 9 + tap (the order of W[co][ci][ky][kx]),
+// K = pixels q; A = im2col(in)^T, B = dout (rows co, zero rows up to bn); D(k, co) =
+// dW[co][k] of the split's pixels, into part[split][co][k].
 struct ConvWgrad {
     const float *in, *dout;
     float *part;
     int N, Cin, Hh, Ww, Cout;
+    static constexpr int kScratch = 0;
     __device__ int kdim() const { return N * Hh * Ww; }
-    __device__ void build_a(uint8_t *tile, int m0, int q0) const {
+    __device__ void build_a(uint8_t *tile, int m0, int q0, float *) const {
         const int r = threadIdx.x, k = m0 + r;
         const int HW = Hh * Ww, Q = N * HW;
         const bool live = k < Cin * 9;
-        const int ci = live ? k / 9 : 0, t = k - ci * 9;
-        const int ky = t / 3, dy = ky - 1, dx = t - 3 * ky - 1;
+        const int ci = live ? k / 9 : 0, t = k - ci * 9;       // k = ci 9 + tap: a warp's rows
+        const int ky = t / 3, dy = ky - 1, dx = t - 3 * ky - 1;  // read nearby pixels
         int n = q0 / HW, p = q0 - n * HW;
         int y = p / Ww, x = p - y * Ww;
+        const bool full = q0 + kTK <= Q;                       // no pixel past the end
+        int q = q0;
+        // offset of the current image's plane of channel ci, and row y + dy of it (pixel x
+        // of the run at rowo + x); both change only when the run wraps to the next row.
+        // Per group of 16 values the offsets and a validity mask come first, then the loads.
+        int plane = (n * Cin + ci) * HW, rowo = 0;
+        bool rowok = false;
+        auto enter_row = [&]() {
+            const int yy = y + dy;
+            rowok = live && yy >= 0 && yy < Hh;
+            rowo = plane + yy * Ww + dx;
+        };
+        enter_row();
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            uint32_t w[4];
+        for (int g = 0; g < 4; ++g) {
+            int o[16];
+            unsigned mask = 0;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                float v2[2];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int q = q0 + c * 8 + e * 2 + h;
-                    const int yy = y + dy, xx = x + dx;
-                    float a = 0.f;
-                    if (live && q < Q && yy >= 0 && yy < Hh && xx >= 0 && xx < Ww)
-                        a = in[((size_t)(n * Cin + ci) * Hh + yy) * Ww + xx];
-                    v2[h] = a;
-                    if (++x == Ww) {
-                        x = 0;
-                        if (++y == Hh) {
-                            y = 0;
-                            ++n;
-                        }
+            for (int j = 0; j < 16; ++j) {
+                o[j] = rowo + x;
+                const bool in_x = (unsigned)(x + dx) < (unsigned)Ww;
+                mask |= rowok && in_x && (full || q < Q) ? 1u << j : 0u;
+                ++q;
+                if (++x == Ww) {
+                    x = 0;
+                    if (++y == Hh) {
+                        y = 0;
+                        plane += Cin * HW;                     // next image
                     }
+                    enter_row();
                 }
-                w[e] = pack_bf16(v2[0], v2[1]);
             }
-            *chunk(tile, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = mask >> j & 1u ? in[o[j]] : 0.f;
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc)
+                *chunk(tile, r, 2 * g + cc) =
+                    make_uint4(pack_bf16(v[8 * cc], v[8 * cc + 1]), pack_bf16(v[8 * cc + 2], v[8 * cc + 3]),
+                               pack_bf16(v[8 * cc + 4], v[8 * cc + 5]),
+                               pack_bf16(v[8 * cc + 6], v[8 * cc + 7]));
         }
     }
     __device__ void build_b(uint8_t *tile, int nrows, int q0) const {
         const int HW = Hh * Ww, Q = N * HW;
+        const bool vec = (HW & 7) == 0;   // a chunk of 8 pixels lies in one image, 32-byte aligned
         for (int i = threadIdx.x; i < nrows * 8; i += kThreads) {
             const int r = i >> 3, c = i & 7;   // row co, pixels q0 + 8 c .. + 7
             int q = q0 + c * 8;
             int n = q / HW, p = q - n * HW;
             uint32_t w[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                float v2[2];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    v2[h] = r < Cout && q < Q ? dout[((size_t)n * Cout + r) * HW + p] : 0.f;
-                    ++q;
-                    if (++p == HW) {
-                        p = 0;
-                        ++n;
-                    }
+            if (vec) {
+                float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+                if (r < Cout && q < Q) {
+                    const float4 *src =
+                        reinterpret_cast<const float4 *>(dout + ((size_t)n * Cout + r) * HW + p);
+                    lo = src[0];
+                    hi = src[1];
                 }
-                w[e] = pack_bf16(v2[0], v2[1]);
+                w[0] = pack_bf16(lo.x, lo.y);
+                w[1] = pack_bf16(lo.z, lo.w);
+                w[2] = pack_bf16(hi.x, hi.y);
+                w[3] = pack_bf16(hi.z, hi.w);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    float v2[2];
+#pragma unroll
+                    for (int hh = 0; hh < 2; ++hh) {
+                        v2[hh] = r < Cout && q < Q ? dout[((size_t)n * Cout + r) * HW + p] : 0.f;
+                        ++q;
+                        if (++p == HW) {
+                            p = 0;
+                            ++n;
+                        }
+                    }
+                    w[e] = pack_bf16(v2[0], v2[1]);
+                }
             }
             *chunk(tile, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
         }
@@ -283,14 +331,15 @@ struct ConvWgrad {
     }
 };
 
-// Wt[ci][co*9 + 8 - t] = W[co][ci*9 + t] (rows of ldw and ldt values, pads untouched)
+// Wt[ci][(8 - t) Cout + co] = W[co][t Cin + ci] (tap-major rows of ldw and ldt values, pads
+// untouched): the transposed convolution's weights, (ky, kx) -> (2-ky, 2-kx)
 __global__ void k_flip(const __nv_bfloat16 *W, int ldw, int Cout, int Cin, __nv_bfloat16 *Wt,
                        int ldt) {
     const int total = Cout * Cin * 9;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const int co = i / (Cin * 9), rem = i - co * Cin * 9;
-        const int ci = rem / 9, t = rem - ci * 9;
-        Wt[(size_t)ci * ldt + co * 9 + (8 - t)] = W[(size_t)co * ldw + rem];   // (ky, kx) -> (2-ky, 2-kx)
+        const int t = rem / Cin, ci = rem - t * Cin;
+        Wt[(size_t)ci * ldt + (8 - t) * Cout + co] = W[(size_t)co * ldw + rem];
     }
 }
 
@@ -422,10 +471,16 @@ __global__ void k_mse_final(const double *work, int nb, size_t n, double *loss) 
     }
 }
 
-// Adam on n FP32 weights; the BF16 copy (if any) of element i goes to
-// wb[(i / row) * ldb + i % row] (rows of `row` values padded to ldb)
+// position in the padded tap-major BF16 rows of FP32 weight i = co 9 Cin + ci 9 + t
+__device__ __forceinline__ size_t bf16_slot(size_t i, int cin, int ldb) {
+    const size_t K = (size_t)cin * 9, co = i / K;
+    const int rem = (int)(i - co * K), ci = rem / 9, t = rem - ci * 9;
+    return co * ldb + (size_t)t * cin + ci;
+}
+
+// Adam on n FP32 weights; the BF16 copy (if any) of weight i goes to bf16_slot(i)
 __global__ void k_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, size_t n,
-                       int row, int ldb, float lr, float b1, float b2, float eps, float c1,
+                       int cin, int ldb, float lr, float b1, float b2, float eps, float c1,
                        float c2) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
@@ -436,17 +491,18 @@ __global__ void k_adam(float *w, float *m, float *v, const float *g, __nv_bfloat
         v[i] = vi;
         const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
         w[i] = wi;
-        if (wb) wb[(i / row) * ldb + i % row] = __float2bfloat16_rn(wi);
+        if (wb) wb[bf16_slot(i, cin, ldb)] = __float2bfloat16_rn(wi);
     }
 }
 
-__global__ void k_to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int row, int ldb) {
+__global__ void k_to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int cin, int ldb) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)
-        wb[(i / row) * ldb + i % row] = __float2bfloat16_rn(w[i]);
+        wb[bf16_slot(i, cin, ldb)] = __float2bfloat16_rn(w[i]);
 }
 
-constexpr int kMaxSmem = 1024 + 2 * kATile + 2 * 256 * 128 + 64;
+constexpr int kMaxScratch = 0;   // the largest Op::kScratch (floats)
+constexpr int kMaxSmem = 1024 + 2 * kATile + 2 * 256 * 128 + 32 + 4 * kMaxScratch;
 
 template <class Op>
 cudaError_t umma_gemm(const Op &op, int rows, int K, int bn, int splits, int *flag,
@@ -461,7 +517,8 @@ cudaError_t umma_gemm(const Op &op, int rows, int K, int bn, int splits, int *fl
     static const cudaError_t attr = cudaFuncSetAttribute(
         k_umma_gemm<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
     if (attr != cudaSuccess) return attr;
-    const int smem = 1024 + 2 * kATile + 2 * bn * 128 + 64;
+    static_assert(Op::kScratch <= kMaxScratch, "scratch fits the attribute");
+    const int smem = 1024 + 2 * kATile + 2 * bn * 128 + 32 + 4 * Op::kScratch;
     k_umma_gemm<Op><<<grid, kThreads, smem, st>>>(op, bn, kchunk, flag);
     return cudaGetLastError();
 }
@@ -474,7 +531,8 @@ int padded_rows(int c) { return (c + 15) / 16 * 16; }
 cudaError_t conv3x3_forward(const float *in, int N, int Cin, int Hh, int Ww,
                             const __nv_bfloat16 *W, const float *bias, int Cout, float *out,
                             bool relu, int *flag, cudaStream_t st) {
-    if (Cout > 256) return cudaErrorInvalidValue;
+    // the operand staging addresses an image's channels with 32-bit offsets
+    if (Cout > 256 || (long long)Cin * Hh * Ww >= (1LL << 31)) return cudaErrorInvalidValue;
     ConvFwd op{in, W, padded_taps(Cin), bias, out, N, Cin, Hh, Ww, Cout, relu ? 1 : 0};
     return umma_gemm(op, N * Hh * Ww, Cin * 9, padded_rows(Cout), 1, flag, st);
 }
@@ -499,7 +557,8 @@ int conv3x3_weight_grad_splits(int N, int Hh, int Ww, int Cin) {
 cudaError_t conv3x3_weight_grad(const float *in, const float *dout, int N, int Cin, int Hh,
                                 int Ww, int Cout, float *dW, float *work, int splits, int *flag,
                                 cudaStream_t st) {
-    if (Cout > 256) return cudaErrorInvalidValue;
+    // the operand staging addresses the whole input with 32-bit offsets
+    if (Cout > 256 || (long long)N * Cin * Hh * Ww >= (1LL << 31)) return cudaErrorInvalidValue;
     const int K = N * Hh * Ww;
     int kchunk = (K + splits - 1) / splits;
     kchunk = (kchunk + kTK - 1) / kTK * kTK;
@@ -564,19 +623,19 @@ cudaError_t mse(const float *y, const float *t, size_t n, float *dy, double *los
 }
 
 cudaError_t adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, size_t n,
-                 int row, int ldb, float lr, float b1, float b2, float eps, int t,
+                 int cin, int ldb, float lr, float b1, float b2, float eps, int t,
                  cudaStream_t st) {
-    if (row < 1 || ldb < row) return cudaErrorInvalidValue;
+    if (wb && (cin < 1 || ldb < 9 * cin)) return cudaErrorInvalidValue;
     const float c1 = (float)(1.0 - std::pow((double)b1, t));
     const float c2 = (float)(1.0 - std::pow((double)b2, t));
-    k_adam<<<grid_1d(n), 256, 0, st>>>(w, m, v, g, wb, n, row, ldb, lr, b1, b2, eps, c1, c2);
+    k_adam<<<grid_1d(n), 256, 0, st>>>(w, m, v, g, wb, n, cin, ldb, lr, b1, b2, eps, c1, c2);
     return cudaGetLastError();
 }
 
-cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int row, int ldb,
+cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int cin, int ldb,
                     cudaStream_t st) {
-    if (row < 1 || ldb < row) return cudaErrorInvalidValue;
-    k_to_bf16<<<grid_1d(n), 256, 0, st>>>(w, wb, n, row, ldb);
+    if (cin < 1 || ldb < 9 * cin) return cudaErrorInvalidValue;
+    k_to_bf16<<<grid_1d(n), 256, 0, st>>>(w, wb, n, cin, ldb);
     return cudaGetLastError();
 }
 

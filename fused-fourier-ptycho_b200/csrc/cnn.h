@@ -12,9 +12,10 @@
 // FP32 master weights with BF16 copies.  Activations are FP32 in memory, NCHW; operands
 // are rounded to BF16 as they are staged into shared memory.
 //
-// BF16 weights are kept in padded rows: layer weights W[co][ci][ky][kx] of a convolution
-// with Cin inputs and Cout outputs as padded_rows(Cout) rows of padded_taps(Cin) values,
-// element (co, j) at co * padded_taps(Cin) + j, zero in every pad.  Every convolution takes
+// BF16 weights are kept in padded tap-major rows: layer weights W[co][ci][ky][kx] of a
+// convolution with Cin inputs and Cout outputs as padded_rows(Cout) rows of
+// padded_taps(Cin) values, W[co][ci][ky][kx] at co * padded_taps(Cin) + (3 ky + kx) Cin + ci,
+// zero in every pad.  Every convolution takes
 // a device int *flag that a tensor-core wait which runs out sets to 1.
 #pragma once
 
@@ -33,8 +34,8 @@ int padded_rows(int c);     // c rounded up to 16
 cudaError_t conv3x3_forward(const float *in, int N, int Cin, int Hh, int Ww,
                             const __nv_bfloat16 *W, const float *bias, int Cout, float *out,
                             bool relu, int *flag, cudaStream_t st);
-// Wt[ci][co][2-ky][2-kx] = W[co][ci][ky][kx], both in padded rows (Wt: padded_rows(Cin)
-// rows of padded_taps(Cout), pads left as they are): the data gradient is
+// Wt[ci][co][2-ky][2-kx] = W[co][ci][ky][kx], both in padded tap-major rows (Wt:
+// padded_rows(Cin) rows of padded_taps(Cout), pads left as they are): the data gradient is
 // conv3x3_forward of the output gradient with Wt
 cudaError_t conv3x3_flip(const __nv_bfloat16 *W, int Cout, int Cin, __nv_bfloat16 *Wt,
                          cudaStream_t st);
@@ -66,12 +67,12 @@ cudaError_t up_backward(const float *dout, int planes, int Hh, int Ww, float *di
 // loss = sum (y - t)^2 / n (FP64, ordered), dy = 2 (y - t) / n
 cudaError_t mse(const float *y, const float *t, size_t n, float *dy, double *loss,
                 double *work, cudaStream_t st);
-// Adam on FP32 master weights w (m, v moments), BF16 copy wb (may be null) with element i
-// at (i / row) * ldb + i % row, step t >= 1
+// Adam on FP32 master weights w (m, v moments) of a convolution with cin inputs, their BF16
+// copy wb (may be null) in padded tap-major rows of ldb, step t >= 1
 cudaError_t adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *wb, size_t n,
-                 int row, int ldb, float lr, float b1, float b2, float eps, int t,
+                 int cin, int ldb, float lr, float b1, float b2, float eps, int t,
                  cudaStream_t st);
-cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int row, int ldb,
+cudaError_t to_bf16(const float *w, __nv_bfloat16 *wb, size_t n, int cin, int ldb,
                     cudaStream_t st);
 
 }  // namespace cnn

@@ -395,7 +395,7 @@ fpm_status fpm_cnn_set_parameters(fpm_cnn *net, const float *params, int64_t n) 
     for (size_t i = 0; i < net->L.size(); ++i) {
         const Layer &l = net->L[i];
         rc = net_cuda(net, cnn::to_bf16(net->w.as<float>() + l.w, net->W((int)i),
-                                        (size_t)l.cout * l.cin * 9, l.cin * 9,
+                                        (size_t)l.cout * l.cin * 9, l.cin,
                                         cnn::padded_taps(l.cin), st),
                       "weights");
         if (rc != FPM_OK) return rc;
@@ -471,11 +471,11 @@ fpm_status fpm_cnn_train_step(fpm_cnn *net, const float *x, const float *t, int3
         float *w = net->w.as<float>(), *m = net->m.as<float>(), *v = net->v.as<float>();
         const float *g = net->g.as<float>();
         cudaError_t e = cnn::adam(w + l.w, m + l.w, v + l.w, g + l.w, net->W((int)i), nw,
-                                  l.cin * 9, cnn::padded_taps(l.cin), lr, 0.9f, 0.999f, 1e-8f,
+                                  l.cin, cnn::padded_taps(l.cin), lr, 0.9f, 0.999f, 1e-8f,
                                   net->step, st);
         if (e == cudaSuccess)
-            e = cnn::adam(w + l.b, m + l.b, v + l.b, g + l.b, nullptr, (size_t)l.cout, l.cout,
-                          l.cout, lr, 0.9f, 0.999f, 1e-8f, net->step, st);
+            e = cnn::adam(w + l.b, m + l.b, v + l.b, g + l.b, nullptr, (size_t)l.cout, 0, 0, lr,
+                          0.9f, 0.999f, 1e-8f, net->step, st);
         rc = net_cuda(net, e, "adam");
         if (rc != FPM_OK) return rc;
     }
