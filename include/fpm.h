@@ -363,8 +363,8 @@ typedef struct fpm_optimizer {
 fpm_status fpm_optimizer_step(fpm_context *ctx, const fpm_optimizer *opt, float *param,
                               const float *grad, size_t n, int32_t memory);
 
-/* Learned warm start (config 5 of the north star; no counterpart in the reference, whose
-   initial object is imresize(Y_1, pratio) with zero phase, codes_v2/main_run_FPM.m:48).
+/* Learned warm start (no counterpart in the reference, whose initial object is
+   imresize(Y_1, pratio) with zero phase, codes_v2/main_run_FPM.m:48).
    A 4-level convolutional encoder-decoder (channels base, 2 base, 4 base, 8 base; base a
    multiple of 8 up to 32; 3x3 convolutions on the tcgen05 tensor cores with BF16 operands
    and FP32 accumulation in tensor memory; FP32 master weights) maps the first in_channels frames of a stack (the central bright-field block
