@@ -755,7 +755,7 @@ def run_instances(args, cfg: Cfg):
 
 
 def run_warmstart(args, cfg: Cfg):
-    """The learned warm start (config 5).  Training set: `--train-pairs` seeded objects of
+    """The learned warm start.  Training set: `--train-pairs` seeded objects of
     1024^2 seen through 11 x 11 LEDs as 256^2 frames (pratio 4); each pair is the 25
     central amplitudes and the low-pass of the plain method's object after 20 epochs (LED
     batch 8, lr 2e-3).  The network (25 inputs, 32 base channels) is trained with Adam in

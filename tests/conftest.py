@@ -62,7 +62,7 @@ def dataset(h, pratio, grid, seed=0, aberration=False):
 
 @pytest.fixture(scope="session")
 def ds_a():
-    """Config A: 11 x 11 LEDs of 128 x 128, pratio 4, seed 0."""
+    """The 128² case: 11 x 11 LEDs of 128 x 128, pratio 4, seed 0."""
     return dataset(128, 4, 11, seed=0)
 
 

@@ -14,7 +14,7 @@ complex128; its complex64 twin (cuFFT) gives the FP32 distance that sets the bar
   engine against the FP64 result exactly as it measures the twin;
 * the per-batch loss: 1e-5 relative to FP64 (a sum over 4M pixels per LED, continuous
   in the inputs);
-* config B end to end (361 LEDs of 512² -> 4096², 10 epochs): the criteria of config A
+* 361 LEDs of 512² -> 4096² end to end (10 epochs): the criteria of the 128² case
   (within max(5x the twin's drift, 3e-2), loss curve to 5e-3, the true object
   reconstructed as well as FP64 reconstructs it, within 2%).
 
@@ -228,10 +228,10 @@ def _truth_err(O, T):
     return float(torch.linalg.vector_norm(a * O - T) / torch.linalg.vector_norm(T))
 
 
-def test_config_b_end_to_end_vs_fp64(engine):
-    """Config B: 19 x 19 LEDs (361 frames) of 512² uint16 -> 4096², Zernike-aberrated
+def test_512x361_end_to_end_vs_fp64(engine):
+    """19 x 19 LEDs (361 frames) of 512² uint16 -> 4096², Zernike-aberrated
     pupil, LED batch 26, 10 epochs, lr 1e-3, beta 0.999 (seeded synthetic data with the
-    optics of config A scaled to the grid), against FP64 with config A's criteria; the
+    optics of the 128² case scaled to the grid), against FP64 with the 128² case's criteria; the
     recovered pupil's error against the true pupil is reported."""
     import torch
     from fpm_b200 import synth
@@ -250,7 +250,7 @@ def test_config_b_end_to_end_vs_fp64(engine):
     r32 = tr.cufpm_pure_v3(O0, P0c, Y, ds.led_idx, P0, 8, 10, 26, opt=opt, ctype=torch.complex64)
     for k in ("object", "pupil", "spectrum"):
         e, t = tr.rel_err(r[k], r64[k]), tr.rel_err(r32[k], r64[k])
-        print(f"config B {k}: engine-vs-fp64 {e:.3e}, fp32-twin-vs-fp64 {t:.3e}")
+        print(f"512x361 {k}: engine-vs-fp64 {e:.3e}, fp32-twin-vs-fp64 {t:.3e}")
         assert e < max(5 * t, 3e-2), k
     loss = np.asarray(r["loss"].cpu())
     np.testing.assert_allclose(loss, r64["loss"], rtol=5e-3)
@@ -259,7 +259,7 @@ def test_config_b_end_to_end_vs_fp64(engine):
     q_e, q_64 = _truth_err(r["object"], T), _truth_err(r64["object"], T)
     Pt = dev(ds.pupil_true)
     p_e, p_64 = _truth_err(r["pupil"], Pt), _truth_err(r64["pupil"], Pt)
-    print(f"config B vs truth: object engine {q_e:.4f} fp64 {q_64:.4f}; "
+    print(f"512x361 vs truth: object engine {q_e:.4f} fp64 {q_64:.4f}; "
           f"pupil engine {p_e:.4f} fp64 {p_64:.4f}")
     assert abs(q_e - q_64) < 0.02 * q_64
     assert abs(p_e - p_64) < 0.02 * p_64

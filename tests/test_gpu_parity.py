@@ -7,7 +7,7 @@ Tolerances (relative L2 error, complex, no phase alignment):
 * long runs on noisy data: the sign() of the feature-domain loss flips on
   near-tied residual differences, a chaotic process, so every FP32
   implementation (the reference's, the FP32 oracle twin, this engine) drifts
-  from FP64 by ~1e-2 after a few epochs of config A.  There the engine must
+  from FP64 by ~1e-2 after a few epochs of the 128² case.  There the engine must
   stay within max(5x the twin's drift, 3e-2), match the loss curve to 5e-3,
   and reconstruct the true object as well as FP64 does (within 2%);
 * integer-exact paths (uint16 ingest, host vs device memory): bit-identical.
@@ -122,8 +122,8 @@ def _truth_err(O, T):
     return float(np.linalg.norm(a * O - T) / np.linalg.norm(T))
 
 
-def test_solve_config_a_vs_oracle(engine, ds_a):
-    """Config A end to end: 121 LEDs, 5 epochs, batch 8, lr 1e-3."""
+def test_solve_128x121_vs_oracle(engine, ds_a):
+    """The 128² case end to end: 121 LEDs, 5 epochs, batch 8, lr 1e-3."""
     ds = ds_a
     opt = (1e-3, 0.999, 1e-4)
     r = _solve(engine, ds, 121, 5, 8, opt)
@@ -133,13 +133,13 @@ def test_solve_config_a_vs_oracle(engine, ds_a):
     for k in ("object", "pupil", "spectrum"):
         e = orc.rel_err(r[k], getattr(o64, k))
         e32 = orc.rel_err(getattr(o32, k), getattr(o64, k))
-        print(f"config A {k}: engine-vs-fp64 {e:.3e}, fp32-oracle-vs-fp64 {e32:.3e}")
+        print(f"128x121 {k}: engine-vs-fp64 {e:.3e}, fp32-oracle-vs-fp64 {e32:.3e}")
         assert e < max(5 * e32, 3e-2), k
     np.testing.assert_allclose(r["loss"], o64.loss, rtol=5e-3)
     assert np.all(np.diff(r["loss"]) < 0)
     q_engine = _truth_err(r["object"], ds.object_true)
     q_fp64 = _truth_err(o64.object, ds.object_true)
-    print(f"config A error vs true object: engine {q_engine:.4f}, fp64 oracle {q_fp64:.4f}")
+    print(f"128x121 error vs true object: engine {q_engine:.4f}, fp64 oracle {q_fp64:.4f}")
     assert abs(q_engine - q_fp64) < 0.02 * q_fp64
 
 
