@@ -731,6 +731,15 @@ def run_instances(args, cfg: Cfg):
         if name == "one_by_one":
             ref = [(O.clone(), P.clone()) for O, P in outs]
     same = all(torch.equal(O, r[0]) and torch.equal(P, r[1]) for (O, P), r in zip(outs, ref))
+    # where the time goes: each instance solved alone (after the warm-up above)
+    per = []
+    for i in range(n):
+        t0 = time.perf_counter()
+        eng._check(eng.solve_raw(probs[i], ress[i]))
+        per.append(time.perf_counter() - t0)
+    pow2 = lambda v: v & (v - 1) == 0
+    any_size = [not (pow2(a["h"]) and pow2(a["h"] * a["pratio"])) for a in inst]
+    t_any = sum(t for t, g in zip(per, any_size) if g)
     value = led_updates / timings["batch"]
     line = {"metric": "aggregate LED-updates/s, 48 uneven FPM instances (fpm_solve_batch)",
             "value": round(value, 1), "unit": "LED-updates/s", "n_gpus": 1, "steps": args.steps,
@@ -748,6 +757,9 @@ def run_instances(args, cfg: Cfg):
             "speedup_vs_one_by_one": round(timings["one_by_one"] / timings["batch"], 3),
             "seconds": {k: round(v, 4) for k, v in timings.items()},
             "batch_equals_one_by_one_bitwise": bool(same),
+            "instance_seconds": [round(t, 4) for t in per],
+            "any_size_instances": int(sum(any_size)),
+            "any_size_share_of_time": round(t_any / max(sum(per), 1e-12), 3),
             "timing": "host wall clock around each call (each returns after its final "
                       "synchronisation), median of the steps"}
     eng.close()

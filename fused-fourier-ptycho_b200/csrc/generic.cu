@@ -99,11 +99,21 @@ __device__ __forceinline__ float2 cmul2(float2 w, float2 v) {
     return make_float2(w.x * v.x - w.y * v.y, w.x * v.y + w.y * v.x);
 }
 
+// k mod p of a butterfly index j < 2^24: the quotient from the float reciprocal of p,
+// corrected to the exact one
+__device__ __forceinline__ int mod_p(int j, int p, float pinv) {
+    int q = __float2int_rz(__int2float_rn(j) * pinv);
+    int r = j - q * p;
+    if (r < 0) r += p;
+    else if (r >= p) r -= p;
+    return r;
+}
+
 // One radix-R stage over a line of n values at s (shared memory), T = ceil(n/V) threads,
-// thread t.
+// thread t; pinv = 1 / p.
 template <int R, int DIR, int V>
-__device__ __noinline__ void gen_stage(float2 *s, int n, int p, int T, int t,
-                                          const float2 *__restrict__ tw) {
+__device__ __forceinline__ void gen_stage_body(float2 *s, int n, int p, float pinv, int T, int t,
+                                               const float2 *__restrict__ tw) {
     constexpr int KMAX = (V + R - 1) / R;    // ceil(n/R / ceil(n/V)) <= ceil(V/R)
     const int nbf = n / R;
     float2 v[KMAX][R];
@@ -121,7 +131,7 @@ __device__ __noinline__ void gen_stage(float2 *s, int n, int p, int T, int t,
     for (int k = 0; k < KMAX; ++k) {
         const int j = t + k * T;
         if (j < nbf) {
-            const int kk = j % p;
+            const int kk = p > 1 ? mod_p(j, p, pinv) : 0;
             if (p > 1) {
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
@@ -139,9 +149,18 @@ __device__ __noinline__ void gen_stage(float2 *s, int n, int p, int T, int t,
     __syncthreads();
 }
 
+// a call per stage keeps the kernel's registers within 128 (inlined, the six radices'
+// bodies spill)
+template <int R, int DIR, int V>
+__device__ __noinline__ void gen_stage(float2 *s, int n, int p, float pinv, int T, int t,
+                                       const float2 *__restrict__ tw) {
+    gen_stage_body<R, DIR, V>(s, n, p, pinv, T, t, tw);
+}
+
 struct GenPlan {
     int n = 0, nst = 0, T = 0, lpc = 1, v = 8;
     int radix[16] = {};
+    float pinv[16] = {};   // 1 / (product of the radices before stage i)
 };
 
 // V values per thread: 8 up to n = 4096, 16 up to 8192, 32 beyond (at most 512 threads
@@ -168,14 +187,15 @@ __global__ void __launch_bounds__(512, 1) k_gen_lines(const float2 *__restrict__
     int p = 1;
     for (int st = 0; st < pl.nst; ++st) {
         const int R = pl.radix[st];
+        const float pinv = pl.pinv[st];
         const int tt = live ? t : (1 << 29);   // idle threads skip every butterfly
         switch (R) {
-            case 2: gen_stage<2, DIR, V>(s, n, p, T, tt, tw); break;
-            case 3: gen_stage<3, DIR, V>(s, n, p, T, tt, tw); break;
-            case 4: gen_stage<4, DIR, V>(s, n, p, T, tt, tw); break;
-            case 5: gen_stage<5, DIR, V>(s, n, p, T, tt, tw); break;
-            case 7: gen_stage<7, DIR, V>(s, n, p, T, tt, tw); break;
-            default: gen_stage<8, DIR, V>(s, n, p, T, tt, tw); break;
+            case 2: gen_stage<2, DIR, V>(s, n, p, pinv, T, tt, tw); break;
+            case 3: gen_stage<3, DIR, V>(s, n, p, pinv, T, tt, tw); break;
+            case 4: gen_stage<4, DIR, V>(s, n, p, pinv, T, tt, tw); break;
+            case 5: gen_stage<5, DIR, V>(s, n, p, pinv, T, tt, tw); break;
+            case 7: gen_stage<7, DIR, V>(s, n, p, pinv, T, tt, tw); break;
+            default: gen_stage<8, DIR, V>(s, n, p, pinv, T, tt, tw); break;
         }
         p *= R;
     }
@@ -190,7 +210,12 @@ GenPlan make_plan(int n) {
     pl.n = n;
     const std::vector<int> rad = gen_fft_radices(n);
     pl.nst = (int)rad.size();
-    for (int i = 0; i < pl.nst; ++i) pl.radix[i] = rad[i];
+    int prod = 1;
+    for (int i = 0; i < pl.nst; ++i) {
+        pl.radix[i] = rad[i];
+        pl.pinv[i] = 1.0f / (float)prod;
+        prod *= rad[i];
+    }
     pl.v = n <= 4096 ? 8 : n <= 8192 ? 16 : 32;
     pl.T = (n + pl.v - 1) / pl.v;
     // lines per CTA: up to 16, within 512 threads and 96 KiB of shared memory
