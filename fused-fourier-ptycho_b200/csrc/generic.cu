@@ -205,6 +205,106 @@ __global__ void __launch_bounds__(512, 1) k_gen_lines(const float2 *__restrict__
     }
 }
 
+// Register-resident form, where every stage's radix divides the values per thread V: a
+// thread holds the canonical elements t + m T (m < V, T = n / V) of its line, loaded and
+// stored straight from global memory.  The first stage's butterflies j = t + k T take
+// their inputs x[j + r n/R] = element t + (k + r V/R) T from the thread's own registers,
+// the last stage's outputs y[j + r p] land on the same elements, and only the stages in
+// between exchange through shared memory; V/R butterflies per thread in every stage.
+struct VPlan {
+    int n = 0, V = 0, T = 0, lpc = 1, nst = 0;
+    int radix[16] = {};
+    float pinv[16] = {};
+};
+
+template <int R, int DIR, int V>
+__device__ __forceinline__ void vstage(float2 (&v)[V], float2 *s, int n, int p, float pinv, int T,
+                                       int t, const float2 *__restrict__ tw, bool first,
+                                       bool last) {
+    constexpr int NB = V / R;
+    const int nbf = n / R;   // = NB T butterflies
+    if (!first) {
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[k + r * NB] = s[t + k * T + r * nbf];
+        __syncthreads();   // every read of the line done before it is rewritten
+    }
+    const int step = n / (p * R);
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const int j = t + k * T;
+        float2 u[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) u[r] = v[k + r * NB];
+        int kk = 0;
+        if (p > 1) {
+            kk = mod_p(j, p, pinv);
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                float2 w = __ldg(tw + r * kk * step);   // < n: (R-1)(p-1) n/(pR) < n
+                if (DIR > 0) w.y = -w.y;
+                u[r] = cmul2(w, u[r]);
+            }
+        }
+        dft_any<R, DIR>(u);
+        if (last) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[k + r * NB] = u[r];   // y[j + r p], p = n/R
+        } else {
+            const int base = (j - kk) * R + kk;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[base + r * p] = u[r];
+        }
+    }
+    if (!last) __syncthreads();   // the stage's outputs visible to the next stage
+}
+
+template <int DIR, int V>
+__global__ void __launch_bounds__(512, 1) k_gen_lines_v(const float2 *__restrict__ in,
+                                                      float2 *__restrict__ out, long long count,
+                                                      size_t ld, VPlan pl,
+                                                      const float2 *__restrict__ tw) {
+    extern __shared__ float2 smem[];
+    const int n = pl.n, T = pl.T;
+    const int line = threadIdx.x / T, t = threadIdx.x - line * T;
+    const long long g = (long long)blockIdx.x * pl.lpc + line;
+    const bool live = g < count;   // lines past the last one join every barrier on zeros
+    float2 *s = smem + (size_t)line * n;
+    float2 v[V];
+    const float2 *src = in + (size_t)(live ? g : 0) * ld;
+#pragma unroll
+    for (int m = 0; m < V; ++m) v[m] = live ? src[t + m * T] : make_float2(0.f, 0.f);
+    int p = 1;
+    for (int st = 0; st < pl.nst; ++st) {
+        const int R = pl.radix[st];
+        const float pinv = pl.pinv[st];
+        const bool first = st == 0, last = st == pl.nst - 1;
+        switch (R) {
+            case 2: vstage<2, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last); break;
+            case 4: vstage<4, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last); break;
+            case 3:
+                if constexpr (V % 3 == 0) vstage<3, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                break;
+            case 5:
+                if constexpr (V % 5 == 0) vstage<5, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                break;
+            case 7:
+                if constexpr (V % 7 == 0) vstage<7, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                break;
+            default:
+                if constexpr (V % 8 == 0) vstage<8, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                break;
+        }
+        p *= R;
+    }
+    if (live) {
+        float2 *dst = out + (size_t)g * ld;
+#pragma unroll
+        for (int m = 0; m < V; ++m) dst[t + m * T] = v[m];
+    }
+}
+
 GenPlan make_plan(int n) {
     GenPlan pl;
     pl.n = n;
@@ -399,12 +499,85 @@ cudaError_t GenFft::table(int n, const float2 **tw) {
     return cudaSuccess;
 }
 
+// A register-resident plan for n: V in {16, 24, 20, 28} values per thread (the radices of
+// each divide it: 8, 4, 2 and 3 for 24; 4, 2 and 5 for 20; 4, 2 and 7 for 28), at least 8
+// and at most 512 threads per line.  False where none fits (odd parts 15, 21, ...): the
+// shared-memory form then runs.
+bool make_vplan(int n, VPlan &pl) {
+    int a = 0, m = n;
+    while (m % 2 == 0) m /= 2, ++a;
+    int odd[3] = {0, 0, 0};
+    const int primes[3] = {3, 5, 7};
+    for (int i = 0; i < 3; ++i)
+        while (m % primes[i] == 0) m /= primes[i], ++odd[i];
+    if (m != 1) return false;
+    int V = 0, pmax = 0, q = 0;
+    if (odd[1] == 0 && odd[2] == 0) {
+        V = odd[0] ? 24 : 16;
+        pmax = 8;
+        q = 3;
+    } else if (odd[0] == 0 && odd[2] == 0) {
+        V = 20, pmax = 4, q = 5;
+    } else if (odd[0] == 0 && odd[1] == 0) {
+        V = 28, pmax = 4, q = 7;
+    } else {
+        return false;
+    }
+    if (n % V != 0) return false;
+    const int T = n / V;
+    if (T < 8 || T > 512) return false;
+    // the order of gen_fft_radices (powers of two first, the odd radix last), so that where
+    // V holds radix 8 every butterfly computes what the shared-memory form computes
+    std::vector<int> rad;
+    const int nq = q == 3 ? odd[0] : q == 5 ? odd[1] : odd[2];
+    while (a >= 3 && pmax >= 8) rad.push_back(8), a -= 3;
+    while (a >= 2) rad.push_back(4), a -= 2;
+    if (a == 1) rad.push_back(2);
+    for (int i = 0; i < nq; ++i) rad.push_back(q);
+    if ((int)rad.size() > 16) return false;
+    pl.n = n;
+    pl.V = V;
+    pl.T = T;
+    pl.nst = (int)rad.size();
+    int prod = 1;
+    for (int i = 0; i < pl.nst; ++i) {
+        pl.radix[i] = rad[i];
+        pl.pinv[i] = 1.0f / (float)prod;
+        prod *= rad[i];
+    }
+    // lines per CTA: about 256 threads, within 96 KiB of shared memory
+    pl.lpc = 1;
+    while (pl.lpc < 16 && (pl.lpc * 2) * T <= 256 && (size_t)(pl.lpc * 2) * n * 8 <= 96 * 1024)
+        pl.lpc *= 2;
+    return prod == n;
+}
+
 cudaError_t GenFft::lines(const float2 *in, float2 *out, int n, long long count, size_t ld,
                           FftDir dir, cudaStream_t st) {
     if (!gen_fft_supported(n) || count < 1 || ld < (size_t)n) return cudaErrorInvalidValue;
     const float2 *tw = nullptr;
     cudaError_t e = table(n, &tw);
     if (e != cudaSuccess) return e;
+    VPlan vp;
+    if (knob("FPM_GEN_REG", 0, 0, 1) != 0 && make_vplan(n, vp)) {
+        const long long vblocks = (count + vp.lpc - 1) / vp.lpc;
+        if (vblocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+        const size_t vsmem = (size_t)vp.lpc * n * sizeof(float2);
+        auto vgo = [&](auto kernel) {
+            cudaError_t e2 = cudaFuncSetAttribute(
+                kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsmem);
+            if (e2 != cudaSuccess) return e2;
+            kernel<<<(unsigned)vblocks, vp.T * vp.lpc, vsmem, st>>>(in, out, count, ld, vp, tw);
+            return cudaGetLastError();
+        };
+        const bool fwd = dir == kForward;
+        switch (vp.V) {
+            case 16: return fwd ? vgo(k_gen_lines_v<-1, 16>) : vgo(k_gen_lines_v<1, 16>);
+            case 20: return fwd ? vgo(k_gen_lines_v<-1, 20>) : vgo(k_gen_lines_v<1, 20>);
+            case 24: return fwd ? vgo(k_gen_lines_v<-1, 24>) : vgo(k_gen_lines_v<1, 24>);
+            default: return fwd ? vgo(k_gen_lines_v<-1, 28>) : vgo(k_gen_lines_v<1, 28>);
+        }
+    }
     const GenPlan pl = make_plan(n);
     const long long blocks = (count + pl.lpc - 1) / pl.lpc;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;

@@ -34,6 +34,23 @@ def test_any_size_fft2_matches_numpy(engine, n):
     assert orc.rel_err(back / (n * n), x) < 2 * tol
 
 
+@pytest.mark.parametrize("n", [192, 768, 1152, 3072, 256])
+def test_register_resident_lines_equal_the_shared_memory_form(engine, n, monkeypatch):
+    """Where radix 8 divides the values per thread (24 for lengths 3^k 2^a, 16 for powers
+    of two) the register-resident line transform runs the shared-memory form's butterflies
+    in the same order on the same values: bit-identical 2-D transforms both ways."""
+    import torch
+    rng = np.random.default_rng(n)
+    x = torch.from_numpy((rng.standard_normal((n, n, 2)) + 1j * rng.standard_normal((n, n, 2)))
+                         .astype(np.complex64)).cuda()
+    got = [engine.fft2(x, direction=d) for d in (-1, 1)]
+    monkeypatch.setenv("FPM_GEN_REG", "0")
+    ref = [engine.fft2(x, direction=d) for d in (-1, 1)]
+    monkeypatch.delenv("FPM_GEN_REG")
+    for a, b in zip(got, ref):
+        assert torch.equal(a, b), n
+
+
 def _noiseless_ds(h, p, grid, seed):
     from fpm_b200 import synth
     ds = dataset(h, p, grid, seed=seed, aberration=True)
