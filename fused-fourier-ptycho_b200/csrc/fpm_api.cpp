@@ -875,7 +875,11 @@ static fpm_status gen_batch(fpm_context *ctx, const Shape &s, const Inputs &in, 
     cudaStream_t st = ctx->stream;
     float2 *S = ctx->S.as<float2>(), *G = ctx->U.as<float2>(), *W = ctx->W.as<float2>();
     float2 *T1 = ctx->T1.as<float2>(), *T2 = ctx->T2.as<float2>(), *Tt = ctx->Xs.as<float2>();
-    FPM_STAGE(ST_SPECTRUM, ctx->gfft.fft2(O, S, W, s.H, 1, kForward, st));   // K1
+    // the batch's crops read the spectrum on the box rows only (un-shifted: centred + H/2),
+    // and the gradient spectrum is zero outside the box columns
+    const int box_r = box.r_lo + s.H / 2, box_c = box.c_lo + s.H / 2;
+    FPM_STAGE(ST_SPECTRUM,
+              ctx->gfft.fft2_box(O, S, W, s.H, kForward, 0, s.H, box_r, box.r_span, st));   // K1
     FPM_STAGE(ST_LR_COLS_INV, launch_gen_crop_pupil(S, s.H, P, s.h, in.led, z_off, nb, T1, st));
     FPM_STAGE(ST_GEN_LR_FFT, ctx->gfft.fft2(T1, T1, Tt, s.h, nb, kInverse, st));        // K3
     FPM_STAGE(ST_GEN_LOSS, launch_feature_grad(T1, in.Y, z_off, nb, s.h, s.pratio, T2,
@@ -888,7 +892,8 @@ static fpm_status gen_batch(fpm_context *ctx, const Shape &s, const Inputs &in, 
                                                box.r_span, box.c_lo, box.c_span, G, st));
     FPM_STAGE(ST_PUPIL_GRAD,
               launch_gen_pupil_grad(S, s.H, T2, s.h, in.led, z_off, nb, ctx->dP.as<float2>(), st));
-    FPM_STAGE(ST_GEN_OBJ_FFT, ctx->gfft.fft2(G, G, W, s.H, 1, kInverse, st));            // K8
+    FPM_STAGE(ST_GEN_OBJ_FFT,
+              ctx->gfft.fft2_box(G, G, W, s.H, kInverse, box_c, box.c_span, 0, s.H, st));   // K8
     return FPM_OK;
 }
 

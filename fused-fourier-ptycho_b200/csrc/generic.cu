@@ -623,6 +623,25 @@ cudaError_t GenFft::fft2(const float2 *in, float2 *out, float2 *tmp, int n, int 
     return e;
 }
 
+cudaError_t GenFft::fft2_box(const float2 *in, float2 *out, float2 *tmp, int n, FftDir dir,
+                             int c_lo, int c_cnt, int r_lo, int r_cnt, cudaStream_t st) {
+    if (c_cnt < 1 || c_cnt > n || r_cnt < 1 || r_cnt > n || (c_cnt < n && in != out))
+        return cudaErrorInvalidValue;
+    // lines [lo, lo + cnt) mod n of a page: one or two contiguous runs
+    auto run = [&](const float2 *src, float2 *dst, int lo, int cnt) {
+        lo = ((lo % n) + n) % n;
+        const int first = std::min(cnt, n - lo);
+        cudaError_t e = lines(src + (size_t)lo * n, dst + (size_t)lo * n, n, first, n, dir, st);
+        if (e == cudaSuccess && cnt > first) e = lines(src, dst, n, cnt - first, n, dir, st);
+        return e;
+    };
+    cudaError_t e = run(in, out, c_lo, c_cnt);                      // along r, box columns
+    if (e == cudaSuccess) e = launch_transpose_pages(out, tmp, n, 1, st);
+    if (e == cudaSuccess) e = run(tmp, tmp, r_lo, r_cnt);          // along c, box rows
+    if (e == cudaSuccess) e = launch_transpose_pages(tmp, out, n, 1, st);
+    return e;
+}
+
 cudaError_t launch_gen_crop_pupil(const float2 *S, int H, const float2 *P, int h, const int2 *led,
                                   int z_off, int nb, float2 *out, cudaStream_t st) {
     if (nb < 1 || nb > 65535) return cudaErrorInvalidValue;
