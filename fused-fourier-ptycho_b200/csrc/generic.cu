@@ -217,17 +217,22 @@ struct VPlan {
     float pinv[16] = {};
 };
 
+// shared-memory position of line element l: l ^ ((l >> 4) & 15) within its 16-element
+// block when n is a multiple of 16 (mask 15: the stride-R stores of a stage and the
+// contiguous loads fall on distinct banks), l itself otherwise (mask 0)
+__device__ __forceinline__ int vswz(int l, int mask) { return l ^ ((l >> 4) & mask); }
+
 template <int R, int DIR, int V>
 __device__ __forceinline__ void vstage(float2 (&v)[V], float2 *s, int n, int p, float pinv, int T,
                                        int t, const float2 *__restrict__ tw, bool first,
-                                       bool last) {
+                                       bool last, int mask) {
     constexpr int NB = V / R;
     const int nbf = n / R;   // = NB T butterflies
     if (!first) {
 #pragma unroll
         for (int k = 0; k < NB; ++k)
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[k + r * NB] = s[t + k * T + r * nbf];
+            for (int r = 0; r < R; ++r) v[k + r * NB] = s[vswz(t + k * T + r * nbf, mask)];
         __syncthreads();   // every read of the line done before it is rewritten
     }
     const int step = n / (p * R);
@@ -254,7 +259,7 @@ __device__ __forceinline__ void vstage(float2 (&v)[V], float2 *s, int n, int p, 
         } else {
             const int base = (j - kk) * R + kk;
 #pragma unroll
-            for (int r = 0; r < R; ++r) s[base + r * p] = u[r];
+            for (int r = 0; r < R; ++r) s[vswz(base + r * p, mask)] = u[r];
         }
     }
     if (!last) __syncthreads();   // the stage's outputs visible to the next stage
@@ -275,25 +280,26 @@ __global__ void __launch_bounds__(512, 1) k_gen_lines_v(const float2 *__restrict
     const float2 *src = in + (size_t)(live ? g : 0) * ld;
 #pragma unroll
     for (int m = 0; m < V; ++m) v[m] = live ? src[t + m * T] : make_float2(0.f, 0.f);
+    const int mask = n % 16 == 0 ? 15 : 0;
     int p = 1;
     for (int st = 0; st < pl.nst; ++st) {
         const int R = pl.radix[st];
         const float pinv = pl.pinv[st];
         const bool first = st == 0, last = st == pl.nst - 1;
         switch (R) {
-            case 2: vstage<2, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last); break;
-            case 4: vstage<4, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last); break;
+            case 2: vstage<2, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last, mask); break;
+            case 4: vstage<4, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last, mask); break;
             case 3:
-                if constexpr (V % 3 == 0) vstage<3, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                if constexpr (V % 3 == 0) vstage<3, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last, mask);
                 break;
             case 5:
-                if constexpr (V % 5 == 0) vstage<5, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                if constexpr (V % 5 == 0) vstage<5, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last, mask);
                 break;
             case 7:
-                if constexpr (V % 7 == 0) vstage<7, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                if constexpr (V % 7 == 0) vstage<7, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last, mask);
                 break;
             default:
-                if constexpr (V % 8 == 0) vstage<8, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last);
+                if constexpr (V % 8 == 0) vstage<8, DIR, V>(v, s, n, p, pinv, T, t, tw, first, last, mask);
                 break;
         }
         p *= R;
