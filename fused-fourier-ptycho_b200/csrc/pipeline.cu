@@ -1123,10 +1123,13 @@ __global__ void __launch_bounds__(fft::LG<N, E>::THREADS, 1)
         pending = false;
         parity ^= 1u;
         float2 v[E];
+        const int in = i + gridDim.x;
+        // the next row's DRAM read starts under this row's FFT; its copy into the exchange
+        // area during the last stage then reads L2
+        if (t == 0 && in < rspan_n) tma::prefetch_l2(Vr + (size_t)in * N, N * 8);
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = line[t + m * G::T];
         __syncthreads();                               // every read before the first exchange
-        const int in = i + gridDim.x;
         fft::line_fft_regs32<N, -1>(v, line, s_hi, s_hi + 128, t, [&] {
             if (t == 0 && in < rspan_n) {
                 tma::fence_proxy_async();

@@ -65,6 +65,12 @@ __device__ __forceinline__ void load_1d(void *dst, const void *src, uint32_t byt
         : "memory");
 }
 
+// Starts bringing `bytes` (a multiple of 16; src 16-byte aligned) from global memory into
+// L2 without a destination or completion: a later copy of the same range reads L2.
+__device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
