@@ -170,6 +170,8 @@ struct fpm_context {
     DevBuf O, m1, S, P, m2, P0, dP, Pt, T1, T2, Rs, Xs, Sbox, Sboxr, U, V, W, Y, led, parts, loss,
         minmax, lut, spec, flag, pie, rows;
     DevBuf opt[6];   // device copies of an optimiser step's host arrays
+    // the last captured epoch; a later capture of the same topology updates it in place
+    cudaGraphExec_t epoch_graph = nullptr;
     // fpm_solve_batch: one worker context per instance, on a pool of streams
     std::vector<fpm_context *> workers;
     std::vector<cudaStream_t> pool;
@@ -770,6 +772,7 @@ void fpm_destroy(fpm_context *ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (fpm_context *w : ctx->workers) fpm_destroy(w);
     for (cudaStream_t sp : ctx->pool) cudaStreamDestroy(sp);
+    if (ctx->epoch_graph) cudaGraphExecDestroy(ctx->epoch_graph);
     ctx->fft.release();
     ctx->gfft.release();
     if (ctx->entry) cudaEventDestroy(ctx->entry);
@@ -1127,7 +1130,10 @@ static void job_lr_after(SolveJob &j, int ep) {
 // the device-side epoch counter names and advances the counter, so one graph serves every
 // epoch that shares the learning rate.  *exec stays null when the capture did not succeed
 // (a call the capture refused, or any failure while recording: nothing ran, and the caller
-// runs the epochs eagerly, where a genuine error shows up again).
+// runs the epochs eagerly, where a genuine error shows up again).  The executable graph
+// belongs to the context and outlives the call: a capture with the same nodes and edges
+// (a later learning rate, or a later solve of the same plan) writes its parameters into it
+// instead of instantiating a new one; launches already enqueued keep the old parameters.
 static fpm_status job_capture(fpm_context *ctx, SolveJob &j, cudaGraphExec_t *exec) {
     *exec = nullptr;
     cudaStream_t st = ctx->stream;
@@ -1152,11 +1158,24 @@ static fpm_status job_capture(fpm_context *ctx, SolveJob &j, cudaGraphExec_t *ex
         ctx->err.clear();
         return FPM_OK;
     }
+    if (ctx->epoch_graph) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ctx->epoch_graph, graph, &info) == cudaSuccess) {
+            cudaGraphDestroy(graph);
+            *exec = ctx->epoch_graph;
+            return FPM_OK;
+        }
+        cudaGetLastError();   // another topology: a new executable graph replaces it
+        cudaGraphExecDestroy(ctx->epoch_graph);
+        ctx->epoch_graph = nullptr;
+    }
     e = cudaGraphInstantiate(exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
         *exec = nullptr;
         cudaGetLastError();
+    } else {
+        ctx->epoch_graph = *exec;
     }
     return FPM_OK;
 }
@@ -1221,11 +1240,10 @@ static fpm_status job_run_epochs(fpm_context *ctx, SolveJob &j, bool graphs) {
     rc = job_epoch(ctx, j, j.loss, E == 1);
     if (rc != FPM_OK) return rc;
     job_lr_after(j, 0);
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec = nullptr;   // owned by the context (job_capture)
     float exec_lr = 0.f;
     for (int ep = 1; ep < E; ++ep) {
         if (graphs && (!exec || exec_lr != j.lr)) {
-            if (exec) cudaGraphExecDestroy(exec);
             exec = nullptr;
             FPM_CK(launch_set_int(j.epoch_counter, ep, st));   // the slot of the next replay
             rc = job_capture(ctx, j, &exec);
@@ -1236,7 +1254,8 @@ static fpm_status job_run_epochs(fpm_context *ctx, SolveJob &j, bool graphs) {
         if (exec) {
             const cudaError_t e = cudaGraphLaunch(exec, st);
             if (e != cudaSuccess) {
-                cudaGraphExecDestroy(exec);
+                cudaGraphExecDestroy(ctx->epoch_graph);
+                ctx->epoch_graph = nullptr;
                 return fail_cuda(ctx, e, "cudaGraphLaunch", __LINE__);
             }
         } else {
@@ -1245,7 +1264,6 @@ static fpm_status job_run_epochs(fpm_context *ctx, SolveJob &j, bool graphs) {
         }
         job_lr_after(j, ep);
     }
-    if (exec) cudaGraphExecDestroy(exec);
     return FPM_OK;
 }
 

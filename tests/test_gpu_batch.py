@@ -73,3 +73,25 @@ def test_epoch_graphs_equal_eager_epochs(engine, h, p):
             del os.environ["FPM_GRAPHS"]
     for k in ("object", "pupil", "spectrum", "loss"):
         np.testing.assert_array_equal(np.asarray(runs["1"][k]), np.asarray(runs["0"][k]), err_msg=k)
+
+
+def test_kept_epoch_graph_equals_a_fresh_one():
+    """A context keeps its executable epoch graph between solves: a later capture with the
+    same nodes (another learning rate, another problem of the same plan) writes its
+    parameters into it, one with other nodes replaces it.  Every solve of a context that
+    went through both must equal, bit for bit, the same solve in a fresh context
+    (problems A and B of one shape, then C of another; lr halved after epoch 1, so each
+    solve also captures twice)."""
+    import fpm_b200
+    probs = []
+    for seed, h, p in ((31, 64, 4), (32, 64, 4), (33, 48, 4), (34, 64, 4)):
+        ds = dataset(h, p, 5, seed=seed, aberration=True)
+        probs.append((ds.O0, ds.P0c, to_matlab_stack(ds.raw), led_matlab(ds.led_idx),
+                      ds.pupil0, p, 4, 8))
+    with fpm_b200.Engine(0) as kept:
+        for args in probs:
+            a = kept.solve(*args, lr=1e-3, lr_halve_after=1)
+            with fpm_b200.Engine(0) as fresh:
+                b = fresh.solve(*args, lr=1e-3, lr_halve_after=1)
+            for k in ("object", "pupil", "spectrum", "loss"):
+                np.testing.assert_array_equal(np.asarray(a[k]), np.asarray(b[k]), err_msg=k)
