@@ -355,6 +355,47 @@ __global__ void __launch_bounds__(256) k_transpose_pages(const float2 *__restric
     }
 }
 
+// Rows [lo, lo + cnt) mod n of a column-major n x n page as cnt contiguous lines, and
+// back: TO_LINES: lines[i][c] = page[c][(lo + i) mod n]; else page[c][(lo + i) mod n] =
+// lines[i][c].  32 x 32 tiles through shared memory, both sides coalesced.
+template <bool TO_LINES>
+__global__ void __launch_bounds__(256) k_transpose_rows(const float2 *__restrict__ in,
+                                                        float2 *__restrict__ out, int n, int lo,
+                                                        int cnt) {
+    __shared__ float2 tile[32][33];
+    const int c0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    auto row = [&](int i) {
+        const int r = lo + i;
+        return r >= n ? r - n : r;
+    };
+    if (TO_LINES) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {   // page: consecutive rows of one column
+            const int c = c0 + ty + 8 * k, i = i0 + tx;
+            if (i < cnt && c < n) tile[ty + 8 * k][tx] = in[(size_t)c * n + row(i)];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {   // lines: consecutive columns of one line
+            const int i = i0 + ty + 8 * k, c = c0 + tx;
+            if (i < cnt && c < n) out[(size_t)i * n + c] = tile[tx][ty + 8 * k];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = i0 + ty + 8 * k, c = c0 + tx;
+            if (i < cnt && c < n) tile[ty + 8 * k][tx] = in[(size_t)i * n + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int c = c0 + ty + 8 * k, i = i0 + tx;
+            if (i < cnt && c < n) out[(size_t)c * n + row(i)] = tile[tx][ty + 8 * k];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // per-batch stages
 // ---------------------------------------------------------------------------
@@ -642,9 +683,25 @@ cudaError_t GenFft::fft2_box(const float2 *in, float2 *out, float2 *tmp, int n, 
         return e;
     };
     cudaError_t e = run(in, out, c_lo, c_cnt);                      // along r, box columns
-    if (e == cudaSuccess) e = launch_transpose_pages(out, tmp, n, 1, st);
-    if (e == cudaSuccess) e = run(tmp, tmp, r_lo, r_cnt);          // along c, box rows
-    if (e == cudaSuccess) e = launch_transpose_pages(tmp, out, n, 1, st);
+    if (r_cnt == n) {
+        if (e == cudaSuccess) e = launch_transpose_pages(out, tmp, n, 1, st);
+        if (e == cudaSuccess) e = run(tmp, tmp, r_lo, r_cnt);      // along c, every row
+        if (e == cudaSuccess) e = launch_transpose_pages(tmp, out, n, 1, st);
+        return e;
+    }
+    // only the box rows go through the transform along c: they alone are turned into
+    // contiguous lines and back; the other rows of out keep the first pass's values
+    const int lo = ((r_lo % n) + n) % n;
+    const dim3 grid((n + 31) / 32, (r_cnt + 31) / 32);
+    if (e == cudaSuccess) {
+        k_transpose_rows<true><<<grid, 256, 0, st>>>(out, tmp, n, lo, r_cnt);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = lines(tmp, tmp, n, r_cnt, n, dir, st);   // along c, box rows
+    if (e == cudaSuccess) {
+        k_transpose_rows<false><<<grid, 256, 0, st>>>(tmp, out, n, lo, r_cnt);
+        e = cudaGetLastError();
+    }
     return e;
 }
 
