@@ -890,7 +890,13 @@ static fpm_status gen_batch(fpm_context *ctx, const Shape &s, const Inputs &in, 
     FPM_STAGE(ST_LOSS, launch_loss_accumulate(ctx->parts.as<double>(),
                                               (int)gen_loss_parts(s.h, nb), loss_slot, st));
     FPM_STAGE(ST_GEN_LR_FFT, ctx->gfft.fft2(T2, T2, Tt, s.h, nb, kForward, st));        // K5
-    FPM_CK(cudaMemsetAsync(G, 0, s.big * 8, st));
+    {   // the inverse transform reads only the box columns (every row of them): those are
+        // cleared, one or two contiguous runs, and the stitch fills its covered positions
+        const int c0 = ((box_c % s.H) + s.H) % s.H, first = std::min(box.c_span, s.H - c0);
+        FPM_CK(cudaMemsetAsync(G + (size_t)c0 * s.H, 0, (size_t)first * s.H * 8, st));
+        if (box.c_span > first)
+            FPM_CK(cudaMemsetAsync(G, 0, (size_t)(box.c_span - first) * s.H * 8, st));
+    }
     FPM_STAGE(ST_GEN_STITCH, launch_gen_stitch(T2, s.h, P, in.led, z_off, nb, s.H, box.r_lo,
                                                box.r_span, box.c_lo, box.c_span, G, st));
     FPM_STAGE(ST_PUPIL_GRAD,

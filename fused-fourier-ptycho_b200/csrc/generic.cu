@@ -355,6 +355,33 @@ __global__ void __launch_bounds__(256) k_transpose_pages(const float2 *__restric
     }
 }
 
+// out[c][r] = in[r][c] for the columns [lo, lo + cnt) mod n of in, zero for the others (which
+// are never read): the transpose of a page whose other columns count as zeros.
+__global__ void __launch_bounds__(256) k_transpose_page_cols(const float2 *__restrict__ in,
+                                                             float2 *__restrict__ out, int n,
+                                                             int lo, int cnt) {
+    __shared__ float2 tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    auto inbox = [&](int c) {
+        int d = c - lo;
+        if (d < 0) d += n;
+        return d < cnt;
+    };
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int c = c0 + ty + 8 * k, r = r0 + tx;
+        if (r < n && c < n)
+            tile[ty + 8 * k][tx] = inbox(c) ? in[(size_t)c * n + r] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = r0 + ty + 8 * k, c = c0 + tx;
+        if (r < n && c < n) out[(size_t)r * n + c] = tile[tx][ty + 8 * k];
+    }
+}
+
 // Rows [lo, lo + cnt) mod n of a column-major n x n page as cnt contiguous lines, and
 // back: TO_LINES: lines[i][c] = page[c][(lo + i) mod n]; else page[c][(lo + i) mod n] =
 // lines[i][c].  32 x 32 tiles through shared memory, both sides coalesced.
@@ -672,7 +699,7 @@ cudaError_t GenFft::fft2(const float2 *in, float2 *out, float2 *tmp, int n, int 
 
 cudaError_t GenFft::fft2_box(const float2 *in, float2 *out, float2 *tmp, int n, FftDir dir,
                              int c_lo, int c_cnt, int r_lo, int r_cnt, cudaStream_t st) {
-    if (c_cnt < 1 || c_cnt > n || r_cnt < 1 || r_cnt > n || (c_cnt < n && in != out))
+    if (c_cnt < 1 || c_cnt > n || r_cnt < 1 || r_cnt > n || (c_cnt < n && (in != out || r_cnt < n)))
         return cudaErrorInvalidValue;
     // lines [lo, lo + cnt) mod n of a page: one or two contiguous runs
     auto run = [&](const float2 *src, float2 *dst, int lo, int cnt) {
@@ -684,7 +711,14 @@ cudaError_t GenFft::fft2_box(const float2 *in, float2 *out, float2 *tmp, int n, 
     };
     cudaError_t e = run(in, out, c_lo, c_cnt);                      // along r, box columns
     if (r_cnt == n) {
-        if (e == cudaSuccess) e = launch_transpose_pages(out, tmp, n, 1, st);
+        if (e == cudaSuccess && c_cnt < n) {   // only the box columns are read
+            const int lo = ((c_lo % n) + n) % n;
+            const dim3 grid((n + 31) / 32, (n + 31) / 32);
+            k_transpose_page_cols<<<grid, 256, 0, st>>>(out, tmp, n, lo, c_cnt);
+            e = cudaGetLastError();
+        } else if (e == cudaSuccess) {
+            e = launch_transpose_pages(out, tmp, n, 1, st);
+        }
         if (e == cudaSuccess) e = run(tmp, tmp, r_lo, r_cnt);      // along c, every row
         if (e == cudaSuccess) e = launch_transpose_pages(tmp, out, n, 1, st);
         return e;

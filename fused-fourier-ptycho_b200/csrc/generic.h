@@ -37,9 +37,10 @@ public:
     cudaError_t fft2(const float2 *in, float2 *out, float2 *tmp, int n, int count, FftDir dir,
                      cudaStream_t st);
     // One n x n page with the work limited to a box: the transform along r runs only on
-    // columns [c_lo, c_lo + c_cnt) mod n (the other columns must be zero, in == out, or
-    // c_cnt == n) and the transform along c only on rows [r_lo, r_lo + r_cnt) mod n (the
-    // other rows of out are left as the first pass made them).  Exact on the box rows.
+    // columns [c_lo, c_lo + c_cnt) mod n (with c_cnt < n: in == out, r_cnt == n, and the
+    // other columns count as zeros whatever they hold) and the transform along c only on
+    // rows [r_lo, r_lo + r_cnt) mod n (the other rows of out are left as the first pass
+    // made them).  Exact on the box rows.
     cudaError_t fft2_box(const float2 *in, float2 *out, float2 *tmp, int n, FftDir dir, int c_lo,
                          int c_cnt, int r_lo, int r_cnt, cudaStream_t st);
     void release();
