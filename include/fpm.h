@@ -153,7 +153,9 @@ fpm_status fpm_create(fpm_context **ctx, const fpm_device_opts *opts);
    first is replayed from a CUDA graph captured once per learning rate (the reference
    launches every kernel and synchronises after every mini-batch,
    cuFPM_pure_v3.cu:202); with stage profiling on (fpm_set_profiling) the epochs run
-   eagerly. */
+   eagerly.  The context keeps the executable graph: a later capture with the same
+   kernels in the same order (the next learning rate, or a later solve of the same
+   shape) updates it in place; every capture carries that solve's own arguments. */
 fpm_status fpm_solve(fpm_context *ctx, const fpm_problem *prob, fpm_result *res);
 
 /* Many independent reconstructions in one call: tiles of a large field of view, or
