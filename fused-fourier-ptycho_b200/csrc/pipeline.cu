@@ -305,6 +305,12 @@ struct L23 {
 __device__ __forceinline__ void cluster_arrive() {
     asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
 }
+// An arrive that publishes no writes: it only tells the cluster that this CTA's loads of
+// the other CTAs' shared memory are finished, and those loads have returned (their values
+// are stored in this CTA's own shared memory before a block barrier) when it runs.
+__device__ __forceinline__ void cluster_arrive_reads_done() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void cluster_wait() {
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
@@ -439,7 +445,7 @@ __global__ void __launch_bounds__(L23<N, CL>::THREADS, L23<N, CL>::MINB)
         }
         __syncthreads();
     }
-    cluster_arrive();   // done with the neighbours' memory; waited for before the area is reused
+    cluster_arrive_reads_done();   // done with the neighbours' memory; waited for before the area is reused
     double lsum = 0.0;
     if (!failed) {
         const float gscale = (float)(g.pratio * g.pratio);
