@@ -265,7 +265,11 @@ __device__ __forceinline__ void vstage(float2 (&v)[V], float2 *s, int n, int p, 
     if (!last) __syncthreads();   // the stage's outputs visible to the next stage
 }
 
-template <int DIR, int V>
+// TOUT: the output is written transposed, for whole n x n pages (count a multiple of n,
+// ld = n, n a multiple of lpc so that a CTA's lines are consecutive columns of one page):
+// element e of line g = page P, column c goes to out[P][e][c].  The CTA's lines are
+// staged in shared memory as [element][line] and stored as rows of lpc columns.
+template <int DIR, int V, bool TOUT>
 __global__ void __launch_bounds__(512, 1) k_gen_lines_v(const float2 *__restrict__ in,
                                                       float2 *__restrict__ out, long long count,
                                                       size_t ld, VPlan pl,
@@ -304,7 +308,20 @@ __global__ void __launch_bounds__(512, 1) k_gen_lines_v(const float2 *__restrict
         }
         p *= R;
     }
-    if (live) {
+    if constexpr (TOUT) {
+        __syncthreads();                        // the last stage's reads of the area done
+        const int W = pl.lpc + 1;               // padded staging row
+#pragma unroll
+        for (int m = 0; m < V; ++m) smem[(size_t)(t + m * T) * W + line] = v[m];
+        __syncthreads();
+        const long long g0 = (long long)blockIdx.x * pl.lpc;
+        const int l = threadIdx.x % pl.lpc;
+        if (g0 + l < count) {
+            const long long page = g0 / n;
+            float2 *dst = out + (size_t)page * n * n + (size_t)(g0 - page * n) + l;
+            for (int e = threadIdx.x / pl.lpc; e < n; e += T) dst[(size_t)e * n] = smem[(size_t)e * W + l];
+        }
+    } else if (live) {
         float2 *dst = out + (size_t)g * ld;
 #pragma unroll
         for (int m = 0; m < V; ++m) dst[t + m * T] = v[m];
@@ -646,10 +663,10 @@ cudaError_t GenFft::lines(const float2 *in, float2 *out, int n, long long count,
         };
         const bool fwd = dir == kForward;
         switch (vp.V) {
-            case 16: return fwd ? vgo(k_gen_lines_v<-1, 16>) : vgo(k_gen_lines_v<1, 16>);
-            case 20: return fwd ? vgo(k_gen_lines_v<-1, 20>) : vgo(k_gen_lines_v<1, 20>);
-            case 24: return fwd ? vgo(k_gen_lines_v<-1, 24>) : vgo(k_gen_lines_v<1, 24>);
-            default: return fwd ? vgo(k_gen_lines_v<-1, 28>) : vgo(k_gen_lines_v<1, 28>);
+            case 16: return fwd ? vgo(k_gen_lines_v<-1, 16, false>) : vgo(k_gen_lines_v<1, 16, false>);
+            case 20: return fwd ? vgo(k_gen_lines_v<-1, 20, false>) : vgo(k_gen_lines_v<1, 20, false>);
+            case 24: return fwd ? vgo(k_gen_lines_v<-1, 24, false>) : vgo(k_gen_lines_v<1, 24, false>);
+            default: return fwd ? vgo(k_gen_lines_v<-1, 28, false>) : vgo(k_gen_lines_v<1, 28, false>);
         }
     }
     const GenPlan pl = make_plan(n);
@@ -679,9 +696,45 @@ cudaError_t launch_transpose_pages(const float2 *in, float2 *out, int n, int cou
     return cudaGetLastError();
 }
 
+// The register-resident transform of count whole n x n pages, written transposed (see
+// k_gen_lines_v); cudaErrorNotSupported where its plan does not allow it.
+cudaError_t GenFft::pages_t(const float2 *in, float2 *out, int n, int count, FftDir dir,
+                            cudaStream_t st) {
+    VPlan vp;
+    if (knob("FPM_GEN_REG", 0, 0, 1) == 0 || !make_vplan(n, vp) || n % vp.lpc != 0)
+        return cudaErrorNotSupported;
+    const size_t smem = (size_t)n * (vp.lpc + 1) * sizeof(float2);
+    if (smem > 110 * 1024) return cudaErrorNotSupported;   // two CTAs per SM
+    const long long lines = (long long)count * n, blocks = lines / vp.lpc;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const float2 *tw = nullptr;
+    cudaError_t e = table(n, &tw);
+    if (e != cudaSuccess) return e;
+    auto go = [&](auto kernel) {
+        cudaError_t e2 = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem);
+        if (e2 != cudaSuccess) return e2;
+        kernel<<<(unsigned)blocks, vp.T * vp.lpc, smem, st>>>(in, out, lines, (size_t)n, vp, tw);
+        return cudaGetLastError();
+    };
+    const bool fwd = dir == kForward;
+    switch (vp.V) {
+        case 16: return fwd ? go(k_gen_lines_v<-1, 16, true>) : go(k_gen_lines_v<1, 16, true>);
+        case 20: return fwd ? go(k_gen_lines_v<-1, 20, true>) : go(k_gen_lines_v<1, 20, true>);
+        case 24: return fwd ? go(k_gen_lines_v<-1, 24, true>) : go(k_gen_lines_v<1, 24, true>);
+        default: return fwd ? go(k_gen_lines_v<-1, 28, true>) : go(k_gen_lines_v<1, 28, true>);
+    }
+}
+
 cudaError_t GenFft::fft2(const float2 *in, float2 *out, float2 *tmp, int n, int count, FftDir dir,
                          cudaStream_t st) {
     const size_t plane = (size_t)n * n;
+    if (count >= 1 && gen_fft_supported(n)) {
+        // two passes, each writing its pages transposed: along r into tmp, along c back
+        cudaError_t e = pages_t(in, tmp, n, count, dir, st);
+        if (e == cudaSuccess) return pages_t(tmp, out, n, count, dir, st);
+        if (e != cudaErrorNotSupported) return e;
+    }
     // transform along r (contiguous), transpose, along c (now contiguous), transpose back;
     // count pages at a time, at most 65535 per transpose launch
     cudaError_t e = lines(in, out, n, (long long)count * n, n, dir, st);
