@@ -265,15 +265,16 @@ __device__ __forceinline__ void vstage(float2 (&v)[V], float2 *s, int n, int p, 
     if (!last) __syncthreads();   // the stage's outputs visible to the next stage
 }
 
-// TOUT: the output is written transposed, for whole n x n pages (count a multiple of n,
-// ld = n, n a multiple of lpc so that a CTA's lines are consecutive columns of one page):
-// element e of line g = page P, column c goes to out[P][e][c].  The CTA's lines are
-// staged in shared memory as [element][line] and stored as rows of lpc columns.
+// Line g is column c = (g_lo + g) mod n of page P = g / n (with g_lo = 0: line g at
+// in + g*ld, the plain batch of lines).  TOUT: the output is written transposed, for
+// n x n pages (ld = n; whole pages, or with g_lo the columns [g_lo, g_lo + count) mod n of
+// one page): element e of line g goes to out[P][e][c].  The CTA's lines are staged in
+// shared memory as [element][line] and stored as rows of lpc columns.
 template <int DIR, int V, bool TOUT>
 __global__ void __launch_bounds__(512, 1) k_gen_lines_v(const float2 *__restrict__ in,
                                                       float2 *__restrict__ out, long long count,
                                                       size_t ld, VPlan pl,
-                                                      const float2 *__restrict__ tw) {
+                                                      const float2 *__restrict__ tw, int g_lo) {
     extern __shared__ float2 smem[];
     const int n = pl.n, T = pl.T;
     const int line = threadIdx.x / T, t = threadIdx.x - line * T;
@@ -281,7 +282,12 @@ __global__ void __launch_bounds__(512, 1) k_gen_lines_v(const float2 *__restrict
     const bool live = g < count;   // lines past the last one join every barrier on zeros
     float2 *s = smem + (size_t)line * n;
     float2 v[V];
-    const float2 *src = in + (size_t)(live ? g : 0) * ld;
+    auto line_of = [&](long long gg) {   // page * n + column of line gg
+        const long long page = gg / n;
+        const int c = (int)((g_lo + (gg - page * n)) % n);
+        return page * n + c;
+    };
+    const float2 *src = in + (size_t)(live ? (TOUT && g_lo ? line_of(g) : g) : 0) * ld;
 #pragma unroll
     for (int m = 0; m < V; ++m) v[m] = live ? src[t + m * T] : make_float2(0.f, 0.f);
     const int mask = n % 16 == 0 ? 15 : 0;
@@ -314,11 +320,11 @@ __global__ void __launch_bounds__(512, 1) k_gen_lines_v(const float2 *__restrict
 #pragma unroll
         for (int m = 0; m < V; ++m) smem[(size_t)(t + m * T) * W + line] = v[m];
         __syncthreads();
-        const long long g0 = (long long)blockIdx.x * pl.lpc;
         const int l = threadIdx.x % pl.lpc;
-        if (g0 + l < count) {
-            const long long page = g0 / n;
-            float2 *dst = out + (size_t)page * n * n + (size_t)(g0 - page * n) + l;
+        const long long gl = (long long)blockIdx.x * pl.lpc + l;
+        if (gl < count) {
+            const long long pc = line_of(gl), page = pc / n;
+            float2 *dst = out + (size_t)page * n * n + (size_t)(pc - page * n);
             for (int e = threadIdx.x / pl.lpc; e < n; e += T) dst[(size_t)e * n] = smem[(size_t)e * W + l];
         }
     } else if (live) {
@@ -658,7 +664,7 @@ cudaError_t GenFft::lines(const float2 *in, float2 *out, int n, long long count,
             cudaError_t e2 = cudaFuncSetAttribute(
                 kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsmem);
             if (e2 != cudaSuccess) return e2;
-            kernel<<<(unsigned)vblocks, vp.T * vp.lpc, vsmem, st>>>(in, out, count, ld, vp, tw);
+            kernel<<<(unsigned)vblocks, vp.T * vp.lpc, vsmem, st>>>(in, out, count, ld, vp, tw, 0);
             return cudaGetLastError();
         };
         const bool fwd = dir == kForward;
@@ -696,16 +702,20 @@ cudaError_t launch_transpose_pages(const float2 *in, float2 *out, int n, int cou
     return cudaGetLastError();
 }
 
-// The register-resident transform of count whole n x n pages, written transposed (see
-// k_gen_lines_v); cudaErrorNotSupported where its plan does not allow it.
-cudaError_t GenFft::pages_t(const float2 *in, float2 *out, int n, int count, FftDir dir,
-                            cudaStream_t st) {
+// The register-resident transform of `lines` lines of n x n pages, written transposed (see
+// k_gen_lines_v): whole pages (g_lo = 0, lines a multiple of n) or the columns
+// [g_lo, g_lo + lines) mod n of one page; cudaErrorNotSupported where its plan does not
+// allow it.
+cudaError_t GenFft::lines_t(const float2 *in, float2 *out, int n, int g_lo, long long lines,
+                            FftDir dir, cudaStream_t st) {
     VPlan vp;
     if (knob("FPM_GEN_REG", 0, 0, 1) == 0 || !make_vplan(n, vp) || n % vp.lpc != 0)
         return cudaErrorNotSupported;
     const size_t smem = (size_t)n * (vp.lpc + 1) * sizeof(float2);
     if (smem > 110 * 1024) return cudaErrorNotSupported;   // two CTAs per SM
-    const long long lines = (long long)count * n, blocks = lines / vp.lpc;
+    if (lines < 1 || (g_lo != 0 && lines > n) || (g_lo == 0 && lines % n != 0 && lines > n))
+        return cudaErrorInvalidValue;
+    const long long blocks = (lines + vp.lpc - 1) / vp.lpc;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const float2 *tw = nullptr;
     cudaError_t e = table(n, &tw);
@@ -714,7 +724,8 @@ cudaError_t GenFft::pages_t(const float2 *in, float2 *out, int n, int count, Fft
         cudaError_t e2 = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem);
         if (e2 != cudaSuccess) return e2;
-        kernel<<<(unsigned)blocks, vp.T * vp.lpc, smem, st>>>(in, out, lines, (size_t)n, vp, tw);
+        kernel<<<(unsigned)blocks, vp.T * vp.lpc, smem, st>>>(in, out, lines, (size_t)n, vp, tw,
+                                                              g_lo);
         return cudaGetLastError();
     };
     const bool fwd = dir == kForward;
@@ -731,8 +742,9 @@ cudaError_t GenFft::fft2(const float2 *in, float2 *out, float2 *tmp, int n, int 
     const size_t plane = (size_t)n * n;
     if (count >= 1 && gen_fft_supported(n)) {
         // two passes, each writing its pages transposed: along r into tmp, along c back
-        cudaError_t e = pages_t(in, tmp, n, count, dir, st);
-        if (e == cudaSuccess) return pages_t(tmp, out, n, count, dir, st);
+        const long long lines = (long long)count * n;
+        cudaError_t e = lines_t(in, tmp, n, 0, lines, dir, st);
+        if (e == cudaSuccess) return lines_t(tmp, out, n, 0, lines, dir, st);
         if (e != cudaErrorNotSupported) return e;
     }
     // transform along r (contiguous), transpose, along c (now contiguous), transpose back;

@@ -47,8 +47,8 @@ public:
 
 private:
     cudaError_t table(int n, const float2 **tw);
-    cudaError_t pages_t(const float2 *in, float2 *out, int n, int count, FftDir dir,
-                        cudaStream_t st);
+    cudaError_t lines_t(const float2 *in, float2 *out, int n, int g_lo, long long lines,
+                        FftDir dir, cudaStream_t st);
     std::map<int, float2 *> tw_;
 };
 
